@@ -1,0 +1,272 @@
+/*
+ * y3b.h -- C ABI of the B200 engine for the DES-Y3 cluster-observable
+ * integrals (number counts N(lambda_obs bin, z_obs bin) and the stacked
+ * miscentred-NFW DeltaSigma one-halo profile in the same bins).
+ *
+ * Plain C: POD structs, raw pointers and sizes, integer status codes.  No
+ * function throws; every failure returns a non-zero y3b_status and leaves a
+ * message for y3b_last_error().  All compute runs on the current CUDA device
+ * (or the one chosen with y3b_device_init); there is no CPU fallback -- on a
+ * machine without a usable sm_100 device every compute entry point returns
+ * Y3B_ERR_CUDA.
+ *
+ * Reference interfaces replaced (paths inside estevesjh/y3_cluster_cpp):
+ *   y3b_sel_function        src/modules/sel_function/sel_function.py:555-615
+ *                           (execute: S_stack producer)
+ *   y3b_selgl_*             src/models/n_operator_sel_gl_t.hh:75-361
+ *                           (SelGLCore, NumCountsSelGL, Shear1hMisSelGL)
+ *   y3b_sigma_crit_inv      src/modules/average_sigma_crit_inv/
+ *                           average_sigma_crit_inv.py:32-61
+ *   y3b_nfw_mis             src/models/nfw_dsigma_mis.hh:95-114 and
+ *                           src/models/nfw_sigma_mis.hh:53-66
+ *   y3b_engine_*            the fused fast_mass form of the same integrals
+ *                           (NumCountsFastMass / Shear1hFastMass, documented
+ *                           as identical to the two modules above), with the
+ *                           lambda_t / lambda_o / z_o integrals of
+ *                           sel_function.py done on fixed quadrature nodes.
+ * The CosmoSIS module ABI (setup/execute/cleanup of
+ * src/utils/module_macros.hh:76-99) is declared in y3b_cosmosis.h.
+ */
+#ifndef Y3B_H
+#define Y3B_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define Y3B_VERSION 1
+
+typedef enum {
+  Y3B_OK = 0,
+  Y3B_ERR_INVALID = 1,     /* bad argument or shape */
+  Y3B_ERR_DOMAIN = 2,      /* query outside an unclamped table (the reference throws std::domain_error) */
+  Y3B_ERR_CUDA = 3,        /* CUDA runtime failure or no usable device */
+  Y3B_ERR_NOMEM = 4,       /* device allocation failed */
+  Y3B_ERR_TIMEOUT = 5,     /* a bounded device-side wait ran out */
+  Y3B_ERR_BUDGET = 6,      /* request exceeds the configured HBM budget */
+  Y3B_ERR_UNSUPPORTED = 7  /* shape the kernel does not support */
+} y3b_status;
+
+/* Message of the last failure on the calling thread ("" if none). */
+const char* y3b_last_error(void);
+int y3b_version(void);
+/* Select the CUDA device for the calling thread; checks it is sm_100. */
+int y3b_device_init(int device);
+/* Number of kernel launches issued by this library since load (all threads). */
+unsigned long long y3b_launch_count(void);
+
+/* ---------------------------------------------------------------------- */
+/* Shared POD types                                                        */
+
+typedef struct {
+  double om, ol, ok, h0, onu, hmf_s, hmf_q; /* cosmological_parameters/{omega_M,
+                                               omega_lambda, omega_k, h0, omega_nu},
+                                               cluster_abundance/{hmf_s, hmf_q} */
+} y3b_cosmo;
+
+/* Per-sample tables, as the DataBlock holds them (all FP64, host or device
+ * memory depending on the call). */
+typedef struct {
+  int n_hm;  const double* hmf_m_h;   /* mass_function/m_h             */
+  int n_hz;  const double* hmf_z;     /* mass_function/z               */
+  const double* dndlnmh;              /* mass_function/dndlnmh [n_hz][n_hm] */
+  int n_dist; const double* dist_z;   /* distances/z                   */
+  const double* dist_da;              /* distances/d_a [Mpc]           */
+  int n_sci; const double* sci_z;     /* average_sigma_crit_inv/zlense (0 if unused) */
+  const double* sci_val;              /* average_sigma_crit_inv/sci_average */
+} y3b_tables;
+
+/* P(lambda_obs | lambda_true, z) coefficient table: 8 rows of n values in
+ * the order a_tau, b_tau, a_mu, b_mu, a_sig, b_sig, a_fprj, b_fprj
+ * (plob_ltr_params section; y3_buzzard/prj_params.py:58-61). */
+typedef struct {
+  int n;
+  const double* z;
+  const double* coef;
+} y3b_plob;
+
+typedef enum { Y3B_MOR_HOD = 0, Y3B_MOR_LOGNORMAL = 1 } y3b_mor_kind;
+
+/* HOD: p = {log10_Mmin, log10_M1, alpha, epsilon, sigma_lambda, z_pivot}
+ * (cluster_mor section, sel_function.py:493-513).
+ * LOGNORMAL: p = {A, B, C, sigma, Mpiv, lam_lo, lam_hi}: ln lambda ~
+ * N(A + B ln(M/Mpiv) + C ln(1+z), sigma) truncated to [lam_lo, lam_hi]. */
+typedef struct {
+  int kind;
+  double p[8];
+} y3b_mor;
+
+/* ---------------------------------------------------------------------- */
+/* sel_function: S_ij(lnM, z) on a shared linear grid (sel_function.py).   */
+
+typedef struct {
+  int n_bins;
+  const double* lam_min; const double* lam_max;   /* per bin */
+  const double* zob_min; const double* zob_max;
+  const double* sigma_z;
+  double zt_low, zt_high, lnm_low, lnm_high;
+  int n_lnm, n_z, n_q;                            /* n_lnm, n_z_shared, N_q */
+} y3b_selfunc_config;
+
+/* Host buffers: lnm_out[n_lnm], z_out[n_z], S_out[n_bins][n_z][n_lnm].
+ * Replaces sel_function.py:555-615. */
+int y3b_sel_function(const y3b_selfunc_config* cfg, const y3b_mor* mor,
+                     const y3b_plob* plob, double* lnm_out, double* z_out,
+                     double* S_out);
+
+/* ---------------------------------------------------------------------- */
+/* SelGLCore: fixed-GL z-contracted mass weights and the two evaluators.  */
+
+typedef struct {
+  int n_lnm, n_z;                       /* defaults 96, 64 */
+  double zt_low, zt_high, lnm_low, lnm_high;
+} y3b_selgl_config;
+
+typedef struct {
+  int n_bins;
+  int n_lnm; const double* lnm;         /* sel_function/lnM */
+  int n_z;   const double* z;           /* sel_function/z   */
+  const double* S_stack;                /* [n_bins][n_z][n_lnm] */
+} y3b_selection;
+
+/* Centred DeltaSigma table haloModel/{r_sigma, lnM, dSigma_nfw[n_lnm][n_r]}
+ * and the miscentring settings of Shear1hMisSelGL. */
+typedef struct {
+  int n_r;   const double* r_sigma;
+  int n_lnm; const double* lnM;
+  const double* dsigma;
+  double f_mis, tau_mis;                /* miscentering/{f_mis, tau_mis}    */
+  int n_lob; const double* lob_centers; /* module option lob_centers        */
+  double conc;                          /* NFW_DSIGMA_MIS concentration (4) */
+  int n_theta, n_s; double s_max;       /* miscentring quadrature (64, 128, 20) */
+  int use_idea2; double stencil_h;      /* method = idea2 / stencil_h       */
+} y3b_shear_table;
+
+typedef struct y3b_selgl y3b_selgl;
+
+/* setup(): GL nodes for the configured box.  n_z/GL on device. */
+int y3b_selgl_create(const y3b_selgl_config* cfg, y3b_selgl** out);
+/* set_sample(): build W_b(lnM_k) (include_sci adds Sigma_crit^-1(z)).
+ * Returns Y3B_ERR_DOMAIN if a GL z node lies outside distances/z. */
+int y3b_selgl_build(y3b_selgl* h, const y3b_cosmo* c, const y3b_tables* t,
+                    const y3b_selection* sel, int include_sci);
+/* NumCountsSelGL::evaluate over a wall of bin indices -> vals[n]. */
+int y3b_selgl_counts(y3b_selgl* h, int n, const int* bin_index, double* vals);
+/* Shear1hMisSelGL::evaluate over (bin_index[i], r[i]) pairs -> vals[n]. */
+int y3b_selgl_shear(y3b_selgl* h, const y3b_shear_table* st, int n,
+                    const int* bin_index, const double* r, double* vals);
+/* Copy out W [n_bins][n_lnm], norm, lnm_eff, mu2 and the GL nodes/weights. */
+int y3b_selgl_weights(y3b_selgl* h, double* W, double* norm, double* lnm_eff,
+                      double* mu2, double* lnm_x, double* lnm_w);
+int y3b_selgl_n_bins(const y3b_selgl* h);
+void y3b_selgl_destroy(y3b_selgl* h);
+
+/* ---------------------------------------------------------------------- */
+/* <Sigma_crit^-1>(z_l) (average_sigma_crit_inv.py:40-58), host buffers.   */
+int y3b_sigma_crit_inv(int n_zl, const double* zl, int n_zs, const double* zs,
+                       const double* pz, double delta_z, double h0,
+                       int n_dist, const double* dist_z, const double* dist_da,
+                       double* out);
+
+/* Miscentred NFW profiles at n points: out[i] = 2 r_s delta_c rho 1e-12 *
+ * <profile>(r[i]/r_s, rmis[i]/r_s), r_s from lnM[i], concentration conc and
+ * rho (NFW_DSIGMA_MIS(c, rho) / NFW_SIGMA_MIS(c, rho) operator()).
+ * which = 0: DeltaSigma_mis, 1: Sigma_mis.  Host buffers. */
+int y3b_nfw_mis(int which, int n, const double* r, const double* rmis,
+                const double* lnM, double conc, double rho, int n_theta,
+                int n_s, double s_max, double* out);
+
+/* ---------------------------------------------------------------------- */
+/* Engine: many parameter points (walkers) on fixed nested Gauss-Legendre */
+/* nodes; FP64 direct form or the mixed form (FP32 integrands, split-BF16  */
+/* tensor-core contraction, FP64 final sums).                              */
+
+typedef struct {
+  int n_m, n_z, n_t, n_o, n_zo;         /* lnM, z_t, ln lam_t, lam_o/bin, z_o/bin */
+  double lnm_lo, lnm_hi, zt_lo, zt_hi;  /* integration box */
+  double lam_t_lo, lam_t_hi;            /* lam_t domain of the MOR */
+  int n_lam_bins, n_z_bins;             /* <= 8, <= 8 */
+  double lam_edges[9];
+  double zob_edges[9];
+  double sz0;                           /* sigma_z(z_t) = sz0 (1 + z_t) */
+} y3b_grid;
+
+typedef struct {
+  int n_R;
+  double R[32];                         /* projected radii [Mpc/h] */
+  double f_mis, tau_mis;
+  double lob_centers[8];                /* per richness bin */
+  double c0, c_slope, c_pivot;          /* c(M) = c0 (M / c_pivot)^c_slope */
+  int n_theta, n_s;
+  double s_max;
+} y3b_shear_opts;
+
+typedef struct {
+  int n_hm, n_hz, n_dist, n_sci;        /* table shapes shared by all points */
+  y3b_plob plob;                        /* P(lam_o | lam_t, z) coefficients */
+  int max_points;                       /* capacity of one eval call */
+  size_t hbm_budget;                    /* bytes of device memory the engine may hold (0: 150 GB) */
+  int with_shear;
+  y3b_shear_opts shear;
+} y3b_engine_config;
+
+typedef struct {
+  y3b_cosmo cosmo;
+  double A, B, C, sigma, Mpiv;          /* lognormal MOR */
+  int grid;                             /* index into the engine's grids */
+  int reserved;
+} y3b_point;
+
+typedef enum { Y3B_FP64 = 0, Y3B_MIXED = 1 } y3b_precision;
+
+typedef struct y3b_engine y3b_engine;
+
+int y3b_engine_create(const y3b_grid* grids, int n_grids,
+                      const y3b_engine_config* cfg, y3b_engine** out);
+void y3b_engine_destroy(y3b_engine* e);
+/* Doubles per point in the packed table buffer (each section 16-byte
+ * aligned): hmf_m_h[n_hm] | hmf_z[n_hz] | dndlnmh[n_hz*n_hm] | dist_z[n_dist]
+ * | dist_da[n_dist] | sci_z[n_sci] | sci_val[n_sci]. */
+size_t y3b_engine_table_stride(const y3b_engine* e);
+/* Offsets (in doubles) of the seven sections inside one point's block. */
+int y3b_engine_table_offsets(const y3b_engine* e, size_t* off7);
+int y3b_engine_n_bins(const y3b_engine* e);
+/* Device bytes the engine holds (tables, scratch, outputs). */
+size_t y3b_engine_device_bytes(const y3b_engine* e);
+
+/* Host-buffer evaluation: copies points and tables in, evaluates, copies
+ * counts [n][n_bins] (and shear [n][n_bins][n_R] if enabled) out.
+ * Synchronous on the engine's stream. */
+int y3b_engine_eval(y3b_engine* e, int precision, int n,
+                    const y3b_point* pts, const double* tables,
+                    double* counts, double* shear);
+/* Device-buffer evaluation, asynchronous on `stream` (a cudaStream_t; NULL
+ * = the engine's stream).  All pointers are device pointers; counts/shear
+ * as above.  Returns after enqueueing; the status of device-side checks is
+ * read with y3b_engine_sync. */
+int y3b_engine_eval_device(y3b_engine* e, int precision, int n,
+                           const y3b_point* pts_dev, const double* tables_dev,
+                           double* counts_dev, double* shear_dev, void* stream);
+/* Wait for the engine's work on `stream` and report device-side errors. */
+int y3b_engine_sync(y3b_engine* e, void* stream);
+/* Optional: the mass weights W_b(lnM_k) of the last eval ([n][n_bins][n_m]
+ * of each point's grid, padded to the largest n_m), host buffer. */
+int y3b_engine_weights(y3b_engine* e, int n, double* W);
+
+/* Self-test of the bounded device wait: launches a kernel that waits on a
+ * barrier nobody arrives at for ~`usec` microseconds and must come back
+ * with Y3B_ERR_TIMEOUT (the context stays usable). */
+int y3b_selftest_wait_timeout(int usec);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,236 @@
+"""Generate the golden fixtures that pin the oracle to the reference.
+
+Run in a container that has the reference checkout at /root/reference
+(read-only); the outputs are committed, so neither the tests nor the GPU runs
+need the reference at run time:
+
+    python tests/golden/make_golden.py [/root/reference]
+
+What it writes (tests/golden/*.npz / *.json):
+
+* sel_function_hod.npz -- S_stack from the reference's own
+  src/modules/sel_function/sel_function.py (setup/execute, HOD MOR, default
+  projection table from y3_buzzard/prj_params.py) on a reduced grid with the
+  DES-Y3 bin layout of cosmosis-models/des_y3.ini:114-133.
+* sel_function_lognormal.npz -- the same reference execute() with its MOR
+  stage (_compute_lam_nodes_and_P_HOD) swapped for the lognormal MOR of the
+  synthetic configs and the constant-in-z projection coefficients published
+  through the plob_ltr_params section; everything downstream of the MOR
+  (plob params, CDF differencing, K_j, packing) is the reference's code.
+* kats.json -- the reference's own known-answer tables read as text:
+  data/test_dv_do_dz.txt + z_da_test.txt + d_a_test.txt
+  (test/dv_do_dz_t.test.cc), data/test_Rmis.txt (test/roffset_t.test.cc),
+  data/test_int_zo_zt_des.txt (test/int_zo_zt_des_t.test.cc), the
+  cluster_toolkit answers of test/nfw_dsigma_mis.test.cu:32-48 and
+  test/nfw_sigma_mis.test.cu:32-46, and the interpolation KATs of
+  test/interp_1d.test.cc / test/interp_2d.test.cc.
+"""
+from __future__ import annotations
+
+import json
+import os
+import re
+import sys
+import tempfile
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _install_cosmosis_stub():
+    mod = types.ModuleType("cosmosis")
+    db = types.ModuleType("cosmosis.datablock")
+    db.option_section = "module_options"
+    names = types.SimpleNamespace(cosmological_parameters="cosmological_parameters")
+    db.names = names
+    mod.datablock = db
+    sys.modules["cosmosis"] = mod
+    sys.modules["cosmosis.datablock"] = db
+
+
+class Options:
+    """The subset of the CosmoSIS options API that sel_function.setup uses."""
+
+    def __init__(self, d):
+        self.d = d
+
+    def _get(self, key):
+        if key not in self.d:
+            raise KeyError(key)
+        return self.d[key]
+
+    def get_double_array_1d(self, sec, key):
+        v = self._get(key)
+        if np.ndim(v) == 0:
+            raise TypeError(key)
+        return np.asarray(v, dtype=float)
+
+    def get_int_array_1d(self, sec, key):
+        return np.asarray(self._get(key), dtype=int)
+
+    def get_double(self, sec, key):
+        v = self._get(key)
+        if np.ndim(v) != 0:
+            raise TypeError(key)
+        return float(v)
+
+    def get_int(self, sec, key):
+        v = self._get(key)
+        if not isinstance(v, (int, np.integer)):
+            raise TypeError(key)
+        return int(v)
+
+
+class Block(dict):
+    """dict keyed by (section, name), like the CosmoSIS DataBlock python API."""
+
+
+BINS = dict(
+    lam_min=[20.0, 30.0, 45.0, 60.0] * 3,
+    lam_max=[30.0, 45.0, 60.0, 200.0] * 3,
+    zob_min=[0.20] * 4 + [0.35] * 4 + [0.50] * 4,
+    zob_max=[0.35] * 4 + [0.50] * 4 + [0.65] * 4,
+    sigma_z=[0.03] * 12,
+)
+ENVELOPE = dict(zt_low=0.05, zt_high=0.80, lnm_low=29.9336, lnm_high=36.8414)
+GRID = dict(n_lnm=24, n_z_shared=12, N_q=16)
+HOD = dict(log10_Mmin=11.4, log10_M1=12.7, alpha=0.86, epsilon=0.0, sigma_lambda=0.18)
+LOGNORMAL = dict(A=3.2, B=0.9, C=0.5, sigma=0.2, Mpiv=3e14, lam_lo=1.0, lam_hi=1000.0)
+
+
+def lognormal_stage(mor_ln):
+    """Swap-in for sel_function._compute_lam_nodes_and_P_HOD: per-cell GL
+    bracket exp(mu -+ 6 sigma) clipped to [lam_lo, lam_hi] and the truncated
+    lognormal density in lambda, renormalised by an erf difference."""
+    from scipy.special import erfc
+
+    def phi_diff(a, b):
+        return np.where(a >= 0, 0.5 * (erfc(a / np.sqrt(2)) - erfc(b / np.sqrt(2))),
+                        np.where(b <= 0, 0.5 * (erfc(-b / np.sqrt(2)) - erfc(-a / np.sqrt(2))),
+                                 1 - 0.5 * erfc(-a / np.sqrt(2)) - 0.5 * erfc(b / np.sqrt(2))))
+
+    def stage(lnM, z, mor, gl_t, gl_w, L=6.0):
+        m = mor_ln
+        mu = (m["A"] + m["B"] * (lnM[:, None] - np.log(m["Mpiv"]))
+              + m["C"] * np.log1p(z[None, :]))
+        a = np.maximum(m["lam_lo"], np.exp(mu - L * m["sigma"]))
+        b = np.minimum(m["lam_hi"], np.exp(mu + L * m["sigma"]))
+        degenerate = b <= a
+        half, mid = 0.5 * (b - a), 0.5 * (a + b)
+        lam_k = mid[..., None] + half[..., None] * gl_t[None, None, :]
+        W_k = half[..., None] * gl_w[None, None, :]
+        D = phi_diff((np.log(m["lam_lo"]) - mu) / m["sigma"],
+                     (np.log(m["lam_hi"]) - mu) / m["sigma"])
+        d = (np.log(lam_k) - mu[..., None]) / m["sigma"]
+        P = np.exp(-0.5 * d * d) / (np.sqrt(2 * np.pi) * m["sigma"] * lam_k * D[..., None])
+        return lam_k, W_k, P, degenerate
+
+    return stage
+
+
+def run_sel_function(ref, lognormal):
+    sys.path.insert(0, os.path.join(ref, "src", "modules", "sel_function"))
+    sys.path.insert(0, ref)
+    import sel_function as sf
+    from y3_buzzard import prj_params as pp
+
+    opts = dict(BINS)
+    opts.update(ENVELOPE)
+    opts["n_lnm"] = GRID["n_lnm"]
+    opts["n_z_shared"] = GRID["n_z_shared"]
+    opts["N_q"] = GRID["N_q"]
+    cfg = sf.setup(Options(opts))
+    block = Block()
+    for k, v in HOD.items():
+        block["cluster_mor", k] = v
+    saved = sf._compute_lam_nodes_and_P_HOD
+    try:
+        if lognormal:
+            sf._compute_lam_nodes_and_P_HOD = lognormal_stage(LOGNORMAL)
+            i = int(np.argmin(np.abs(pp.PrjParams.default().z - 0.45)))
+            base = pp.PrjParams.default()
+            block["plob_ltr_params", "z"] = np.array([0.0, 2.0])
+            const = dict(a_tau=base.a_tau[i], b_tau=base.b_tau[i], a_mu=0.0, b_mu=1.0,
+                         a_sig=1.0, b_sig=0.1, a_fprj=0.0, b_fprj=0.1)
+            for k, v in const.items():
+                block["plob_ltr_params", k] = np.array([v, v])
+        sf.execute(block, cfg)
+    finally:
+        sf._compute_lam_nodes_and_P_HOD = saved
+    return (np.asarray(block["sel_function", "lnM"]), np.asarray(block["sel_function", "z"]),
+            np.asarray(block["sel_function", "S_stack"]))
+
+
+def _floats(text):
+    return [float(x) for x in re.findall(r"[-+]?\d*\.\d+(?:[eE][-+]?\d+)?|[-+]?\d+(?:[eE][-+]?\d+)?", text)]
+
+
+def _array_literal(src, name):
+    m = re.search(r"std::vector<double>\s+" + name + r"\s*\{(.*?)\};", src, re.S)
+    body = re.sub(r"//[^\n]*", "", m.group(1))
+    return _floats(body)
+
+
+def kats(ref):
+    out = {}
+    d = os.path.join(ref, "data")
+    tab = np.loadtxt(os.path.join(d, "test_dv_do_dz.txt"))
+    out["dv_do_dz"] = dict(z=tab[:, 0].tolist(), dv=tab[:, 1].tolist(),
+                           dist_z=np.loadtxt(os.path.join(d, "z_da_test.txt")).tolist(),
+                           dist_da=np.loadtxt(os.path.join(d, "d_a_test.txt")).tolist(),
+                           om=0.3, ol=0.7, ok=0.0, h=0.7, epsrel=1e-3,
+                           source="test/dv_do_dz_t.test.cc:15-53")
+    tab = np.loadtxt(os.path.join(d, "test_Rmis.txt"), comments="#")
+    out["roffset"] = dict(r=tab[:, 0].tolist(), p=tab[:, 1].tolist(), tau=0.15,
+                          epsrel=1e-6, source="test/roffset_t.test.cc:10-55")
+    tab = np.loadtxt(os.path.join(d, "test_int_zo_zt_des.txt"), comments="#")
+    out["int_zo_zt"] = dict(zmin=tab[:, 0].tolist(), zmax=tab[:, 1].tolist(),
+                            zt=tab[:, 2].tolist(), sigma=tab[:, 3].tolist(),
+                            integral=tab[:, 4].tolist(), epsrel=1e-6, epsabs=1e-12,
+                            source="test/int_zo_zt_des_t.test.cc:13-60")
+    for name, fn, tol in (("dsigma_mis", "nfw_dsigma_mis.test.cu", 5e-3),
+                          ("sigma_mis", "nfw_sigma_mis.test.cu", 1e-3)):
+        src = open(os.path.join(ref, "test", fn)).read()
+        out[name] = dict(r=_array_literal(src, "r"), rmis=_array_literal(src, "rmis"),
+                         lnM=_array_literal(src, "lnMs"), answers=_array_literal(src, "answers"),
+                         conc=4.0, omega_m=0.3, epsrel=tol, epsabs=1e-12,
+                         source=f"test/{fn}:18-77")
+    out["interp2d"] = dict(
+        xs=[1.0, 2.0, 3.0], ys=[4.0, 5.0], f="3*x*y + 2*x + 4*y",
+        cases=[[2.5, 4.5, 56.75]],
+        clamp=[[0, 4.5, 1, 4.5], [4, 4.5, 3, 4.5], [2, 3, 2, 4], [2, 5.5, 2, 5],
+               [0, 0, 1, 4], [4, 3, 3, 4], [0, 6, 1, 5], [4, 6, 3, 5]],
+        source="test/interp_2d.test.cc:27-60")
+    out["interp2d_linear"] = dict(xs=[1.0, 2.0, 3.0], ys=[1.0, 2.0, 3.0, 4.0],
+                                  f="2*x + 3*y - 5", cases=[[2.5, 1.5, 4.5]],
+                                  source="test/interp_2d.test.cc:92-114")
+    out["interp1d"] = dict(xs=[1.0, 2.0, 3.0], f="x*x", cases=[[1.41421, 2.24263, 1e-4]],
+                           throws=[[-5.0, 5.0, -10.0], [-5.0, 5.0, 10.0]],
+                           source="test/interp_1d.test.cc:23-44")
+    return out
+
+
+def main(ref="/root/reference"):
+    _install_cosmosis_stub()
+    with tempfile.TemporaryDirectory():
+        lnm, z, S = run_sel_function(ref, lognormal=False)
+        np.savez(os.path.join(HERE, "sel_function_hod.npz"), lnM=lnm, z=z, S_stack=S,
+                 **{k: np.asarray(v) for k, v in BINS.items()},
+                 **{k: np.asarray(v) for k, v in ENVELOPE.items()},
+                 **{k: np.asarray(v) for k, v in GRID.items()},
+                 **{"hod_" + k: np.asarray(v) for k, v in HOD.items()})
+        lnm, z, S = run_sel_function(ref, lognormal=True)
+        np.savez(os.path.join(HERE, "sel_function_lognormal.npz"), lnM=lnm, z=z, S_stack=S,
+                 **{k: np.asarray(v) for k, v in BINS.items()},
+                 **{k: np.asarray(v) for k, v in ENVELOPE.items()},
+                 **{k: np.asarray(v) for k, v in GRID.items()},
+                 **{"ln_" + k: np.asarray(v) for k, v in LOGNORMAL.items()})
+    with open(os.path.join(HERE, "kats.json"), "w") as f:
+        json.dump(kats(ref), f, indent=1)
+    print("wrote golden fixtures to", HERE)
+
+
+if __name__ == "__main__":
+    main(*sys.argv[1:])

@@ -1,0 +1,150 @@
+"""The CosmoSIS module objects driven through setup / execute / cleanup on a
+standalone DataBlock, against the library and the oracle."""
+import numpy as np
+import pytest
+
+import oracle as O
+from y3_cluster_cpp_b200 import engine as E
+from y3_cluster_cpp_b200 import sel_function as SF
+from y3_cluster_cpp_b200 import synthetic
+from y3_cluster_cpp_b200.cosmosis import DataBlock, Module
+
+pytestmark = pytest.mark.gpu
+
+BINS = dict(lam_min=[20.0, 30.0, 45.0, 60.0] * 3, lam_max=[30.0, 45.0, 60.0, 200.0] * 3,
+            zob_min=[0.20] * 4 + [0.35] * 4 + [0.50] * 4,
+            zob_max=[0.35] * 4 + [0.50] * 4 + [0.65] * 4, sigma_z=[0.03] * 12)
+
+
+class Options:
+    """The CosmoSIS python options API used by sel_function.setup."""
+
+    def __init__(self, d):
+        self.d = d
+
+    def get_double_array_1d(self, s, k):
+        v = self.d[k]
+        if np.ndim(v) == 0:
+            raise TypeError(k)
+        return np.asarray(v, float)
+
+    def get_int_array_1d(self, s, k):
+        return np.asarray(self.d[k], int)
+
+    def get_double(self, s, k):
+        return float(self.d[k])
+
+    def get_int(self, s, k):
+        v = self.d[k]
+        if not isinstance(v, int):
+            raise TypeError(k)
+        return v
+
+    def get_string(self, s, k):
+        return str(self.d[k])
+
+
+def _sample_block(p, mor="hod"):
+    b = DataBlock()
+    b["cosmological_parameters", "omega_M"] = p.om
+    b["cosmological_parameters", "omega_lambda"] = 1 - p.om
+    b["cosmological_parameters", "omega_k"] = 0.0
+    b["cosmological_parameters", "h0"] = p.h0
+    b["cosmological_parameters", "omega_nu"] = 0.0
+    b["cluster_abundance", "hmf_s"] = 0.0
+    b["cluster_abundance", "hmf_q"] = 1.0
+    t = p.tables
+    b["mass_function", "m_h"] = t["hmf_m_h"]
+    b["mass_function", "z"] = t["hmf_z"]
+    b["mass_function", "dndlnmh"] = t["dndlnmh"]
+    b["distances", "z"] = t["dist_z"]
+    b["distances", "d_a"] = t["dist_da"]
+    b["average_sigma_crit_inv", "zlense"] = t["sci_z"]
+    b["average_sigma_crit_inv", "sci_average"] = t["sci_val"]
+    for k, v in dict(log10_Mmin=11.4, log10_M1=12.7, alpha=0.86, epsilon=0.0,
+                     sigma_lambda=0.18).items():
+        b["cluster_mor", k] = v
+    return b
+
+
+def test_pipeline_sel_function_then_numcounts(gpu):
+    """sel_function (python module) -> NumCountsSel.so on one DataBlock, as
+    the des_y3.ini pipeline runs them; compared with the oracle chain."""
+    p = synthetic.fiducial()
+    opts = dict(BINS, zt_low=0.05, zt_high=0.8, lnm_low=29.9336, lnm_high=36.8414,
+                n_lnm=96, n_z_shared=32, N_q=24)
+    cfg = SF.setup(Options(opts))
+    block = _sample_block(p)
+    assert SF.execute(block, cfg) == 0
+    S = block["sel_function", "S_stack"]
+    assert S.shape == (12, 32, 96)
+
+    m = Module("NumCountsSel")
+    o = DataBlock()
+    o["NumCountsSel", "bin_index"] = np.arange(12)
+    o["NumCountsSel", "zt_low"] = 0.1
+    o["NumCountsSel", "zt_high"] = 0.8
+    o["NumCountsSel", "lnm_low"] = 29.9336
+    o["NumCountsSel", "lnm_high"] = 35.69
+    o["NumCountsSel", "n_lnm"] = 64
+    o["NumCountsSel", "n_z"] = 32
+    assert m.setup(o)
+    assert m.execute(block) == 0
+    vals = block["numcountssel", "vals"]
+    sel = (block["sel_function", "lnM"], block["sel_function", "z"], S)
+    _, norm, _, _ = O.selgl_weights(64, 32, 0.1, 0.8, 29.9336, 35.69, O.cosmo(p.om, p.h0),
+                                    p.tables, sel)
+    np.testing.assert_allclose(vals, norm, rtol=1e-8)
+    assert m.cleanup() == 0
+
+
+def test_shear_module_and_fast_mass_aliases(gpu):
+    p = synthetic.fiducial()
+    pz, pc = synthetic.plob_baseline()
+    cfg = dict(BINS, zt_low=0.05, zt_high=0.8, lnm_low=29.9336, lnm_high=36.8414,
+               n_lnm=64, n_z=32, n_q=16)
+    mor = [11.4, 12.7, 0.86, 0.0, 0.18, 0.45]
+    lnm, z, S = E.sel_function(cfg, O.MOR_HOD, mor, pz, pc)
+    block = _sample_block(p)
+    block["sel_function", "lnM"] = lnm
+    block["sel_function", "z"] = z
+    block["sel_function", "S_stack"] = S
+    R = np.logspace(-2, 1.7, 40)
+    lnM = np.linspace(29.9, 36.9, 30)
+    block["haloModel", "r_sigma"] = R
+    block["haloModel", "lnM"] = lnM
+    block["haloModel", "dSigma_nfw"] = np.outer(np.exp(0.1 * (lnM - 32)), 1.0 / (R + 0.1))
+    out = {}
+    for name, sec in (("Shear1hMisSel", "shear1hmissel"), ("Shear1hFastMass", "shear1h_fast_mass")):
+        m = Module(name)
+        o = DataBlock()
+        o[name, "bin_index"] = np.arange(12)
+        o[name, "r_perp"] = np.array([0.2, 1.0, 5.0])
+        for k, v in dict(zt_low=0.1, zt_high=0.8, lnm_low=29.9336, lnm_high=36.73).items():
+            o[name, k] = v
+        o[name, "n_lnm"] = 32
+        o[name, "n_z"] = 32
+        assert m.setup(o)
+        assert m.execute(block) == 0
+        out[name] = block[sec, "vals"]
+        assert out[name].shape == (36,)
+        m.cleanup()
+    np.testing.assert_array_equal(out["Shear1hMisSel"], out["Shear1hFastMass"])
+    h = E.SelGL(32, 32, 0.1, 0.8, 29.9336, 36.73)
+    h.build(E.cosmo(p.om, p.h0), p.tables, (lnm, z, S), include_sci=True)
+    halo = dict(r_sigma=R, lnM=lnM, dSigma_nfw=block["haloModel", "dSigma_nfw"])
+    direct = h.shear(np.repeat(np.arange(12), 3), np.tile([0.2, 1.0, 5.0], 12), halo)
+    np.testing.assert_allclose(out["Shear1hMisSel"], direct, rtol=1e-12)
+
+
+def test_module_errors_return_nonzero_status(gpu):
+    m = Module("NumCountsSel")
+    o = DataBlock()
+    o["NumCountsSel", "bin_index"] = np.arange(12)
+    assert not m.setup(o)            # missing zt_low etc. -> NULL, not an exception
+    for k, v in dict(zt_low=0.1, zt_high=0.8, lnm_low=29.9, lnm_high=35.7).items():
+        o["NumCountsSel", k] = v
+    assert m.setup(o)
+    empty = DataBlock()
+    assert m.execute(empty) != 0     # missing sample sections -> non-zero status
+    m.cleanup()

@@ -1,0 +1,276 @@
+"""GPU parity: the CUDA path through the C ABI against the FP64 CPU oracle
+(and the reference's golden vectors).  Tolerances:
+  * FP64 paths (sel_function, SelGL, engine FP64): <= 1e-8 relative (the
+    north-star bar); observed ~1e-13.
+  * mixed engine (FP32 integrands, split-BF16 tcgen05 contraction, FP64
+    final sums): <= 1e-4 relative."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from y3_cluster_cpp_b200 import engine as E
+from y3_cluster_cpp_b200 import prj_params, synthetic
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+TOL64 = 1e-8
+TOLMIX = 1e-4
+
+
+def _cfg(g):
+    cfg = {k: g[k] for k in ("lam_min", "lam_max", "zob_min", "zob_max", "sigma_z")}
+    cfg.update(zt_low=float(g["zt_low"]), zt_high=float(g["zt_high"]),
+               lnm_low=float(g["lnm_low"]), lnm_high=float(g["lnm_high"]),
+               n_lnm=int(g["n_lnm"]), n_z=int(g["n_z_shared"]), n_q=int(g["N_q"]))
+    return cfg
+
+
+@pytest.mark.parametrize("kind", ["hod", "lognormal"])
+def test_sel_function_gpu_matches_golden_and_oracle(gpu, kind):
+    g = np.load(os.path.join(GOLD, f"sel_function_{kind}.npz"))
+    if kind == "hod":
+        mk = O.MOR_HOD
+        mor = [float(g["hod_" + k]) for k in ("log10_Mmin", "log10_M1", "alpha", "epsilon",
+                                              "sigma_lambda")] + [0.45]
+        pz, pc = prj_params.default_table()
+    else:
+        mk = O.MOR_LOGNORMAL
+        mor = [float(g["ln_" + k]) for k in ("A", "B", "C", "sigma", "Mpiv", "lam_lo", "lam_hi")]
+        pz, pc = prj_params.baseline_constant_table()
+    lnm, z, S = E.sel_function(_cfg(g), mk, mor, pz, pc)
+    _, _, So = O.sel_function(_cfg(g), mk, mor, pz, pc)
+    scale = np.max(g["S_stack"])
+    assert np.max(np.abs(S - g["S_stack"])) <= 1e-10 * scale
+    assert np.max(np.abs(S - So)) <= 1e-12 * scale
+    np.testing.assert_allclose(lnm, g["lnM"], atol=1e-12)
+
+
+def test_sel_function_full_size_reference_grid(gpu):
+    """The des_y3.ini production grid (12 bins, 192 lnM x 64 z x 32 lam_t)."""
+    g = np.load(os.path.join(GOLD, "sel_function_hod.npz"))
+    cfg = _cfg(g)
+    cfg.update(n_lnm=192, n_z=64, n_q=32, lnm_high=36.8414)
+    mor = [11.4, 12.7, 0.86, 0.0, 0.18, 0.45]
+    pz, pc = prj_params.default_table()
+    _, _, S = E.sel_function(cfg, O.MOR_HOD, mor, pz, pc)
+    _, _, So = O.sel_function(cfg, O.MOR_HOD, mor, pz, pc)
+    assert np.max(np.abs(S - So)) <= 1e-12 * np.max(So)
+
+
+def _selgl_case(n_lnm=96, n_z=64):
+    p = synthetic.fiducial()
+    g = synthetic.grid(1)
+    pz, pc = synthetic.plob_baseline()
+    cfg = dict(lam_min=np.tile(g["lam_edges"][:-1], 3), lam_max=np.tile(g["lam_edges"][1:], 3),
+               zob_min=np.repeat(g["zob_edges"][:-1], 4),
+               zob_max=np.repeat(g["zob_edges"][1:], 4), sigma_z=np.full(12, 0.0145),
+               zt_low=0.1, zt_high=0.8, lnm_low=g["lnm_lo"], lnm_high=g["lnm_hi"],
+               n_lnm=96, n_z=48, n_q=32)
+    mor = [p.A, p.B, p.C, p.sigma, p.Mpiv, 1.0, 1000.0]
+    sel = O.sel_function(cfg, O.MOR_LOGNORMAL, mor, pz, pc)
+    box = (n_lnm, n_z, 0.1, 0.8, g["lnm_lo"], g["lnm_hi"])
+    return p, sel, box
+
+
+def test_numcounts_selgl_matches_oracle(gpu):
+    p, sel, box = _selgl_case()
+    c = O.cosmo(p.om, p.h0)
+    W, norm, eff, mu2 = O.selgl_weights(*box, c, p.tables, sel)
+    h = E.SelGL(*box)
+    h.build(E.cosmo(p.om, p.h0), p.tables, sel)
+    vals = h.counts(np.arange(12))
+    np.testing.assert_allclose(vals, norm, rtol=TOL64)
+    w = h.weights()
+    np.testing.assert_allclose(w["W"], W, rtol=TOL64, atol=1e-12 * np.max(np.abs(W)))
+    np.testing.assert_allclose(w["lnm_eff"], eff, rtol=1e-12)
+    np.testing.assert_allclose(w["mu2"], mu2, rtol=1e-8)
+    with pytest.raises(E.A.Y3BError):
+        h.counts([12])  # bin_index outside S_stack range
+    h.close()
+
+
+def _halo_table(om):
+    R = np.logspace(-2, 1.7, 40)
+    lnM = np.linspace(np.log(1e13), np.log(10 ** 15.5), 30)
+    rho = 2.77533742639e11 * om
+    ds = np.empty((len(lnM), len(R)))
+    for i, m in enumerate(lnM):
+        c = 5.0 * (np.exp(m) / 1e14) ** -0.1
+        rs = O.lib().y3o_nfw_rs(m, c, rho)
+        nrm = O.lib().y3o_nfw_norm(m, c, rho)
+        ds[i] = [nrm * O.lib().y3o_nfw_dsigma_unit(r / rs) for r in R]
+    return dict(r_sigma=R, lnM=lnM, dSigma_nfw=ds)
+
+
+@pytest.mark.parametrize("idea2", [False, True])
+def test_shear1h_mis_selgl_matches_oracle(gpu, idea2):
+    p, sel, box = _selgl_case(n_lnm=48, n_z=32)
+    c = O.cosmo(p.om, p.h0)
+    W, norm, eff, mu2 = O.selgl_weights(*box, c, p.tables, sel,
+                                        sci=(p.tables["sci_z"], p.tables["sci_val"]))
+    halo = _halo_table(p.om)
+    R = np.array([0.1, 0.4, 1.5, 6.0])
+    h = E.SelGL(*box)
+    h.build(E.cosmo(p.om, p.h0), p.tables, sel, include_sci=True)
+    bins = np.repeat(np.arange(12), len(R))
+    rr = np.tile(R, 12)
+    got = h.shear(bins, rr, halo, n_theta=16, n_s=32, idea2=idea2)
+    x, w = O.gl_nodes(box[4], box[5], box[0])
+    if not idea2:
+        ref = O.shear1h_mis(x, w, W, R, 0.22, 0.17, [25, 37.5, 52.5, 130], p.om, 4.0,
+                            halo["r_sigma"], halo["lnM"], halo["dSigma_nfw"], 16, 32, 20.0)
+        np.testing.assert_allclose(got, ref.ravel(), rtol=TOL64)
+    else:
+        # idea2: norm [phi(eff) + mu2/2 phi''] with a 3-point stencil
+        wts = h.weights()
+        one = np.ones(1)
+        for b in range(12):
+            for r_i, r in enumerate(R):
+                vals = []
+                for dy in (0.0, 0.15, -0.15):
+                    vals.append(O.shear1h_mis(np.array([wts["lnm_eff"][b] + dy]), one,
+                                              np.ones((12, 1)), [r], 0.22, 0.17,
+                                              [25, 37.5, 52.5, 130], p.om, 4.0,
+                                              halo["r_sigma"], halo["lnM"], halo["dSigma_nfw"],
+                                              16, 32, 20.0)[b, 0])
+                d2 = (vals[1] - 2 * vals[0] + vals[2]) / 0.15 ** 2
+                ref = wts["norm"][b] * (vals[0] + 0.5 * wts["mu2"][b] * d2)
+                assert got[b * len(R) + r_i] == pytest.approx(ref, rel=1e-8)
+    h.close()
+
+
+def test_sigma_crit_inv_matches_oracle(gpu):
+    p = synthetic.fiducial()
+    zs, pz = synthetic.source_nz()
+    zl = np.linspace(0.05, 0.85, 64)
+    got = E.sigma_crit_inv(zl, zs, pz, 0.0, p.h0, p.tables["dist_z"], p.tables["dist_da"])
+    ref = O.sigma_crit_inv(zl, zs, pz, 0.0, p.h0, p.tables["dist_z"], p.tables["dist_da"])
+    np.testing.assert_allclose(got, ref, rtol=1e-12)
+    np.testing.assert_allclose(got, p.tables["sci_val"], rtol=1e-10)
+
+
+def test_nfw_mis_matches_oracle_and_kats(gpu):
+    import json
+    kats = json.load(open(os.path.join(GOLD, "kats.json")))
+    for which, fn in (("dsigma", O.dsigma_mis_unit), ("sigma", O.sigma_mis_unit)):
+        d = kats[which + "_mis"]
+        rho = 2.77533742639e11 * 0.3
+        r = np.repeat(d["r"], 3)[:len(d["answers"])]
+        rm = np.tile(d["rmis"], len(d["r"]))[:len(d["answers"])]
+        got = E.nfw_mis(which, r, rm, d["lnM"][0], 4.0, rho)
+        rs = O.lib().y3o_nfw_rs(d["lnM"][0], 4.0, rho)
+        nrm = O.lib().y3o_nfw_norm(d["lnM"][0], 4.0, rho)
+        ref = np.array([nrm * fn(a / rs, b / rs, 64, 128, 20.0) for a, b in zip(r, rm)])
+        np.testing.assert_allclose(got, ref, rtol=1e-10)
+        tol = np.where((rm >= 2.0) & (r >= 5.0) & (which == "sigma"), 1.5e-3, d["epsrel"])
+        assert np.all(np.abs(got / np.array(d["answers"]) - 1) <= tol)
+
+
+# ---------------------------------------------------------------------------
+# Engine (direct nested quadrature, FP64 and mixed)
+
+def _engine(grids, n_max=8, shear=None):
+    p = synthetic.fiducial()
+    t = p.tables
+    pz, pc = synthetic.plob_baseline()
+    return E.Engine(grids, len(t["hmf_m_h"]), len(t["hmf_z"]), len(t["dist_z"]), (pz, pc),
+                    max_points=n_max, n_sci=len(t["sci_z"]), shear=shear)
+
+
+@pytest.mark.parametrize("density", [1, 2, 4])
+def test_engine_counts_match_oracle(gpu, density):
+    g = synthetic.grid(density)
+    eng = _engine([g])
+    p = synthetic.fiducial()
+    pz, pc = synthetic.plob_baseline()
+    ref, Wref, _ = O.direct_eval(g, pz, pc, p.mor, O.cosmo(p.om, p.h0), p.tables)
+    r64 = eng.eval([p], E.FP64, grid_of=lambda _: 0, weights=True)
+    rmx = eng.eval([p], E.MIXED, grid_of=lambda _: 0, weights=True)
+    np.testing.assert_allclose(r64["counts"][0], ref, rtol=TOL64)
+    np.testing.assert_allclose(rmx["counts"][0], ref, rtol=TOLMIX)
+    np.testing.assert_allclose(r64["W"][0], Wref, rtol=TOL64, atol=TOL64 * np.max(Wref))
+    np.testing.assert_allclose(rmx["W"][0], Wref, rtol=0, atol=TOLMIX * np.max(Wref))
+    eng.close()
+
+
+def test_engine_batched_walkers_mixed_densities(gpu):
+    """Uneven grids in one call; each point equals its own evaluation alone
+    (bitwise) and the oracle (tolerance)."""
+    grids = [synthetic.grid(d) for d in (1, 2, 4)]
+    pts = synthetic.walkers(6, seed=1)
+    gi = {1: 0, 2: 1, 4: 2}
+    eng = _engine(grids, n_max=8)
+    pz, pc = synthetic.plob_baseline()
+    for prec, tol in ((E.FP64, TOL64), (E.MIXED, TOLMIX)):
+        batch = eng.eval(pts, prec, grid_of=lambda p: gi[p.density])["counts"]
+        for i, p in enumerate(pts):
+            alone = eng.eval([p], prec, grid_of=lambda q: gi[q.density])["counts"][0]
+            assert np.array_equal(alone, batch[i])
+            ref, _, _ = O.direct_eval(grids[gi[p.density]], pz, pc, p.mor, O.cosmo(p.om, p.h0),
+                                      p.tables)
+            np.testing.assert_allclose(batch[i], ref, rtol=tol)
+    eng.close()
+
+
+def test_engine_reruns_bit_identical(gpu):
+    eng = _engine([synthetic.grid(4)], n_max=4)
+    pts = synthetic.walkers(4, seed=3, densities=(4,))
+    for prec in (E.FP64, E.MIXED):
+        a = eng.eval(pts, prec, grid_of=lambda _: 0)["counts"]
+        b = eng.eval(pts, prec, grid_of=lambda _: 0)["counts"]
+        assert np.array_equal(a, b)
+    eng.close()
+
+
+def test_engine_shear_matches_oracle(gpu):
+    g = synthetic.grid(1, n_m=32)
+    sh = synthetic.shear_opts(n_theta=16, n_s=32, n_R=5)
+    eng = _engine([g], n_max=2, shear=sh)
+    p = synthetic.fiducial()
+    pz, pc = synthetic.plob_baseline()
+    so = dict(sh, sci_z=p.tables["sci_z"], sci_val=p.tables["sci_val"])
+    ref, _, rsh = O.direct_eval(g, pz, pc, p.mor, O.cosmo(p.om, p.h0), p.tables, shear=so)
+    r64 = eng.eval([p], E.FP64, grid_of=lambda _: 0)
+    rmx = eng.eval([p], E.MIXED, grid_of=lambda _: 0)
+    np.testing.assert_allclose(r64["shear"][0], rsh, rtol=TOL64)
+    np.testing.assert_allclose(rmx["shear"][0], rsh, rtol=TOLMIX)
+    np.testing.assert_allclose(r64["counts"][0], ref, rtol=TOL64)
+    eng.close()
+
+
+def test_engine_domain_error_and_recovery(gpu):
+    g = synthetic.grid(1)
+    eng = _engine([g], n_max=2)
+    p = synthetic.fiducial()
+    bad = synthetic.Point(**{k: getattr(p, k) for k in ("om", "sigma8", "h0", "A", "B", "C",
+                                                         "sigma", "Mpiv", "density")})
+    bad.tables = dict(p.tables)
+    bad.tables["dist_z"] = p.tables["dist_z"] * 0.3   # table ends at z = 0.6 < zt_hi
+    with pytest.raises(E.A.Y3BError) as e:
+        eng.eval([bad], E.FP64, grid_of=lambda _: 0)
+    assert e.value.status == 2
+    ok = eng.eval([p], E.MIXED, grid_of=lambda _: 0)["counts"]
+    assert np.all(np.isfinite(ok)) and np.all(ok > 0)
+    eng.close()
+
+
+def test_bounded_wait_reports_timeout(gpu):
+    assert E.selftest_wait_timeout(2000) == 5  # Y3B_ERR_TIMEOUT
+    # the context stays usable
+    assert np.all(np.isfinite(E.nfw_mis("dsigma", [0.5], [0.1], [32.0], 4.0, 8e10)))
+
+
+def test_engine_rejects_bad_arguments(gpu):
+    eng = _engine([synthetic.grid(1)], n_max=2)
+    p = synthetic.fiducial()
+    with pytest.raises(E.A.Y3BError) as e:
+        eng.eval([p, p, p], E.FP64, grid_of=lambda _: 0)    # above max_points
+    assert e.value.status == 1
+    with pytest.raises(E.A.Y3BError):
+        eng.eval([p], E.FP64, grid_of=lambda _: 3)          # no such grid
+    eng.close()
+    with pytest.raises(E.A.Y3BError) as e:
+        E.Engine([synthetic.grid(1, n_z=40)], 100, 50, 200, synthetic.plob_baseline())
+    assert e.value.status == 7

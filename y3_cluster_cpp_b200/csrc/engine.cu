@@ -1,0 +1,926 @@
+// engine.cu -- batched evaluation of the cluster-observable integrals on
+// fixed nested Gauss-Legendre nodes (the fast_mass form of
+// src/models/n_operator_sel_gl_t.hh with the lambda_t / lambda_o / z_o
+// integrals of src/modules/sel_function/sel_function.py done on nodes):
+//
+//   K_i(t,q) = sum_o a_o P(lam_o | lam_t, z_q)           per grid, FP64
+//   K_j(q)   = sum_zo b N(z_o; z_q, sz0 (1 + z_q))       per grid, FP64
+//   S_i(k,q) = sum_t u_t K_i(t,q) phi((l_t - mu_kq)/s) / (s D_kq)
+//   W_ij(k)  = sum_q v_q dV(z_q) Omega(z_q) [Sci(z_q)] K_j(q) n(M_k, z_q) S_i(k,q)
+//   N_ij     = sum_k w_k W_ij(k);   N_ij(R) = sum_k w_k W^g_ij(k) Phi_i(R, k)
+//
+// Two precisions share the per-point prep (FP64 tables, z factors, MOR
+// normalisation D_kq by an erf difference):
+//   * FP64 "plain" form: one exp per (k, q, t) in FP64 (direct_main_kernel).
+//   * mixed form: the lambda_t sum as a split-BF16 tcgen05 GEMM
+//     (mixed_gemm.cu) with FP32 integrands and FP64 final sums.
+// Reductions are fixed-order trees; reruns are bit-identical.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "common.cuh"
+#include "engine_internal.h"
+#include "host_common.h"
+#include "mis_quad.cuh"
+
+namespace y3b {
+
+// ---------------------------------------------------------------------------
+// Per-grid precompute.
+__global__ void
+ki_kernel(int nI, int n_z, int n_t, int n_o, const double* xz, const double* xl,
+          const double* lo_x, const double* lo_w, int n_plob, const double* plob_z,
+          const double* plob_coef, double* Ki)
+{
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nI * n_z * n_t) return;
+  const int t = idx % n_t, q = (idx / n_t) % n_z, i = idx / (n_t * n_z);
+  const double lam = exp(xl[t]);
+  double mu, sg, tau, fp;
+  plob_params(n_plob, plob_z, plob_coef, lam, xz[q], &mu, &sg, &tau, &fp);
+  double acc = 0.0;
+  for (int o = 0; o < n_o; ++o)
+    acc += lo_w[i * n_o + o] * pdf_lob(lo_x[i * n_o + o], mu, sg, tau, fp);
+  Ki[idx] = acc;
+}
+
+__global__ void
+uk_kernel(int nI, int n_z, int n_t, int n_t_pad, const double* wl, const double* Ki, float* UK)
+{
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nI * n_z * n_t_pad) return;
+  const int t = idx % n_t_pad, iq = idx / n_t_pad;
+  UK[idx] = t < n_t ? (float)(wl[t] * Ki[(size_t)iq * n_t + t]) : 0.f;
+}
+
+__global__ void
+kj_kernel(int nJ, int n_z, int n_zo, double sz0, const double* xz, const double* zo_x,
+          const double* zo_w, double* Kj, double* omz)
+{
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nJ * n_z) return;
+  const int q = idx % n_z, j = idx / n_z;
+  const double z = xz[q], sz = sz0 * (1.0 + z);
+  double acc = 0.0;
+  for (int o = 0; o < n_zo; ++o) {
+    double d = (zo_x[j * n_zo + o] - z) / sz;
+    acc += zo_w[j * n_zo + o] * exp(-0.5 * d * d) / (kSqrt2Pi * sz);
+  }
+  Kj[idx] = acc;
+  if (j == 0) omz[q] = omega_z_des(z);
+}
+
+// ---------------------------------------------------------------------------
+// Per-point prep.  One CTA per point.  The point's packed tables are staged
+// into shared memory with one bulk (TMA) copy completing on an mbarrier.
+__device__ __forceinline__ uint32_t
+smem_addr(const void* p)
+{
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+struct PrepArgs {
+  const GridDev* grids;
+  const PointDev* pts;
+  const double* tables;
+  TableLayout lay;
+  int mixed;
+  double* s64;
+  float* s32;
+  int* status;
+};
+
+__global__ void __launch_bounds__(256)
+prep_kernel(PrepArgs a)
+{
+  extern __shared__ __align__(16) double psh[];
+  const int p = blockIdx.x;
+  const PointDev pt = a.pts[p];
+  const GridDev& G = a.grids[pt.grid];
+  const int n_m = G.n_m, n_z = G.n_z, tid = threadIdx.x;
+  const TableLayout& L = a.lay;
+
+  double* tab = psh;                                   // [stride]
+  double* ka = tab + L.stride;                         // alpha_k       [n_m]
+  double* kt = ka + n_m;                               // hmf x weight  [n_m]
+  double* kf = kt + n_m;                               // (s, q) factor [n_m]
+  int* kx = reinterpret_cast<int*>(kf + n_m);          // hmf x cell    [n_m]
+  double* qb = reinterpret_cast<double*>(kx + ((n_m + 1) & ~1));  // beta_q [n_z]
+  double* qu = qb + n_z;                               // hmf y weight  [n_z]
+  double* qc = qu + n_z;                               // cz            [n_z]
+  double* qs = qc + n_z;                               // czs           [n_z]
+  int* qy = reinterpret_cast<int*>(qs + n_z);          // hmf y cell    [n_z]
+  double* red = reinterpret_cast<double*>(qy + ((n_z + 1) & ~1));  // [8]
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int timed_out;
+
+  // Bulk copy of this point's table block (16-byte aligned, multiple of 16).
+  const double* src = a.tables + (size_t)p * L.stride;
+  const uint32_t bytes = (uint32_t)(L.stride * sizeof(double));
+  if (tid == 0) {
+    timed_out = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar)),
+                 "r"(bytes)
+                 : "memory");
+    asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+        "r"(smem_addr(tab)),
+      "l"(src), "r"(bytes), "r"(smem_addr(&bar))
+      : "memory");
+  }
+  {
+    long long t0 = clock64();
+    uint32_t ok = 0;
+    while (!ok) {
+      asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(&bar))
+        : "memory");
+      if (!ok && clock64() - t0 > 2000000000LL) {
+        timed_out = 1;
+        break;
+      }
+    }
+  }
+  __syncthreads();
+  if (timed_out) {  // uniform exit; the copy only targets this CTA's shared memory
+    if (tid == 0) set_err(a.status, kDevTimeout);
+    return;
+  }
+  double* mh = tab + L.off[0];
+  const double* hz = tab + L.off[1];
+  const double* dn = tab + L.off[2];
+  const double* dz = tab + L.off[3];
+  const double* da = tab + L.off[4];
+  const double* sz = tab + L.off[5];
+  const double* sv = tab + L.off[6];
+  // HMF mass axis ln(m_h (Omega_M - Omega_nu)) (hmf_t.hh:15-25), in place.
+  for (int i = tid; i < L.n_hm; i += blockDim.x) mh[i] = log(mh[i] * (pt.om - pt.onu));
+  __syncthreads();
+  const double lnMpiv = log(pt.Mpiv);
+  for (int k = tid; k < n_m; k += blockDim.x) {
+    const double x = G.xm[k];
+    ka[k] = pt.B * (x - lnMpiv);
+    const double xx = fmin(fmax(x, mh[0]), mh[L.n_hm - 1]);
+    const int xi = bsearch_cell(mh, L.n_hm, xx);
+    kx[k] = xi;
+    kt[k] = (xx - mh[xi]) / (mh[xi + 1] - mh[xi]);
+    kf[k] = pt.hmf_s * (x * kLog10e - kHmfPivot) + pt.hmf_q;
+  }
+  for (int q = tid; q < n_z; q += blockDim.x) {
+    const double z = G.xz[q];
+    qb[q] = pt.A + pt.C * log1p(z);
+    const double zz = fmin(fmax(z, hz[0]), hz[L.n_hz - 1]);
+    const int yi = bsearch_cell(hz, L.n_hz, zz);
+    qy[q] = yi;
+    qu[q] = (zz - hz[yi]) / (hz[yi + 1] - hz[yi]);
+    double dv;
+    if (!dv_do_dz(dz, da, L.n_dist, pt.om, pt.ol, pt.ok, pt.h0, z, &dv)) {
+      set_err(a.status, kDevDomain);
+      dv = 0.0;
+    }
+    const double cz = G.wz[q] * dv * G.omz[q];
+    qc[q] = cz;
+    qs[q] = cz * (L.n_sci > 1 ? interp1d_clamp(sz, sv, L.n_sci, z) : 1.0);
+  }
+  __syncthreads();
+  if (tid == 0) {  // centres of the alpha and beta ranges (serial, n <= 1024)
+    double amin = ka[0], amax = ka[0], bmin = qb[0], bmax = qb[0];
+    for (int k = 1; k < n_m; ++k) {
+      amin = fmin(amin, ka[k]);
+      amax = fmax(amax, ka[k]);
+    }
+    for (int q = 1; q < n_z; ++q) {
+      bmin = fmin(bmin, qb[q]);
+      bmax = fmax(bmax, qb[q]);
+    }
+    red[0] = 0.5 * (amin + amax);
+    red[1] = 0.5 * (bmin + bmax);
+  }
+  __syncthreads();
+  const double A0 = red[0], B0 = red[1];
+  const double sig = pt.sigma, inv2s2 = 0.5 / (sig * sig);
+  const double norm0 = 1.0 / (kSqrt2Pi * sig);
+  double* s64 = a.s64 + (size_t)p * G.s64_stride;
+  float* s32 = a.s32 + (size_t)p * G.s32_stride;
+  for (int q = tid; q < n_z; q += blockDim.x) {
+    s64[G.o_cz + q] = qc[q];
+    s64[G.o_czs + q] = qs[q];
+    s64[G.o_beta + q] = qb[q];
+  }
+  for (int k = tid; k < n_m; k += blockDim.x) s64[G.o_alpha + k] = ka[k];
+  // (k, q) products: HMF bilinear (separable cells), D_kq, and the form's
+  // per-(k, q) factor.
+  for (int idx = tid; idx < n_m * n_z; idx += blockDim.x) {
+    const int q = idx / n_m, k = idx % n_m;
+    const double t = kt[k], u = qu[q];
+    const double* r0 = dn + (size_t)qy[q] * L.n_hm + kx[k];
+    const double* r1 = r0 + L.n_hm;
+    const double n = ((1.0 - t) * (1.0 - u) * r0[0] + t * (1.0 - u) * r0[1] +
+                      (1.0 - t) * u * r1[0] + t * u * r1[1]) *
+                     kf[k];
+    const double mu = ka[k] + qb[q];
+    const double D = phi_diff((G.ll_lo - mu) / sig, (G.ll_hi - mu) / sig);
+    if (!a.mixed) {
+      s64[G.o_P0 + idx] = n * norm0 / D;
+    } else {
+      const double aa = ka[k] - A0, bb = qb[q] - B0;
+      const double H = exp(-(2.0 * aa * bb + bb * bb) * inv2s2);
+      s32[G.f_Yt + (size_t)q * G.n_m_pad + k] = (float)(n * H * norm0 / D);
+    }
+  }
+  if (a.mixed) {
+    const double L0 = A0 + B0;
+    for (int k = tid; k < G.n_m_pad; k += blockDim.x) {
+      s32[G.f_a + k] = k < n_m ? (float)(ka[k] - A0) : 0.f;
+      if (k >= n_m)
+        for (int q = 0; q < n_z; ++q) s32[G.f_Yt + (size_t)q * G.n_m_pad + k] = 0.f;
+    }
+    for (int q = tid; q < n_z; q += blockDim.x) {
+      s32[G.f_b + q] = (float)(qb[q] - B0);
+      for (int j = 0; j < G.nJ; ++j) {
+        s32[G.f_CN + j * n_z + q] = (float)(qc[q] * G.Kj[j * n_z + q]);
+        s32[G.f_CG + j * n_z + q] = (float)(qs[q] * G.Kj[j * n_z + q]);
+      }
+    }
+    for (int t = tid; t < G.n_t_pad; t += blockDim.x)
+      s32[G.f_delta + t] = t < G.n_t ? (float)(G.xl[t] - L0) : 0.f;
+    if (tid == 0) {
+      const double log2e = 1.4426950408889634;
+      s32[G.f_scal] = (float)(log2e * inv2s2);      // c1: F = exp2(-(d - a)^2 c1)
+      s32[G.f_scal + 1] = (float)(log2e / (sig * sig));  // c2: G = exp2(d b c2)
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 plain form.  CTA = (z node q, point); thread k sums over lam_t with one
+// FP64 exp per node: V_i(q, k) = P0_kq sum_t u_t K_i(t, q) exp(-(l_t - mu)^2/2s^2).
+__global__ void __launch_bounds__(256)
+direct_main_kernel(const GridDev* grids, const PointDev* pts, double* s64all, int grid_mask)
+{
+  extern __shared__ double dsh[];
+  const int p = blockIdx.y, q = blockIdx.x;
+  const PointDev pt = pts[p];
+  if (!((grid_mask >> pt.grid) & 1)) return;
+  const GridDev& G = grids[pt.grid];
+  if (q >= G.n_z) return;
+  const int n_t = G.n_t, nI = G.nI;
+  double* wk = dsh;                 // [nI][n_t] = u_t K_i(t, q)
+  double* xl = dsh + nI * n_t;      // [n_t]
+  for (int u = threadIdx.x; u < nI * n_t; u += blockDim.x) {
+    const int i = u / n_t, t = u % n_t;
+    wk[u] = G.wl[t] * G.Ki[((size_t)i * G.n_z + q) * n_t + t];
+  }
+  for (int t = threadIdx.x; t < n_t; t += blockDim.x) xl[t] = G.xl[t];
+  __syncthreads();
+  double* s64 = s64all + (size_t)p * G.s64_stride;
+  const double beta = s64[G.o_beta + q];
+  const double inv2s2 = 0.5 / (pt.sigma * pt.sigma);
+  for (int k = threadIdx.x; k < G.n_m; k += blockDim.x) {
+    const double mu = s64[G.o_alpha + k] + beta;
+    double S[kMaxLamBins];
+    for (int i = 0; i < nI; ++i) S[i] = 0.0;
+    for (int t = 0; t < n_t; ++t) {
+      const double d = xl[t] - mu;
+      const double e = exp(-d * d * inv2s2);
+      for (int i = 0; i < nI; ++i) S[i] += wk[i * n_t + t] * e;
+    }
+    const double P0 = s64[G.o_P0 + (size_t)q * G.n_m + k];
+    for (int i = 0; i < nI; ++i) s64[G.o_V + ((size_t)i * G.n_z + q) * G.n_m + k] = P0 * S[i];
+  }
+}
+
+// W_ij(k) = sum_q cz_q K_j(q) V_i(q, k) (and the Sigma_crit-weighted W^g),
+// fixed order over q.  CTA per point.
+__global__ void __launch_bounds__(256)
+direct_wreduce_kernel(const GridDev* grids, const PointDev* pts, const double* s64all,
+                      double* W, double* Wg, int w_stride, int grid_mask)
+{
+  const int p = blockIdx.x;
+  const PointDev pt = pts[p];
+  if (!((grid_mask >> pt.grid) & 1)) return;
+  const GridDev& G = grids[pt.grid];
+  const double* s64 = s64all + (size_t)p * G.s64_stride;
+  for (int k = threadIdx.x; k < G.n_m; k += blockDim.x) {
+    for (int i = 0; i < G.nI; ++i) {
+      double acc[kMaxZBins], accg[kMaxZBins];
+      for (int j = 0; j < G.nJ; ++j) acc[j] = accg[j] = 0.0;
+      for (int q = 0; q < G.n_z; ++q) {
+        const double v = s64[G.o_V + ((size_t)i * G.n_z + q) * G.n_m + k];
+        const double c = s64[G.o_cz + q], cs = s64[G.o_czs + q];
+        for (int j = 0; j < G.nJ; ++j) {
+          const double kj = G.Kj[j * G.n_z + q];
+          acc[j] += c * kj * v;
+          accg[j] += cs * kj * v;
+        }
+      }
+      for (int j = 0; j < G.nJ; ++j) {
+        const size_t o = ((size_t)p * G.nB + i + G.nI * j) * w_stride + k;
+        W[o] = acc[j];
+        Wg[o] = accg[j];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stacked miscentred profile Phi_i(R, k) = norm_k [(1 - f) DSigma(R / r_s)
+// + f DSigma_mis(R / r_s, tau R_lambda(lam_i) / r_s)], c(M) = c0 (M/Mp)^s,
+// rho = Omega_m rho_crit.  One warp per (point, i, R, k).
+template <typename T>
+__global__ void __launch_bounds__(128)
+shear_phi_kernel(const GridDev* grids, const PointDev* pts, int n_points, int w_stride,
+                 ShearDev sh, MisQuad quad, double* Phi, int nI_max, int grid_mask)
+{
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const long long per_point = (long long)nI_max * sh.n_R * w_stride;
+  if (w >= per_point * n_points) return;
+  const int p = (int)(w / per_point);
+  long long r = w % per_point;
+  const int k = (int)(r % w_stride);
+  r /= w_stride;
+  const int iR = (int)(r % sh.n_R);
+  const int i = (int)(r / sh.n_R);
+  const PointDev pt = pts[p];
+  if (!((grid_mask >> pt.grid) & 1)) return;
+  const GridDev& G = grids[pt.grid];
+  if (i >= G.nI || k >= G.n_m) return;
+  const double lnM = G.xm[k];
+  const double c = sh.c0 * pow(exp(lnM) / sh.c_pivot, sh.c_slope);
+  const double rho = kRhoCrit * pt.om;
+  const double rs = nfw_rs(lnM, c, rho);
+  const double rmis = sh.tau_mis * pow(sh.lob[i] / 100.0, 0.2);
+  const double R = sh.R[iR];
+  T mis = mis_partial<T>(quad, (T)(R / rs), (T)(rmis / rs), true, lane);
+  mis = warp_sum(mis);
+  if (lane == 0) {
+    const double cen = (double)NfwUnit<T>::dsigma((T)(R / rs));
+    Phi[(((size_t)p * nI_max + i) * sh.n_R + iR) * w_stride + k] =
+      nfw_norm(lnM, c, rho) * ((1.0 - sh.f_mis) * cen + sh.f_mis * (double)mis);
+  }
+}
+
+// N_b = sum_k w_k W_b(k); N_b(R) = sum_k w_k W^g_b(k) Phi_i(R, k).  CTA per
+// point, warp per output, fixed xor-tree order.
+__global__ void __launch_bounds__(256)
+finalize_kernel(const GridDev* grids, const PointDev* pts, const double* W, const double* Wg,
+                const double* Phi, int w_stride, int nB_max, int nI_max, int n_R,
+                double* counts, double* shear, int grid_mask)
+{
+  const int p = blockIdx.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const PointDev pt = pts[p];
+  if (!((grid_mask >> pt.grid) & 1)) return;
+  const GridDev& G = grids[pt.grid];
+  const int nw = blockDim.x >> 5;
+  for (int b = warp; b < G.nB; b += nw) {
+    const double* Wb = W + ((size_t)p * G.nB + b) * w_stride;
+    double acc = 0.0;
+    for (int k = lane; k < G.n_m; k += 32) acc += G.wm[k] * Wb[k];
+    acc = warp_sum(acc);
+    if (lane == 0) counts[(size_t)p * nB_max + b] = acc;
+  }
+  if (shear && Phi) {
+    for (int u = warp; u < G.nB * n_R; u += nw) {
+      const int b = u / n_R, iR = u % n_R, i = b % G.nI;
+      const double* Wb = Wg + ((size_t)p * G.nB + b) * w_stride;
+      const double* ph = Phi + (((size_t)p * nI_max + i) * n_R + iR) * w_stride;
+      double acc = 0.0;
+      for (int k = lane; k < G.n_m; k += 32) acc += G.wm[k] * Wb[k] * ph[k];
+      acc = warp_sum(acc);
+      if (lane == 0) shear[((size_t)p * nB_max + b) * n_R + iR] = acc;
+    }
+  }
+}
+
+int gl_nodes_device(double a, double b, int n, double* xs, double* ws, cudaStream_t s);
+
+struct GridBufs {
+  DevBuf<double> xm, wm, xz, wz, xl, wl, lo_x, lo_w, zo_x, zo_w, Ki, Kj, omz;
+  DevBuf<float> UK;
+};
+
+}  // namespace y3b
+
+struct y3b_engine {
+  y3b_engine_config cfg;
+  std::vector<double> plob_z, plob_coef;
+  std::vector<y3b_grid> grids_in;
+  std::vector<y3b::GridDev> grids;
+  std::vector<y3b::GridBufs*> gbufs;
+  y3b::DevBuf<y3b::GridDev> d_grids;
+  y3b::TableLayout lay;
+  y3b::ShearDev shear;
+  y3b::MisQuadCache quad;
+  cudaStream_t stream = nullptr;
+  y3b::DevBuf<y3b::PointDev> pts;
+  y3b::DevBuf<double> tables, s64, W, Wg, Phi, counts, shear_out;
+  y3b::DevBuf<float> s32;
+  y3b::DevBuf<int> status;
+  size_t s64_stride = 0, s32_stride = 0;
+  int w_stride = 0, nB_max = 0, nI_max = 0, nz_max = 0, nt_max = 0;
+  size_t prep_smem = 0, direct_smem = 0;
+  size_t device_bytes = 0;
+  int last_n = 0;
+  ~y3b_engine()
+  {
+    for (auto* g : gbufs) delete g;
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace y3b {
+
+static size_t
+pad2(size_t n)
+{
+  return (n + 1) & ~size_t(1);
+}
+
+static int
+build_grid(y3b_engine* e, int gi)
+{
+  const y3b_grid& in = e->grids_in[gi];
+  GridDev g{};
+  GridBufs* b = e->gbufs[gi];
+  cudaStream_t s = e->stream;
+  g.n_m = in.n_m;
+  g.n_z = in.n_z;
+  g.n_t = in.n_t;
+  g.n_o = in.n_o;
+  g.n_zo = in.n_zo;
+  g.nI = in.n_lam_bins;
+  g.nJ = in.n_z_bins;
+  g.nB = g.nI * g.nJ;
+  g.n_m_pad = (g.n_m + kGemmRows - 1) / kGemmRows * kGemmRows;
+  g.n_t_pad = (g.n_t + kKChunk - 1) / kKChunk * kKChunk;
+  g.n_cols = g.nI * g.n_z;
+  g.n_cols_pad = (g.n_cols + 15) / 16 * 16;
+  g.lnm_lo = in.lnm_lo;
+  g.lnm_hi = in.lnm_hi;
+  g.zt_lo = in.zt_lo;
+  g.zt_hi = in.zt_hi;
+  g.ll_lo = std::log(in.lam_t_lo);
+  g.ll_hi = std::log(in.lam_t_hi);
+  g.sz0 = in.sz0;
+  Y3B_TRY(b->xm.alloc(g.n_m));
+  Y3B_TRY(b->wm.alloc(g.n_m));
+  Y3B_TRY(b->xz.alloc(g.n_z));
+  Y3B_TRY(b->wz.alloc(g.n_z));
+  Y3B_TRY(b->xl.alloc(g.n_t));
+  Y3B_TRY(b->wl.alloc(g.n_t));
+  Y3B_TRY(b->lo_x.alloc((size_t)g.n_o * g.nI));
+  Y3B_TRY(b->lo_w.alloc((size_t)g.n_o * g.nI));
+  Y3B_TRY(b->zo_x.alloc((size_t)g.n_zo * g.nJ));
+  Y3B_TRY(b->zo_w.alloc((size_t)g.n_zo * g.nJ));
+  Y3B_TRY(b->Ki.alloc((size_t)g.nI * g.n_z * g.n_t));
+  Y3B_TRY(b->UK.alloc((size_t)g.nI * g.n_z * g.n_t_pad));
+  Y3B_TRY(b->Kj.alloc((size_t)g.nJ * g.n_z));
+  Y3B_TRY(b->omz.alloc(g.n_z));
+  Y3B_TRY(gl_nodes_device(in.lnm_lo, in.lnm_hi, g.n_m, b->xm.get(), b->wm.get(), s));
+  Y3B_TRY(gl_nodes_device(in.zt_lo, in.zt_hi, g.n_z, b->xz.get(), b->wz.get(), s));
+  Y3B_TRY(gl_nodes_device(g.ll_lo, g.ll_hi, g.n_t, b->xl.get(), b->wl.get(), s));
+  for (int i = 0; i < g.nI; ++i)
+    Y3B_TRY(gl_nodes_device(in.lam_edges[i], in.lam_edges[i + 1], g.n_o, b->lo_x.get() + i * g.n_o,
+                            b->lo_w.get() + i * g.n_o, s));
+  for (int j = 0; j < g.nJ; ++j)
+    Y3B_TRY(gl_nodes_device(in.zob_edges[j], in.zob_edges[j + 1], g.n_zo,
+                            b->zo_x.get() + j * g.n_zo, b->zo_w.get() + j * g.n_zo, s));
+  DevBuf<double> pz, pc;
+  Y3B_TRY(pz.upload(e->plob_z.data(), e->plob_z.size(), s));
+  Y3B_TRY(pc.upload(e->plob_coef.data(), e->plob_coef.size(), s));
+  int nki = g.nI * g.n_z * g.n_t;
+  ki_kernel<<<(nki + 127) / 128, 128, 0, s>>>(g.nI, g.n_z, g.n_t, g.n_o, b->xz.get(), b->xl.get(),
+                                             b->lo_x.get(), b->lo_w.get(), (int)e->plob_z.size(),
+                                             pz.get(), pc.get(), b->Ki.get());
+  count_launch();
+  Y3B_CUDA(cudaGetLastError());
+  int nuk = g.nI * g.n_z * g.n_t_pad;
+  uk_kernel<<<(nuk + 255) / 256, 256, 0, s>>>(g.nI, g.n_z, g.n_t, g.n_t_pad, b->wl.get(),
+                                             b->Ki.get(), b->UK.get());
+  count_launch();
+  Y3B_CUDA(cudaGetLastError());
+  int nkj = g.nJ * g.n_z;
+  kj_kernel<<<(nkj + 127) / 128, 128, 0, s>>>(g.nJ, g.n_z, g.n_zo, g.sz0, b->xz.get(),
+                                             b->zo_x.get(), b->zo_w.get(), b->Kj.get(),
+                                             b->omz.get());
+  count_launch();
+  Y3B_CUDA(cudaGetLastError());
+  Y3B_CUDA(cudaStreamSynchronize(s));  // pz/pc are freed on return
+  g.xm = b->xm.get();
+  g.wm = b->wm.get();
+  g.xz = b->xz.get();
+  g.wz = b->wz.get();
+  g.xl = b->xl.get();
+  g.wl = b->wl.get();
+  g.Ki = b->Ki.get();
+  g.UK = b->UK.get();
+  g.Kj = b->Kj.get();
+  g.omz = b->omz.get();
+  // Scratch layouts.
+  size_t o = 0;
+  g.o_cz = o;
+  o += pad2(g.n_z);
+  g.o_czs = o;
+  o += pad2(g.n_z);
+  g.o_alpha = o;
+  o += pad2(g.n_m);
+  g.o_beta = o;
+  o += pad2(g.n_z);
+  g.o_P0 = o;
+  o += pad2((size_t)g.n_z * g.n_m);
+  g.o_V = o;
+  o += pad2((size_t)g.nI * g.n_z * g.n_m);
+  g.s64_stride = o;
+  size_t f = 0;
+  g.f_a = f;
+  f += g.n_m_pad;
+  g.f_b = f;
+  f += (g.n_z + 3) & ~3;
+  g.f_delta = f;
+  f += g.n_t_pad;
+  g.f_scal = f;
+  f += 4;
+  g.f_Yt = f;
+  f += (size_t)g.n_z * g.n_m_pad;
+  g.f_CN = f;
+  f += (size_t)g.nJ * g.n_z;
+  g.f_CG = f;
+  f += (size_t)g.nJ * g.n_z;
+  g.s32_stride = (f + 3) & ~size_t(3);
+  e->grids[gi] = g;
+  return Y3B_OK;
+}
+
+static int
+validate_grid(const y3b_grid& g)
+{
+  if (g.n_m < 2 || g.n_z < 2 || g.n_t < 2 || g.n_o < 1 || g.n_zo < 1 || g.n_lam_bins < 1 ||
+      g.n_z_bins < 1 || g.n_lam_bins > kMaxLamBins || g.n_z_bins > kMaxZBins) {
+    set_error("y3b_engine_create: grid needs n >= 2 nodes per axis and 1..8 bins per axis");
+    return Y3B_ERR_INVALID;
+  }
+  if (g.n_m > 1024 || g.n_z % 16 != 0 || g.n_lam_bins * g.n_z > kMaxCols || g.n_t > 4096) {
+    set_error("y3b_engine_create: unsupported grid (n_m <= 1024, n_z a multiple of 16, "
+              "n_lam_bins * n_z <= 512, n_t <= 4096)");
+    return Y3B_ERR_UNSUPPORTED;
+  }
+  if (!(g.lnm_hi > g.lnm_lo) || !(g.zt_hi > g.zt_lo) || !(g.lam_t_lo > 0.0) ||
+      !(g.lam_t_hi > g.lam_t_lo) || !(g.sz0 > 0.0)) {
+    set_error("y3b_engine_create: grid bounds must be ordered and positive");
+    return Y3B_ERR_INVALID;
+  }
+  for (int i = 0; i < g.n_lam_bins; ++i)
+    if (!(g.lam_edges[i + 1] > g.lam_edges[i])) {
+      set_error("y3b_engine_create: lam_edges must increase");
+      return Y3B_ERR_INVALID;
+    }
+  for (int j = 0; j < g.n_z_bins; ++j)
+    if (!(g.zob_edges[j + 1] > g.zob_edges[j])) {
+      set_error("y3b_engine_create: zob_edges must increase");
+      return Y3B_ERR_INVALID;
+    }
+  return Y3B_OK;
+}
+
+}  // namespace y3b
+
+using namespace y3b;
+
+extern "C" void
+y3b_engine_destroy(y3b_engine* e)
+{
+  delete e;
+}
+
+extern "C" int
+y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* cfg,
+                  y3b_engine** out)
+{
+  clear_error();
+  if (!grids || !cfg || !out || n_grids < 1 || n_grids > 31) {
+    set_error("y3b_engine_create: need 1..31 grids, a config and an output handle");
+    return Y3B_ERR_INVALID;
+  }
+  *out = nullptr;
+  for (int g = 0; g < n_grids; ++g) {
+    Y3B_TRY(validate_grid(grids[g]));
+    if (grids[g].n_lam_bins != grids[0].n_lam_bins || grids[g].n_z_bins != grids[0].n_z_bins) {
+      set_error("y3b_engine_create: all grids must share the bin layout");
+      return Y3B_ERR_INVALID;
+    }
+  }
+  if (cfg->n_hm < 2 || cfg->n_hz < 2 || cfg->n_dist < 2 || cfg->max_points < 1 ||
+      cfg->plob.n < 1 || !cfg->plob.z || !cfg->plob.coef ||
+      (cfg->with_shear && (cfg->n_sci < 2 || cfg->shear.n_R < 1 || cfg->shear.n_R > kMaxR))) {
+    set_error("y3b_engine_create: invalid table shapes, capacity, P(lam_o|lam_t) table or "
+              "shear options (n_sci >= 2 and 1 <= n_R <= 32 with shear)");
+    return Y3B_ERR_INVALID;
+  }
+  Y3B_TRY(require_device());
+  y3b_engine* e = new (std::nothrow) y3b_engine();
+  if (!e) {
+    set_error("y3b_engine_create: out of host memory");
+    return Y3B_ERR_NOMEM;
+  }
+  auto fail = [&](int rc) {
+    delete e;
+    return rc;
+  };
+  e->cfg = *cfg;
+  e->plob_z.assign(cfg->plob.z, cfg->plob.z + cfg->plob.n);
+  e->plob_coef.assign(cfg->plob.coef, cfg->plob.coef + 8 * (size_t)cfg->plob.n);
+  e->cfg.plob.z = e->plob_z.data();
+  e->cfg.plob.coef = e->plob_coef.data();
+  e->grids_in.assign(grids, grids + n_grids);
+  e->grids.resize(n_grids);
+  for (int g = 0; g < n_grids; ++g) e->gbufs.push_back(new (std::nothrow) GridBufs());
+  int rc = cuda_status(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking),
+                       "cudaStreamCreate");
+  if (rc) return fail(rc);
+  for (int g = 0; g < n_grids; ++g) {
+    rc = build_grid(e, g);
+    if (rc) return fail(rc);
+  }
+  // Table layout: each section 16-byte aligned.
+  TableLayout& L = e->lay;
+  L.n_hm = cfg->n_hm;
+  L.n_hz = cfg->n_hz;
+  L.n_dist = cfg->n_dist;
+  L.n_sci = cfg->n_sci;
+  size_t sizes[7] = {(size_t)cfg->n_hm,   (size_t)cfg->n_hz,   (size_t)cfg->n_hz * cfg->n_hm,
+                     (size_t)cfg->n_dist, (size_t)cfg->n_dist, (size_t)cfg->n_sci,
+                     (size_t)cfg->n_sci};
+  size_t o = 0;
+  for (int i = 0; i < 7; ++i) {
+    L.off[i] = o;
+    o += pad2(sizes[i]);
+  }
+  L.stride = o;
+  for (const auto& g : e->grids) {
+    e->s64_stride = std::max(e->s64_stride, g.s64_stride);
+    e->s32_stride = std::max(e->s32_stride, g.s32_stride);
+    e->w_stride = std::max(e->w_stride, g.n_m);
+    e->nB_max = std::max(e->nB_max, g.nB);
+    e->nI_max = std::max(e->nI_max, g.nI);
+    e->nz_max = std::max(e->nz_max, g.n_z);
+    e->nt_max = std::max(e->nt_max, g.n_t);
+  }
+  // Every grid uses the engine-wide strides (offsets are within a block).
+  for (auto& g : e->grids) {
+    g.s64_stride = e->s64_stride;
+    g.s32_stride = e->s32_stride;
+  }
+  int nm_max = e->w_stride, nz_max = e->nz_max;
+  e->prep_smem = L.stride * 8 + (3 * nm_max + 4 * nz_max) * 8 + ((nm_max + 1) & ~1) * 4 +
+                 ((nz_max + 1) & ~1) * 4 + 8 * 8 + 64;
+  e->direct_smem = ((size_t)e->nI_max * e->nt_max + e->nt_max) * 8;
+  if (e->prep_smem > 200 * 1024 || e->direct_smem > 200 * 1024) {
+    set_error("y3b_engine_create: per-point tables too large for shared-memory staging");
+    return fail(Y3B_ERR_UNSUPPORTED);
+  }
+  for (int g = 0; g < n_grids; ++g) {
+    const GridDev& gd = e->grids[g];
+    if (mixed_gemm_smem_bytes(gd.n_cols_pad, gd.n_z, gd.n_t_pad, gd.nJ) > 227 * 1024) {
+      set_error("y3b_engine_create: grid %d needs more shared memory than one CTA has", g);
+      return fail(Y3B_ERR_UNSUPPORTED);
+    }
+  }
+  // Shear options.
+  ShearDev& sh = e->shear;
+  std::memset(&sh, 0, sizeof(sh));
+  if (cfg->with_shear) {
+    sh.n_R = cfg->shear.n_R;
+    for (int r = 0; r < sh.n_R; ++r) sh.R[r] = cfg->shear.R[r];
+    sh.f_mis = cfg->shear.f_mis;
+    sh.tau_mis = cfg->shear.tau_mis;
+    for (int i = 0; i < kMaxLamBins; ++i) sh.lob[i] = cfg->shear.lob_centers[i];
+    sh.c0 = cfg->shear.c0;
+    sh.c_slope = cfg->shear.c_slope;
+    sh.c_pivot = cfg->shear.c_pivot;
+    rc = e->quad.ensure(cfg->shear.n_theta, cfg->shear.n_s, cfg->shear.s_max, e->stream);
+    if (rc) return fail(rc);
+  }
+  // Device memory against the HBM budget.
+  const size_t N = cfg->max_points;
+  size_t bytes = N * sizeof(PointDev) + N * L.stride * 8 + N * e->s64_stride * 8 +
+                 N * e->s32_stride * 4 + 2 * N * e->nB_max * (size_t)e->w_stride * 8 +
+                 N * e->nB_max * 8;
+  if (cfg->with_shear)
+    bytes += N * (size_t)e->nI_max * sh.n_R * e->w_stride * 8 + N * e->nB_max * sh.n_R * 8;
+  const size_t budget = cfg->hbm_budget ? cfg->hbm_budget : (size_t)150 << 30;
+  if (bytes > budget) {
+    set_error("y3b_engine_create: %zu bytes for %d points exceed the HBM budget of %zu bytes",
+              bytes, cfg->max_points, budget);
+    return fail(Y3B_ERR_BUDGET);
+  }
+  e->device_bytes = bytes;
+  if ((rc = e->pts.alloc(N)) || (rc = e->tables.alloc(N * L.stride)) ||
+      (rc = e->s64.alloc(N * e->s64_stride)) || (rc = e->s32.alloc(N * e->s32_stride)) ||
+      (rc = e->W.alloc(N * e->nB_max * (size_t)e->w_stride)) ||
+      (rc = e->Wg.alloc(N * e->nB_max * (size_t)e->w_stride)) ||
+      (rc = e->counts.alloc(N * e->nB_max)) || (rc = e->status.alloc(1)))
+    return fail(rc);
+  if (cfg->with_shear) {
+    if ((rc = e->Phi.alloc(N * (size_t)e->nI_max * sh.n_R * e->w_stride)) ||
+        (rc = e->shear_out.alloc(N * e->nB_max * (size_t)sh.n_R)))
+      return fail(rc);
+  }
+  // Zero the weight buffers once: rows a grid does not fill stay zero.
+  rc = cuda_status(cudaMemsetAsync(e->W.get(), 0, e->W.size() * 8, e->stream), "memset");
+  if (!rc) rc = cuda_status(cudaMemsetAsync(e->Wg.get(), 0, e->Wg.size() * 8, e->stream), "memset");
+  if (!rc) rc = e->d_grids.upload(e->grids.data(), e->grids.size(), e->stream);
+  if (!rc) rc = cuda_status(cudaStreamSynchronize(e->stream), "sync");
+  if (rc) return fail(rc);
+  Y3B_CUDA(cudaFuncSetAttribute(prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)e->prep_smem));
+  Y3B_CUDA(cudaFuncSetAttribute(direct_main_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)e->direct_smem));
+  *out = e;
+  return Y3B_OK;
+}
+
+extern "C" size_t
+y3b_engine_table_stride(const y3b_engine* e)
+{
+  return e ? e->lay.stride : 0;
+}
+
+extern "C" int
+y3b_engine_table_offsets(const y3b_engine* e, size_t* off7)
+{
+  if (!e || !off7) return Y3B_ERR_INVALID;
+  for (int i = 0; i < 7; ++i) off7[i] = e->lay.off[i];
+  return Y3B_OK;
+}
+
+extern "C" int
+y3b_engine_n_bins(const y3b_engine* e)
+{
+  return e ? e->nB_max : 0;
+}
+
+extern "C" size_t
+y3b_engine_device_bytes(const y3b_engine* e)
+{
+  return e ? e->device_bytes : 0;
+}
+
+namespace y3b {
+
+// Enqueue one evaluation on `s`.  grid_mask selects the grids present.
+static int
+enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_tables,
+        double* d_counts, double* d_shear, cudaStream_t s, int grid_mask)
+{
+  Y3B_CUDA(cudaMemsetAsync(e->status.get(), 0, sizeof(int), s));
+  PrepArgs pa{e->d_grids.get(), d_pts, d_tables, e->lay, prec == Y3B_MIXED, e->s64.get(),
+              e->s32.get(), e->status.get()};
+  prep_kernel<<<n, 256, e->prep_smem, s>>>(pa);
+  count_launch();
+  Y3B_CUDA(cudaGetLastError());
+  if (prec == Y3B_FP64) {
+    dim3 g1(e->nz_max, n);
+    direct_main_kernel<<<g1, 256, e->direct_smem, s>>>(e->d_grids.get(), d_pts, e->s64.get(),
+                                                       grid_mask);
+    count_launch();
+    Y3B_CUDA(cudaGetLastError());
+    direct_wreduce_kernel<<<n, 256, 0, s>>>(e->d_grids.get(), d_pts, e->s64.get(), e->W.get(),
+                                            e->Wg.get(), e->w_stride, grid_mask);
+    count_launch();
+    Y3B_CUDA(cudaGetLastError());
+  } else {
+    for (int g = 0; g < (int)e->grids.size(); ++g) {
+      if (!((grid_mask >> g) & 1)) continue;
+      MixedLaunch L{e->d_grids.get(), d_pts, g, n, &e->grids[g], e->s32.get(), e->W.get(),
+                    e->Wg.get(), e->w_stride, e->status.get(), s};
+      Y3B_TRY(launch_mixed_gemm(L));
+    }
+  }
+  const bool shear = e->cfg.with_shear && d_shear;
+  if (shear) {
+    long long warps = (long long)n * e->nI_max * e->shear.n_R * e->w_stride;
+    long long blocks = (warps * 32 + 127) / 128;
+    if (prec == Y3B_FP64)
+      shear_phi_kernel<double><<<(unsigned)blocks, 128, 0, s>>>(
+        e->d_grids.get(), d_pts, n, e->w_stride, e->shear, e->quad.view(), e->Phi.get(),
+        e->nI_max, grid_mask);
+    else
+      shear_phi_kernel<float><<<(unsigned)blocks, 128, 0, s>>>(
+        e->d_grids.get(), d_pts, n, e->w_stride, e->shear, e->quad.view(), e->Phi.get(),
+        e->nI_max, grid_mask);
+    count_launch();
+    Y3B_CUDA(cudaGetLastError());
+  }
+  finalize_kernel<<<n, 256, 0, s>>>(e->d_grids.get(), d_pts, e->W.get(), e->Wg.get(),
+                                    shear ? e->Phi.get() : nullptr, e->w_stride, e->nB_max,
+                                    e->nI_max, e->shear.n_R, d_counts, shear ? d_shear : nullptr,
+                                    grid_mask);
+  count_launch();
+  Y3B_CUDA(cudaGetLastError());
+  e->last_n = n;
+  return Y3B_OK;
+}
+
+}  // namespace y3b
+
+extern "C" int
+y3b_engine_eval_device(y3b_engine* e, int precision, int n, const y3b_point* pts_dev,
+                       const double* tables_dev, double* counts_dev, double* shear_dev,
+                       void* stream)
+{
+  clear_error();
+  if (!e || n < 1 || n > e->cfg.max_points || !pts_dev || !tables_dev || !counts_dev ||
+      (precision != Y3B_FP64 && precision != Y3B_MIXED)) {
+    set_error("y3b_engine_eval_device: invalid arguments (1 <= n <= max_points)");
+    return Y3B_ERR_INVALID;
+  }
+  if (((uintptr_t)tables_dev & 15u) != 0) {
+    set_error("y3b_engine_eval_device: tables must be 16-byte aligned");
+    return Y3B_ERR_INVALID;
+  }
+  static_assert(sizeof(y3b_point) == sizeof(PointDev), "y3b_point layout");
+  cudaStream_t s = stream ? (cudaStream_t)stream : e->stream;
+  int mask = (1 << (int)e->grids.size()) - 1;
+  return enqueue(e, precision, n, reinterpret_cast<const PointDev*>(pts_dev), tables_dev,
+                 counts_dev, shear_dev, s, mask);
+}
+
+extern "C" int
+y3b_engine_sync(y3b_engine* e, void* stream)
+{
+  clear_error();
+  if (!e) return Y3B_ERR_INVALID;
+  cudaStream_t s = stream ? (cudaStream_t)stream : e->stream;
+  int rc = read_device_status(e->status.get(), s);
+  if (rc == Y3B_ERR_DOMAIN) set_error("y3b engine: a z_t node lies outside distances/z");
+  if (rc == Y3B_ERR_TIMEOUT) set_error("y3b engine: a bounded device wait ran out");
+  return rc;
+}
+
+extern "C" int
+y3b_engine_eval(y3b_engine* e, int precision, int n, const y3b_point* pts,
+                const double* tables, double* counts, double* shear)
+{
+  clear_error();
+  if (!e || n < 1 || n > e->cfg.max_points || !pts || !tables || !counts ||
+      (precision != Y3B_FP64 && precision != Y3B_MIXED)) {
+    set_error("y3b_engine_eval: invalid arguments (1 <= n <= max_points)");
+    return Y3B_ERR_INVALID;
+  }
+  int mask = 0;
+  for (int i = 0; i < n; ++i) {
+    const y3b_point& p = pts[i];
+    if (p.grid < 0 || p.grid >= (int)e->grids.size()) {
+      set_error("y3b_engine_eval: point %d has grid %d outside [0, %d)", i, p.grid,
+                (int)e->grids.size());
+      return Y3B_ERR_INVALID;
+    }
+    if (!(p.sigma > 0.0) || !(p.Mpiv > 0.0) || !(p.cosmo.om - p.cosmo.onu > 0.0) ||
+        !(p.cosmo.h0 > 0.0)) {
+      set_error("y3b_engine_eval: point %d has non-positive sigma, Mpiv, h0 or omega_M - omega_nu",
+                i);
+      return Y3B_ERR_INVALID;
+    }
+    mask |= 1 << p.grid;
+  }
+  cudaStream_t s = e->stream;
+  Y3B_CUDA(cudaMemcpyAsync(e->pts.get(), pts, n * sizeof(y3b_point), cudaMemcpyHostToDevice, s));
+  Y3B_CUDA(cudaMemcpyAsync(e->tables.get(), tables, n * e->lay.stride * sizeof(double),
+                           cudaMemcpyHostToDevice, s));
+  const bool want_shear = e->cfg.with_shear && shear;
+  Y3B_TRY(enqueue(e, precision, n, e->pts.get(), e->tables.get(), e->counts.get(),
+                  want_shear ? e->shear_out.get() : nullptr, s, mask));
+  Y3B_CUDA(cudaMemcpyAsync(counts, e->counts.get(), (size_t)n * e->nB_max * sizeof(double),
+                           cudaMemcpyDeviceToHost, s));
+  if (want_shear)
+    Y3B_CUDA(cudaMemcpyAsync(shear, e->shear_out.get(),
+                             (size_t)n * e->nB_max * e->shear.n_R * sizeof(double),
+                             cudaMemcpyDeviceToHost, s));
+  return y3b_engine_sync(e, nullptr);
+}
+
+extern "C" int
+y3b_engine_weights(y3b_engine* e, int n, double* W)
+{
+  clear_error();
+  if (!e || !W || n < 1 || n > e->last_n) {
+    set_error("y3b_engine_weights: n must be within the last evaluation");
+    return Y3B_ERR_INVALID;
+  }
+  Y3B_CUDA(cudaStreamSynchronize(e->stream));
+  Y3B_CUDA(cudaMemcpy(W, e->W.get(), (size_t)n * e->nB_max * e->w_stride * sizeof(double),
+                      cudaMemcpyDeviceToHost));
+  return Y3B_OK;
+}
