@@ -1,0 +1,367 @@
+#!/usr/bin/env python
+"""Benchmark: parameter-point evaluations per second of the cluster
+number-count integral N(lambda_obs bin, z_obs bin) at the 4x node density
+(256 lnM x 128 z_t x 256 lambda_t x 256 lambda_obs/bin x 64 z_obs/bin),
+mixed precision (FP32 integrands, split-BF16 tcgen05 contraction, FP64 final
+sums), on batches of walkers drawn from the batched-config prior, each point
+with its own HMF / dV/dz / Sigma_crit tables (seeded synthetic data).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+One JSON line on rank 0.  `value` is device-timed with inputs resident in
+HBM (L2 flushed between steps); `e2e` goes through the C ABI with pinned host
+buffers, host<->device copies inside the timed region.  Under torchrun every
+rank evaluates its own batch (weak scaling, no data-path collective) and the
+time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "param-point evals/sec at <=1e-4 rel err vs FP64 (counts, 4x nodes)"
+UNIT = "points/s"
+WORKLOAD = ("number counts N(lambda_obs, z_obs), 12 bins, 4x nodes 256 lnM x 128 z_t x 256 "
+            "lam_t x 256 lam_o/bin x 64 z_o/bin, walkers from the batched-config prior")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=2048, help="points per step per GPU")
+    ap.add_argument("--unique", type=int, default=256, help="distinct walker tables per batch")
+    ap.add_argument("--density", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=2, help="points in the CPU baseline sample")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d.get("bf16_tflops", 1590.0), d.get("hbm_gbs", 6650.0), "measured"
+    return 1590.0, 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        loaded = [s for s in sm if s > 0.5 * smax] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": smax, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def cpu_baseline(density, n_points):
+    """The FP64 oracle (a port of the reference algorithm) on the host, one
+    thread, on a bounded sample of the same workload."""
+    import numpy as np  # noqa: F401
+
+    import oracle
+    from y3_cluster_cpp_b200 import synthetic
+    g = synthetic.grid(density)
+    pz, pc = synthetic.plob_baseline()
+    pts = synthetic.walkers(n_points, seed=11, densities=(density,), with_sci=False)
+    oracle.lib()
+    t0 = time.perf_counter()
+    for p in pts:
+        oracle.direct_eval(g, pz, pc, p.mor, oracle.cosmo(p.om, p.h0), p.tables)
+    dt = time.perf_counter() - t0
+    return {"value": n_points / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{n_points} points at {density}x nodes, FP64 oracle (C), 1 thread, "
+                      f"{dt:.1f} s"}
+
+
+def _ref_worker(args):
+    density, seed = args
+    import oracle
+    from y3_cluster_cpp_b200 import synthetic
+    g = synthetic.grid(density)
+    pz, pc = synthetic.plob_baseline()
+    p = synthetic.walkers(1, seed=seed, densities=(density,), with_sci=False)[0]
+    oracle.direct_eval(g, pz, pc, p.mor, oracle.cosmo(p.om, p.h0), p.tables)
+    return 1
+
+
+def run_reference(a):
+    """Reference arm: the reference algorithm's CPU form (the oracle port; the
+    reference's own C++ needs CosmoSIS/GSL and is not buildable here) on all
+    host cores, one point per worker per step."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    import oracle
+    oracle.build()
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        for w in range(a.warmup):
+            pool.map(_ref_worker, [(a.density, 100 + w * cores + i) for i in range(cores)])
+        t0 = time.perf_counter()
+        for s in range(a.steps):
+            pool.map(_ref_worker, [(a.density, 1000 + s * cores + i) for i in range(cores)])
+        dt = time.perf_counter() - t0
+    value = a.steps * cores / dt
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * dt / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded walkers, HMF/dV/dz/Sigma_crit tables)",
+            "config": {"workload": WORKLOAD, "points_per_step": cores, "density": a.density},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{cores} points per step (one per core), FP64 oracle"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(a):
+    import numpy as np
+    import torch
+
+    from y3_cluster_cpp_b200 import _capi, engine, sharding, synthetic
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    engine.check(engine.lib().y3b_device_init(local))
+    dev = torch.device("cuda", local)
+
+    # ---- inputs: B points, `unique` distinct walker tables (seed + rank) ----
+    B = a.batch
+    uniq = synthetic.walkers(min(a.unique, B), seed=1 + 1000 * rank, densities=(a.density,))
+    pts = [uniq[i % len(uniq)] for i in range(B)]
+    g = synthetic.grid(a.density)
+    t0 = uniq[0].tables
+    pz, pc = synthetic.plob_baseline()
+    eng = engine.Engine([g], len(t0["hmf_m_h"]), len(t0["hmf_z"]), len(t0["dist_z"]), (pz, pc),
+                        max_points=B, n_sci=len(t0["sci_z"]))
+    n_bins = eng.n_bins
+    tab_u = eng.pack(uniq)
+    tables_h = torch.empty((B, eng.stride), dtype=torch.float64, pin_memory=True)
+    tables_h.numpy()[:] = tab_u[np.arange(B) % len(uniq)]
+    parr = eng.points_array(pts, grid_of=lambda _: 0)
+    pts_h = torch.empty(C.sizeof(parr), dtype=torch.uint8, pin_memory=True)
+    C.memmove(pts_h.data_ptr(), C.addressof(parr), C.sizeof(parr))
+    counts_h = torch.empty((B, n_bins), dtype=torch.float64, pin_memory=True)
+    tables_d = tables_h.to(dev)
+    pts_d = pts_h.to(dev)
+    counts_d = torch.empty((B, n_bins), dtype=torch.float64, device=dev)
+    # A dedicated (non-default) stream: the library launches on it and the
+    # CUDA events below are recorded on it.
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    sp = stream.cuda_stream
+
+    def step(prec, n=B):
+        eng.eval_device(prec, n, pts_d.data_ptr(), tables_d.data_ptr(), counts_d.data_ptr(),
+                        0, sp)
+
+    # ---- accuracy of the mixed form vs FP64 on this batch (untimed) ----
+    step(engine.FP64)
+    eng.sync(sp)
+    c64 = counts_d.double().cpu().numpy().copy()
+    step(engine.MIXED)
+    eng.sync(sp)
+    cmx = counts_d.double().cpu().numpy().copy()
+    max_rel = float(np.max(np.abs(cmx / c64 - 1)))
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2 (126 MB)
+
+    # ---- device-resident timed region ----
+    for _ in range(a.warmup):
+        flush.zero_()
+        step(engine.MIXED)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    launches0 = engine.launch_count()
+    eng.profile(True)
+    torch.cuda.synchronize(dev)
+    for s in range(a.steps):
+        flush.zero_()
+        starts[s].record(stream)
+        step(engine.MIXED)
+        ends[s].record(stream)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    launches = engine.launch_count() - launches0
+    prof = eng.profile_read()
+    eng.profile(False)
+    eng.sync(sp)
+    clk = clocks.stop()
+    step_ms = [st.elapsed_time(en) for st, en in zip(starts, ends)]
+    total_ms = sharding.max_over_ranks(sum(step_ms), dev)
+    value = world * B * a.steps / (total_ms / 1e3)
+
+    # ---- roofline of the dominant kernel (the tcgen05 contraction) ----
+    gemm_ms = prof["contraction"] / max(prof["evals"], 1)
+    flops_alg = 2.0 * g["n_m"] * (len(g["lam_edges"]) - 1) * g["n_z"] * g["n_t"] * B
+    peak_tf, peak_gbs, peak_kind = measured_peaks()
+    achieved_tf = flops_alg / (gemm_ms / 1e3) / 1e12
+    stage_share = {k: prof[k] / max(sum(prof[x] for x in ("prep", "contraction", "shear",
+                                                             "final")), 1e-12)
+                   for k in ("prep", "contraction", "final")}
+
+    # ---- plain FP64 GPU form: one point per call (the metric's denominator) ----
+    n_plain = 16
+    for _ in range(3):
+        step(engine.FP64, 1)
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(n_plain):
+        step(engine.FP64, 1)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    plain_fp64 = n_plain / (e0.elapsed_time(e1) / 1e3)
+    # batched FP64 on the same batch, for context
+    flush.zero_()
+    e0.record(stream)
+    step(engine.FP64)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    fp64_batched = B / (e0.elapsed_time(e1) / 1e3)
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    lib = engine.lib()
+    PPt = C.cast(C.c_void_p(pts_h.data_ptr()), C.POINTER(_capi.Point))
+    TPt = C.cast(C.c_void_p(tables_h.data_ptr()), _capi.PD)
+    CPt = C.cast(C.c_void_p(counts_h.data_ptr()), _capi.PD)
+    for _ in range(2):
+        engine.check(lib.y3b_engine_eval(eng.handle, engine.MIXED, B, PPt, TPt, CPt, None))
+    e2e_t = []
+    for _ in range(max(3, a.steps // 2)):
+        t_0 = time.perf_counter()
+        engine.check(lib.y3b_engine_eval(eng.handle, engine.MIXED, B, PPt, TPt, CPt, None))
+        e2e_t.append(time.perf_counter() - t_0)
+    e2e_total = sharding.max_over_ranks(sum(e2e_t), dev)
+    e2e_value = world * B * len(e2e_t) / e2e_total
+    h2d = B * (C.sizeof(_capi.Point) + eng.stride * 8)
+    d2h = B * n_bins * 8
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(a.density, a.cpu_sample)
+
+    if world > 1:
+        torch.distributed.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": total_ms / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32/bf16x3 (f64 final sums)",
+            "data": "synthetic (seeded walkers; per-point HMF, dV/dz, Sigma_crit tables)",
+            "config": {"workload": WORKLOAD, "points_per_step_per_gpu": B,
+                       "distinct_walker_tables": len(uniq), "density": a.density,
+                       "l2": "flushed between timed steps (256 MB write)",
+                       "parallelism": f"walker-sharded x{world}"},
+            "max_rel_err_vs_fp64": max_rel,
+            "plain_fp64": {"value": plain_fp64, "unit": UNIT,
+                           "mode": "FP64 direct quadrature, one point per call"},
+            "fp64_batched": {"value": fp64_batched, "unit": UNIT},
+            "speedup_vs_plain_fp64": value / world / plain_fp64,
+            "roofline": {"bound": "tensor", "achieved": achieved_tf, "peak": peak_tf,
+                         "unit": "TFLOP/s", "frac": achieved_tf / peak_tf, "traffic": None,
+                         "kernel": "mixed_gemm_kernel",
+                         "algorithmic_flops_per_launch": flops_alg,
+                         "tensor_pipe_flops_per_launch": 3 * flops_alg,
+                         "peak_source": f"bf16_tflops ({peak_kind})",
+                         "avg_launch_ms": gemm_ms},
+            "stage_share": stage_share,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -258,6 +258,15 @@ int y3b_engine_sync(y3b_engine* e, void* stream);
  * of each point's grid, padded to the largest n_m), host buffer. */
 int y3b_engine_weights(y3b_engine* e, int n, double* W);
 
+/* Stage timing with CUDA events recorded on the launching stream around each
+ * stage of every evaluation: 0 = per-point prep, 1 = lambda_t contraction
+ * (tcgen05 GEMM or FP64 direct sum + z reduction), 2 = miscentred profile,
+ * 3 = final sums.  enable = 1 starts (and zeroes) the accumulators, 0 stops.
+ * y3b_engine_profile_read synchronises the engine's work and writes the
+ * accumulated milliseconds ms[4] and the number of evaluations timed. */
+int y3b_engine_profile(y3b_engine* e, int enable);
+int y3b_engine_profile_read(y3b_engine* e, double* ms, int* n_evals);
+
 /* Self-test of the bounded device wait: launches a kernel that waits on a
  * barrier nobody arrives at for ~`usec` microseconds and must come back
  * with Y3B_ERR_TIMEOUT (the context stays usable). */

@@ -95,6 +95,16 @@ interp2d_clamp(const double* xs, int nx, const double* ys, int ny,
          (1.0 - t) * u * r1[0] + t * u * r1[1];
 }
 
+// 2^x on the MUFU unit (PTX ex2.approx.ftz.f32; ~2 ulp, subnormals flush
+// to zero -- used only where such values are negligible).
+__device__ __forceinline__ float
+fast_exp2(float x)
+{
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // ---------------------------------------------------------------------------
 // Cosmology.
 __device__ __forceinline__ double

@@ -91,7 +91,50 @@ struct PrepArgs {
   double* s64;
   float* s32;
   int* status;
+  int grid_mask;
 };
+
+// MOR normalisation D = Phi(b) - Phi(a) in FP64, a = (l_lo - mu)/s,
+// b = (l_hi - mu)/s.  The lam_t domain is many sigma wide, so at most one
+// tail is open: D = 1 exactly when both are below half an FP64 ulp
+// (a < -8.5, b > 8.5); with one tail closed D = Phi(b) or Phi(-a), a single
+// erfc on the side that does not cancel.  Kept out of line: the rare path.
+__device__ __noinline__ double
+mor_norm_slow(double a, double b)
+{
+  if (a < -8.5)  // low tail closed: D = Phi(b)
+    return b < 0.0 ? 0.5 * erfc(-b / kSqrt2) : 1.0 - 0.5 * erfc(b / kSqrt2);
+  if (b > 8.5)  // high tail closed: D = Phi(-a)
+    return a > 0.0 ? 0.5 * erfc(a / kSqrt2) : 1.0 - 0.5 * erfc(-a / kSqrt2);
+  return phi_diff(a, b);
+}
+
+__device__ __forceinline__ double
+mor_norm(double a, double b)
+{
+  if (a < -8.5 && b > 8.5) return 1.0;
+  return mor_norm_slow(a, b);
+}
+
+// Per-point prep, one CTA per point.  The point's packed tables are staged
+// into shared memory with one bulk (TMA) copy completing on an mbarrier;
+// then, per point:
+//   FP64: cz_q = v_q dV(z_q) Omega(z_q), czs_q = cz_q Sci(z_q), alpha_k,
+//         beta_q (s64), and for the FP64 form P0 = n(M_k,z_q) / (sqrt(2 pi)
+//         s D_kq);
+//   mixed form: a_k, b_q, delta_t, c1, c2, C_j(q), C^g_j(q) and
+//         Y = n H / (sqrt(2 pi) s D) in FP32 (D in FP64 where not exactly 1).
+// Shared memory: table block | FP32 dn/dlnM | per-k and per-q vectors.
+__host__ __device__ inline size_t
+prep_smem_bytes(size_t stride, int n_hz, int n_hm, int n_m, int n_z)
+{
+  size_t b = stride * 8;                                   // table block
+  b += (((size_t)n_hz * n_hm * 4) + 15) & ~size_t(15);     // FP32 dn/dlnM
+  b += (size_t)n_m * (8 + 8 + 8 + 4 + 4);                  // alpha, t, kf, xi, pad
+  b += (size_t)n_z * (8 + 8 + 4 + 4);                      // beta, u, yi, pad
+  b += (size_t)n_m * 12;                                   // FP32 t, kf, alpha - A0
+  return b + 64;
+}
 
 __global__ void __launch_bounds__(256)
 prep_kernel(PrepArgs a)
@@ -99,25 +142,25 @@ prep_kernel(PrepArgs a)
   extern __shared__ __align__(16) double psh[];
   const int p = blockIdx.x;
   const PointDev pt = a.pts[p];
-  const GridDev& G = a.grids[pt.grid];
-  const int n_m = G.n_m, n_z = G.n_z, tid = threadIdx.x;
+  if (!((a.grid_mask >> pt.grid) & 1)) return;
+  const GridDev* __restrict__ Gp = a.grids + pt.grid;
+  const int n_m = Gp->n_m, n_z = Gp->n_z, n_m_pad = Gp->n_m_pad, tid = threadIdx.x;
   const TableLayout& L = a.lay;
-
-  double* tab = psh;                                   // [stride]
-  double* ka = tab + L.stride;                         // alpha_k       [n_m]
-  double* kt = ka + n_m;                               // hmf x weight  [n_m]
-  double* kf = kt + n_m;                               // (s, q) factor [n_m]
-  int* kx = reinterpret_cast<int*>(kf + n_m);          // hmf x cell    [n_m]
-  double* qb = reinterpret_cast<double*>(kx + ((n_m + 1) & ~1));  // beta_q [n_z]
-  double* qu = qb + n_z;                               // hmf y weight  [n_z]
-  double* qc = qu + n_z;                               // cz            [n_z]
-  double* qs = qc + n_z;                               // czs           [n_z]
-  int* qy = reinterpret_cast<int*>(qs + n_z);          // hmf y cell    [n_z]
-  double* red = reinterpret_cast<double*>(qy + ((n_z + 1) & ~1));  // [8]
+  const int n_hm = L.n_hm, n_hz = L.n_hz;
+  double* tab = psh;                                                  // [stride]
+  float* h32 = reinterpret_cast<float*>(tab + L.stride);              // [n_hz n_hm]
+  double* k_alpha = reinterpret_cast<double*>(
+    reinterpret_cast<uint8_t*>(h32) + ((((size_t)n_hz * n_hm * 4) + 15) & ~size_t(15)));
+  double* k_t = k_alpha + n_m;
+  double* k_f = k_t + n_m;
+  double* q_beta = k_f + n_m;
+  double* q_u = q_beta + n_z;
+  int* k_x = reinterpret_cast<int*>(q_u + n_z);
+  int* q_y = k_x + n_m;
   __shared__ __align__(8) uint64_t bar;
   __shared__ int timed_out;
+  __shared__ double red[2];
 
-  // Bulk copy of this point's table block (16-byte aligned, multiple of 16).
   const double* src = a.tables + (size_t)p * L.stride;
   const uint32_t bytes = (uint32_t)(L.stride * sizeof(double));
   if (tid == 0) {
@@ -165,100 +208,171 @@ prep_kernel(PrepArgs a)
   const double* sz = tab + L.off[5];
   const double* sv = tab + L.off[6];
   // HMF mass axis ln(m_h (Omega_M - Omega_nu)) (hmf_t.hh:15-25), in place.
-  for (int i = tid; i < L.n_hm; i += blockDim.x) mh[i] = log(mh[i] * (pt.om - pt.onu));
+  for (int i = tid; i < n_hm; i += blockDim.x) mh[i] = log(mh[i] * (pt.om - pt.onu));
+  if (a.mixed)
+    for (int i = tid; i < n_hz * n_hm; i += blockDim.x) h32[i] = (float)dn[i];
   __syncthreads();
+  double* s64 = a.s64 + (size_t)p * Gp->s64_stride;
+  float* s32 = a.s32 + (size_t)p * Gp->s32_stride;
   const double lnMpiv = log(pt.Mpiv);
+  const double* xm = Gp->xm;
+  const double* xz = Gp->xz;
   for (int k = tid; k < n_m; k += blockDim.x) {
-    const double x = G.xm[k];
-    ka[k] = pt.B * (x - lnMpiv);
-    const double xx = fmin(fmax(x, mh[0]), mh[L.n_hm - 1]);
-    const int xi = bsearch_cell(mh, L.n_hm, xx);
-    kx[k] = xi;
-    kt[k] = (xx - mh[xi]) / (mh[xi + 1] - mh[xi]);
-    kf[k] = pt.hmf_s * (x * kLog10e - kHmfPivot) + pt.hmf_q;
+    const double x = xm[k];
+    const double alpha = pt.B * (x - lnMpiv);
+    k_alpha[k] = alpha;
+    s64[Gp->o_alpha + k] = alpha;
+    const double xx = fmin(fmax(x, mh[0]), mh[n_hm - 1]);
+    const int xi = bsearch_cell(mh, n_hm, xx);
+    k_x[k] = xi;
+    k_t[k] = (xx - mh[xi]) / (mh[xi + 1] - mh[xi]);
+    k_f[k] = pt.hmf_s * (x * kLog10e - kHmfPivot) + pt.hmf_q;
   }
+  const size_t o_cz = Gp->o_cz, o_czs = Gp->o_czs, o_beta = Gp->o_beta;
+  const double* Kj = Gp->Kj;
+  const int nJ = Gp->nJ;
   for (int q = tid; q < n_z; q += blockDim.x) {
-    const double z = G.xz[q];
-    qb[q] = pt.A + pt.C * log1p(z);
-    const double zz = fmin(fmax(z, hz[0]), hz[L.n_hz - 1]);
-    const int yi = bsearch_cell(hz, L.n_hz, zz);
-    qy[q] = yi;
-    qu[q] = (zz - hz[yi]) / (hz[yi + 1] - hz[yi]);
+    const double z = xz[q];
+    const double beta = pt.A + pt.C * log1p(z);
+    q_beta[q] = beta;
+    s64[o_beta + q] = beta;
+    const double zz = fmin(fmax(z, hz[0]), hz[n_hz - 1]);
+    const int yi = bsearch_cell(hz, n_hz, zz);
+    q_y[q] = yi;
+    q_u[q] = (zz - hz[yi]) / (hz[yi + 1] - hz[yi]);
     double dv;
     if (!dv_do_dz(dz, da, L.n_dist, pt.om, pt.ol, pt.ok, pt.h0, z, &dv)) {
       set_err(a.status, kDevDomain);
       dv = 0.0;
     }
-    const double cz = G.wz[q] * dv * G.omz[q];
-    qc[q] = cz;
-    qs[q] = cz * (L.n_sci > 1 ? interp1d_clamp(sz, sv, L.n_sci, z) : 1.0);
+    const double cz = Gp->wz[q] * dv * Gp->omz[q];
+    const double czs = cz * (L.n_sci > 1 ? interp1d_clamp(sz, sv, L.n_sci, z) : 1.0);
+    s64[o_cz + q] = cz;
+    s64[o_czs + q] = czs;
+    if (a.mixed) {
+      for (int j = 0; j < nJ; ++j) {
+        s32[Gp->f_CN + j * n_z + q] = (float)(cz * Kj[j * n_z + q]);
+        s32[Gp->f_CG + j * n_z + q] = (float)(czs * Kj[j * n_z + q]);
+      }
+    }
   }
   __syncthreads();
-  if (tid == 0) {  // centres of the alpha and beta ranges (serial, n <= 1024)
-    double amin = ka[0], amax = ka[0], bmin = qb[0], bmax = qb[0];
-    for (int k = 1; k < n_m; ++k) {
-      amin = fmin(amin, ka[k]);
-      amax = fmax(amax, ka[k]);
+  {  // centres of the alpha and beta ranges: block min/max
+    double amin = 1e300, amax = -1e300, bmin = 1e300, bmax = -1e300;
+    for (int k = tid; k < n_m; k += blockDim.x) {
+      amin = fmin(amin, k_alpha[k]);
+      amax = fmax(amax, k_alpha[k]);
     }
-    for (int q = 1; q < n_z; ++q) {
-      bmin = fmin(bmin, qb[q]);
-      bmax = fmax(bmax, qb[q]);
+    for (int q = tid; q < n_z; q += blockDim.x) {
+      bmin = fmin(bmin, q_beta[q]);
+      bmax = fmax(bmax, q_beta[q]);
     }
-    red[0] = 0.5 * (amin + amax);
-    red[1] = 0.5 * (bmin + bmax);
+    for (int off = 16; off > 0; off >>= 1) {
+      amin = fmin(amin, __shfl_xor_sync(0xffffffffu, amin, off));
+      amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, off));
+      bmin = fmin(bmin, __shfl_xor_sync(0xffffffffu, bmin, off));
+      bmax = fmax(bmax, __shfl_xor_sync(0xffffffffu, bmax, off));
+    }
+    __shared__ double wred[4][32];
+    const int w = tid >> 5, nw = blockDim.x >> 5;
+    if ((tid & 31) == 0) {
+      wred[0][w] = amin;
+      wred[1][w] = amax;
+      wred[2][w] = bmin;
+      wred[3][w] = bmax;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      for (int i = 1; i < nw; ++i) {
+        amin = fmin(amin, wred[0][i]);
+        amax = fmax(amax, wred[1][i]);
+        bmin = fmin(bmin, wred[2][i]);
+        bmax = fmax(bmax, wred[3][i]);
+      }
+      red[0] = 0.5 * (amin + amax);
+      red[1] = 0.5 * (bmin + bmax);
+      s64[Gp->o_scal] = red[0];
+      s64[Gp->o_scal + 1] = red[1];
+    }
   }
   __syncthreads();
   const double A0 = red[0], B0 = red[1];
-  const double sig = pt.sigma, inv2s2 = 0.5 / (sig * sig);
+  const double sig = pt.sigma, inv_s = 1.0 / sig;
   const double norm0 = 1.0 / (kSqrt2Pi * sig);
-  double* s64 = a.s64 + (size_t)p * G.s64_stride;
-  float* s32 = a.s32 + (size_t)p * G.s32_stride;
-  for (int q = tid; q < n_z; q += blockDim.x) {
-    s64[G.o_cz + q] = qc[q];
-    s64[G.o_czs + q] = qs[q];
-    s64[G.o_beta + q] = qb[q];
-  }
-  for (int k = tid; k < n_m; k += blockDim.x) s64[G.o_alpha + k] = ka[k];
-  // (k, q) products: HMF bilinear (separable cells), D_kq, and the form's
-  // per-(k, q) factor.
-  for (int idx = tid; idx < n_m * n_z; idx += blockDim.x) {
-    const int q = idx / n_m, k = idx % n_m;
-    const double t = kt[k], u = qu[q];
-    const double* r0 = dn + (size_t)qy[q] * L.n_hm + kx[k];
-    const double* r1 = r0 + L.n_hm;
-    const double n = ((1.0 - t) * (1.0 - u) * r0[0] + t * (1.0 - u) * r0[1] +
-                      (1.0 - t) * u * r1[0] + t * u * r1[1]) *
-                     kf[k];
-    const double mu = ka[k] + qb[q];
-    const double D = phi_diff((G.ll_lo - mu) / sig, (G.ll_hi - mu) / sig);
-    if (!a.mixed) {
-      s64[G.o_P0 + idx] = n * norm0 / D;
-    } else {
-      const double aa = ka[k] - A0, bb = qb[q] - B0;
-      const double H = exp(-(2.0 * aa * bb + bb * bb) * inv2s2);
-      s32[G.f_Yt + (size_t)q * G.n_m_pad + k] = (float)(n * H * norm0 / D);
+  const double ll_lo = Gp->ll_lo, ll_hi = Gp->ll_hi;
+  if (!a.mixed) {
+    double* __restrict__ P0 = s64 + Gp->o_P0;
+    for (int idx = tid; idx < n_z * n_m; idx += blockDim.x) {
+      const int q = idx / n_m, k = idx - q * n_m;
+      const double t = k_t[k], u = q_u[q];
+      const double* r0 = dn + (size_t)q_y[q] * n_hm + k_x[k];
+      const double* r1 = r0 + n_hm;
+      const double n = ((1.0 - t) * (1.0 - u) * r0[0] + t * (1.0 - u) * r0[1] +
+                        (1.0 - t) * u * r1[0] + t * u * r1[1]) *
+                       k_f[k];
+      const double mu = k_alpha[k] + q_beta[q];
+      P0[idx] = n * norm0 / mor_norm((ll_lo - mu) * inv_s, (ll_hi - mu) * inv_s);
     }
+    return;
   }
-  if (a.mixed) {
-    const double L0 = A0 + B0;
-    for (int k = tid; k < G.n_m_pad; k += blockDim.x) {
-      s32[G.f_a + k] = k < n_m ? (float)(ka[k] - A0) : 0.f;
-      if (k >= n_m)
-        for (int q = 0; q < n_z; ++q) s32[G.f_Yt + (size_t)q * G.n_m_pad + k] = 0.f;
-    }
-    for (int q = tid; q < n_z; q += blockDim.x) {
-      s32[G.f_b + q] = (float)(qb[q] - B0);
-      for (int j = 0; j < G.nJ; ++j) {
-        s32[G.f_CN + j * n_z + q] = (float)(qc[q] * G.Kj[j * n_z + q]);
-        s32[G.f_CG + j * n_z + q] = (float)(qs[q] * G.Kj[j * n_z + q]);
+  // Mixed form: factor vectors and Y(k, q).
+  const double L0 = A0 + B0;
+  const int n_t = Gp->n_t, n_t_pad = Gp->n_t_pad;
+  for (int k = tid; k < n_m_pad; k += blockDim.x)
+    s32[Gp->f_a + k] = k < n_m ? (float)(k_alpha[k] - A0) : 0.f;
+  for (int q = tid; q < n_z; q += blockDim.x) s32[Gp->f_b + q] = (float)(q_beta[q] - B0);
+  for (int t = tid; t < n_t_pad; t += blockDim.x)
+    s32[Gp->f_delta + t] = t < n_t ? (float)(Gp->xl[t] - L0) : 0.f;
+  if (tid == 0) {
+    const double log2e = 1.4426950408889634;
+    s32[Gp->f_scal] = (float)(log2e * 0.5 / (sig * sig));  // c1: F = exp2(-(d - a)^2 c1)
+    s32[Gp->f_scal + 1] = (float)(log2e / (sig * sig));    // c2: G = exp2(d b c2)
+  }
+  float* __restrict__ Yt = s32 + Gp->f_Yt;
+  const float c2 = (float)(1.4426950408889634 / (sig * sig));
+  const float norm0f = (float)norm0;
+  // D_kq = 1 exactly when mu is more than 8.5 sigma inside the lam_t domain;
+  // the FP32 test keeps a 1e-3 margin, everything else takes the FP64 path.
+  const float mu_sat_lo = (float)(ll_lo + 8.5 * sig - L0) + 1e-3f;
+  const float mu_sat_hi = (float)(ll_hi - 8.5 * sig - L0) - 1e-3f;
+  // FP32 copies of the per-k vectors, reusing the FP64 arrays' space is not
+  // possible (they are read below), so they go after them in h32's tail.
+  float* kt_f = reinterpret_cast<float*>(q_y + n_z);  // [n_m]
+  float* kf_f = kt_f + n_m;                            // [n_m]
+  float* ka_f = kf_f + n_m;                            // [n_m] alpha - A0
+  for (int k = tid; k < n_m; k += blockDim.x) {
+    kt_f[k] = (float)k_t[k];
+    kf_f[k] = (float)k_f[k];
+    ka_f[k] = (float)(k_alpha[k] - A0);
+  }
+  __syncthreads();
+  // One warp per z row; lanes over lnM (no divides, FP32 in the common path).
+  const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+  for (int q = warp; q < n_z; q += nw) {
+    const float u = (float)q_u[q];
+    const float bb = (float)(q_beta[q] - B0);
+    const float* hr0 = h32 + q_y[q] * n_hm;
+    const float* hr1 = hr0 + n_hm;
+    float* yrow = Yt + (size_t)q * n_m_pad;
+    for (int k = lane; k < n_m_pad; k += 32) {
+      float y = 0.f;
+      if (k < n_m) {
+        const float t = kt_f[k];
+        const int xi = k_x[k];
+        const float n = ((1.f - t) * (1.f - u) * hr0[xi] + t * (1.f - u) * hr0[xi + 1] +
+                         (1.f - t) * u * hr1[xi] + t * u * hr1[xi + 1]) *
+                        kf_f[k];
+        const float aa = ka_f[k];
+        const float H = fast_exp2(-(aa * bb + 0.5f * bb * bb) * c2);
+        const float mu_rel = aa + bb;  // mu - (A0 + B0)
+        float scale = norm0f;
+        if (!(mu_rel > mu_sat_lo && mu_rel < mu_sat_hi)) {
+          const double mu = k_alpha[k] + q_beta[q];
+          scale = (float)(norm0 / mor_norm_slow((ll_lo - mu) * inv_s, (ll_hi - mu) * inv_s));
+        }
+        y = n * H * scale;
       }
-    }
-    for (int t = tid; t < G.n_t_pad; t += blockDim.x)
-      s32[G.f_delta + t] = t < G.n_t ? (float)(G.xl[t] - L0) : 0.f;
-    if (tid == 0) {
-      const double log2e = 1.4426950408889634;
-      s32[G.f_scal] = (float)(log2e * inv2s2);      // c1: F = exp2(-(d - a)^2 c1)
-      s32[G.f_scal + 1] = (float)(log2e / (sig * sig));  // c2: G = exp2(d b c2)
+      yrow[k] = y;
     }
   }
 }
@@ -433,8 +547,21 @@ struct y3b_engine {
   size_t prep_smem = 0, direct_smem = 0;
   size_t device_bytes = 0;
   int last_n = 0;
+  // stage timing (y3b_engine_profile)
+  bool prof = false;
+  int prof_evals = 0;
+  double prof_ms[4] = {0, 0, 0, 0};
+  struct Pending {
+    int stage;
+    cudaEvent_t a, b;
+  };
+  std::vector<Pending> pending;
   ~y3b_engine()
   {
+    for (auto& p : pending) {
+      cudaEventDestroy(p.a);
+      cudaEventDestroy(p.b);
+    }
     for (auto* g : gbufs) delete g;
     if (stream) cudaStreamDestroy(stream);
   }
@@ -467,6 +594,9 @@ build_grid(y3b_engine* e, int gi)
   g.n_t_pad = (g.n_t + kKChunk - 1) / kKChunk * kKChunk;
   g.n_cols = g.nI * g.n_z;
   g.n_cols_pad = (g.n_cols + 15) / 16 * 16;
+  g.nIc = std::max(1, std::min(g.nI, 256 / g.n_z));
+  g.n_bg = (g.nI + g.nIc - 1) / g.nIc;
+  g.ncp_c = (g.nIc * g.n_z + 15) / 16 * 16;
   g.lnm_lo = in.lnm_lo;
   g.lnm_hi = in.lnm_hi;
   g.zt_lo = in.zt_lo;
@@ -518,6 +648,17 @@ build_grid(y3b_engine* e, int gi)
   count_launch();
   Y3B_CUDA(cudaGetLastError());
   Y3B_CUDA(cudaStreamSynchronize(s));  // pz/pc are freed on return
+  g.uk_zindep = 1;
+  {
+    const int np = (int)e->plob_z.size();
+    for (int r = 0; r < 8 && g.uk_zindep; ++r)
+      for (int i = 1; i < np; ++i)
+        if (e->plob_coef[(size_t)r * np + i] != e->plob_coef[(size_t)r * np]) {
+          g.uk_zindep = 0;
+          break;
+        }
+    if ((size_t)g.nIc * g.n_t_pad * 4 > 16384) g.uk_zindep = 0;
+  }
   g.xm = b->xm.get();
   g.wm = b->wm.get();
   g.xz = b->xz.get();
@@ -530,6 +671,18 @@ build_grid(y3b_engine* e, int gi)
   g.omz = b->omz.get();
   // Scratch layouts.
   size_t o = 0;
+  g.o_scal = o;
+  o += 4;
+  g.o_kx = o;
+  o += pad2(g.n_m);
+  g.o_kt = o;
+  o += pad2(g.n_m);
+  g.o_kf = o;
+  o += pad2(g.n_m);
+  g.o_qy = o;
+  o += pad2(g.n_z);
+  g.o_qu = o;
+  o += pad2(g.n_z);
   g.o_cz = o;
   o += pad2(g.n_z);
   g.o_czs = o;
@@ -571,9 +724,9 @@ validate_grid(const y3b_grid& g)
     set_error("y3b_engine_create: grid needs n >= 2 nodes per axis and 1..8 bins per axis");
     return Y3B_ERR_INVALID;
   }
-  if (g.n_m > 1024 || g.n_z % 16 != 0 || g.n_lam_bins * g.n_z > kMaxCols || g.n_t > 4096) {
-    set_error("y3b_engine_create: unsupported grid (n_m <= 1024, n_z a multiple of 16, "
-              "n_lam_bins * n_z <= 512, n_t <= 4096)");
+  if (g.n_m > 1024 || g.n_z % 16 != 0 || g.n_z > 256 || g.n_t > 4096) {
+    set_error("y3b_engine_create: unsupported grid (n_m <= 1024, n_z a multiple of 16 and "
+              "<= 256, n_t <= 4096)");
     return Y3B_ERR_UNSUPPORTED;
   }
   if (!(g.lnm_hi > g.lnm_lo) || !(g.zt_hi > g.zt_lo) || !(g.lam_t_lo > 0.0) ||
@@ -622,9 +775,10 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
     }
   }
   if (cfg->n_hm < 2 || cfg->n_hz < 2 || cfg->n_dist < 2 || cfg->max_points < 1 ||
+      cfg->max_points > 65535 ||
       cfg->plob.n < 1 || !cfg->plob.z || !cfg->plob.coef ||
       (cfg->with_shear && (cfg->n_sci < 2 || cfg->shear.n_R < 1 || cfg->shear.n_R > kMaxR))) {
-    set_error("y3b_engine_create: invalid table shapes, capacity, P(lam_o|lam_t) table or "
+    set_error("y3b_engine_create: invalid table shapes, capacity (1..65535), P(lam_o|lam_t) table or "
               "shear options (n_sci >= 2 and 1 <= n_R <= 32 with shear)");
     return Y3B_ERR_INVALID;
   }
@@ -682,9 +836,7 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
     g.s64_stride = e->s64_stride;
     g.s32_stride = e->s32_stride;
   }
-  int nm_max = e->w_stride, nz_max = e->nz_max;
-  e->prep_smem = L.stride * 8 + (3 * nm_max + 4 * nz_max) * 8 + ((nm_max + 1) & ~1) * 4 +
-                 ((nz_max + 1) & ~1) * 4 + 8 * 8 + 64;
+  e->prep_smem = prep_smem_bytes(L.stride, L.n_hz, L.n_hm, e->w_stride, e->nz_max);
   e->direct_smem = ((size_t)e->nI_max * e->nt_max + e->nt_max) * 8;
   if (e->prep_smem > 200 * 1024 || e->direct_smem > 200 * 1024) {
     set_error("y3b_engine_create: per-point tables too large for shared-memory staging");
@@ -692,7 +844,7 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
   }
   for (int g = 0; g < n_grids; ++g) {
     const GridDev& gd = e->grids[g];
-    if (mixed_gemm_smem_bytes(gd.n_cols_pad, gd.n_z, gd.n_t_pad, gd.nJ) > 227 * 1024) {
+    if (mixed_gemm_smem_bytes(gd.ncp_c, gd.n_z, gd.n_t_pad, gd.nJ, gd.nIc) > 227 * 1024) {
       set_error("y3b_engine_create: grid %d needs more shared memory than one CTA has", g);
       return fail(Y3B_ERR_UNSUPPORTED);
     }
@@ -780,16 +932,44 @@ y3b_engine_device_bytes(const y3b_engine* e)
 namespace y3b {
 
 // Enqueue one evaluation on `s`.  grid_mask selects the grids present.
+// Records an event pair around one stage when profiling is on.
+struct StageTimer {
+  y3b_engine* e;
+  cudaStream_t s;
+  int stage;
+  cudaEvent_t a = nullptr;
+  StageTimer(y3b_engine* e_, cudaStream_t s_, int st) : e(e_), s(s_), stage(st)
+  {
+    if (e->prof && cudaEventCreate(&a) == cudaSuccess) cudaEventRecord(a, s);
+  }
+  ~StageTimer()
+  {
+    if (!a) return;
+    cudaEvent_t b;
+    if (cudaEventCreate(&b) == cudaSuccess) {
+      cudaEventRecord(b, s);
+      e->pending.push_back({stage, a, b});
+    } else {
+      cudaEventDestroy(a);
+    }
+  }
+};
+
 static int
 enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_tables,
         double* d_counts, double* d_shear, cudaStream_t s, int grid_mask)
 {
   Y3B_CUDA(cudaMemsetAsync(e->status.get(), 0, sizeof(int), s));
+  if (e->prof) ++e->prof_evals;
   PrepArgs pa{e->d_grids.get(), d_pts, d_tables, e->lay, prec == Y3B_MIXED, e->s64.get(),
-              e->s32.get(), e->status.get()};
-  prep_kernel<<<n, 256, e->prep_smem, s>>>(pa);
-  count_launch();
-  Y3B_CUDA(cudaGetLastError());
+              e->s32.get(), e->status.get(), grid_mask};
+  {
+    StageTimer t(e, s, 0);
+    prep_kernel<<<n, 256, e->prep_smem, s>>>(pa);
+    count_launch();
+    Y3B_CUDA(cudaGetLastError());
+  }
+  StageTimer* tc = new StageTimer(e, s, 1);
   if (prec == Y3B_FP64) {
     dim3 g1(e->nz_max, n);
     direct_main_kernel<<<g1, 256, e->direct_smem, s>>>(e->d_grids.get(), d_pts, e->s64.get(),
@@ -804,12 +984,19 @@ enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_t
     for (int g = 0; g < (int)e->grids.size(); ++g) {
       if (!((grid_mask >> g) & 1)) continue;
       MixedLaunch L{e->d_grids.get(), d_pts, g, n, &e->grids[g], e->s32.get(), e->W.get(),
-                    e->Wg.get(), e->w_stride, e->status.get(), s};
-      Y3B_TRY(launch_mixed_gemm(L));
+                    e->Wg.get(), e->w_stride, e->status.get(), s,
+                    e->cfg.with_shear && d_shear != nullptr};
+      int rc = launch_mixed_gemm(L);
+      if (rc) {
+        delete tc;
+        return rc;
+      }
     }
   }
+  delete tc;
   const bool shear = e->cfg.with_shear && d_shear;
   if (shear) {
+    StageTimer t(e, s, 2);
     long long warps = (long long)n * e->nI_max * e->shear.n_R * e->w_stride;
     long long blocks = (warps * 32 + 127) / 128;
     if (prec == Y3B_FP64)
@@ -823,12 +1010,15 @@ enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_t
     count_launch();
     Y3B_CUDA(cudaGetLastError());
   }
-  finalize_kernel<<<n, 256, 0, s>>>(e->d_grids.get(), d_pts, e->W.get(), e->Wg.get(),
-                                    shear ? e->Phi.get() : nullptr, e->w_stride, e->nB_max,
-                                    e->nI_max, e->shear.n_R, d_counts, shear ? d_shear : nullptr,
-                                    grid_mask);
-  count_launch();
-  Y3B_CUDA(cudaGetLastError());
+  {
+    StageTimer t(e, s, 3);
+    finalize_kernel<<<n, 256, 0, s>>>(e->d_grids.get(), d_pts, e->W.get(), e->Wg.get(),
+                                      shear ? e->Phi.get() : nullptr, e->w_stride, e->nB_max,
+                                      e->nI_max, e->shear.n_R, d_counts,
+                                      shear ? d_shear : nullptr, grid_mask);
+    count_launch();
+    Y3B_CUDA(cudaGetLastError());
+  }
   e->last_n = n;
   return Y3B_OK;
 }
@@ -922,5 +1112,42 @@ y3b_engine_weights(y3b_engine* e, int n, double* W)
   Y3B_CUDA(cudaStreamSynchronize(e->stream));
   Y3B_CUDA(cudaMemcpy(W, e->W.get(), (size_t)n * e->nB_max * e->w_stride * sizeof(double),
                       cudaMemcpyDeviceToHost));
+  return Y3B_OK;
+}
+
+extern "C" int
+y3b_engine_profile(y3b_engine* e, int enable)
+{
+  clear_error();
+  if (!e) return Y3B_ERR_INVALID;
+  if (enable) {
+    for (auto& p : e->pending) {
+      cudaEventDestroy(p.a);
+      cudaEventDestroy(p.b);
+    }
+    e->pending.clear();
+    for (double& v : e->prof_ms) v = 0.0;
+    e->prof_evals = 0;
+  }
+  e->prof = enable != 0;
+  return Y3B_OK;
+}
+
+extern "C" int
+y3b_engine_profile_read(y3b_engine* e, double* ms, int* n_evals)
+{
+  clear_error();
+  if (!e || !ms) return Y3B_ERR_INVALID;
+  for (auto& p : e->pending) {
+    Y3B_CUDA(cudaEventSynchronize(p.b));
+    float t = 0.f;
+    Y3B_CUDA(cudaEventElapsedTime(&t, p.a, p.b));
+    e->prof_ms[p.stage] += t;
+    cudaEventDestroy(p.a);
+    cudaEventDestroy(p.b);
+  }
+  e->pending.clear();
+  for (int i = 0; i < 4; ++i) ms[i] = e->prof_ms[i];
+  if (n_evals) *n_evals = e->prof_evals;
   return Y3B_OK;
 }

@@ -25,6 +25,10 @@ struct GridDev {
   int n_t_pad;     // lam_t nodes padded to kKChunk
   int n_cols;      // nI * n_z
   int n_cols_pad;  // padded to 16
+  int uk_zindep;   // P(lam_o | lam_t) has no z dependence: K_i(t, q) = K_i(t)
+  int nIc;         // richness bins per tensor-core CTA (nIc * n_z <= 256 columns)
+  int n_bg;        // bin groups = ceil(nI / nIc)
+  int ncp_c;       // TMEM columns per CTA: nIc * n_z padded to 16
   double lnm_lo, lnm_hi, zt_lo, zt_hi, ll_lo, ll_hi, sz0;
   const double* xm;   // [n_m]  lnM nodes
   const double* wm;
@@ -38,6 +42,7 @@ struct GridDev {
   const double* omz;  // [n_z] survey area Omega(z_q)
   // per-point scratch layout (offsets in elements of the scratch block)
   size_t s64_stride;  // doubles per point in the FP64 scratch
+  size_t o_scal, o_kx, o_kt, o_kf, o_qy, o_qu;  // A0/B0, HMF cells and weights
   size_t o_cz, o_czs, o_alpha, o_beta, o_P0, o_V;
   size_t s32_stride;  // floats per point in the FP32 scratch
   size_t f_a, f_b, f_delta, f_scal, f_Yt, f_CN, f_CG;
@@ -76,9 +81,10 @@ struct MixedLaunch {
   int w_stride;             // max n_m over grids
   int* status;
   cudaStream_t stream;
+  bool shear;               // also accumulate the Sigma_crit-weighted W^g
 };
 
 int launch_mixed_gemm(const MixedLaunch& L);
-size_t mixed_gemm_smem_bytes(int ncp, int n_z, int n_t_pad, int nJ);
+size_t mixed_gemm_smem_bytes(int ncp, int n_z, int n_t_pad, int nJ, int nIc);
 
 }  // namespace y3b

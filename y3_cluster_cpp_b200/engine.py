@@ -271,6 +271,17 @@ class Engine:
                                            C.c_void_p(shear_dev or None),
                                            C.c_void_p(stream or None)))
 
+    def profile(self, enable=True):
+        check(lib().y3b_engine_profile(self._h, 1 if enable else 0))
+
+    def profile_read(self):
+        """Accumulated stage milliseconds (prep, contraction, shear, final) and
+        the number of evaluations timed."""
+        ms = np.zeros(4)
+        n = C.c_int()
+        check(lib().y3b_engine_profile_read(self._h, ptr(ms), C.byref(n)))
+        return dict(prep=ms[0], contraction=ms[1], shear=ms[2], final=ms[3], evals=n.value)
+
     def sync(self, stream=0):
         check(lib().y3b_engine_sync(self._h, C.c_void_p(stream or None)))
 
