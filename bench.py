@@ -20,6 +20,7 @@ import argparse
 import ctypes as C
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -335,7 +336,8 @@ def run_ours(a):
             "fp64_batched": {"value": fp64_batched, "unit": UNIT},
             "speedup_vs_plain_fp64": value / world / plain_fp64,
             "roofline": {"bound": "tensor", "achieved": achieved_tf, "peak": peak_tf,
-                         "unit": "TFLOP/s", "frac": achieved_tf / peak_tf, "traffic": None,
+                         "unit": "TFLOP/s", "frac": achieved_tf / peak_tf,
+                         "traffic": ncu_traffic(a.density, B),
                          "kernel": "mixed_gemm_kernel",
                          "algorithmic_flops_per_launch": flops_alg,
                          "tensor_pipe_flops_per_launch": 3 * flops_alg,
@@ -353,6 +355,18 @@ def run_ours(a):
     eng.close()
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def ncu_traffic(density, points):
+    """DRAM bytes (read + write) of one contraction launch, from the committed
+    ncu capture of the 4x kernel, scaled by the points one launch processes
+    (each point reads its own operand vectors, so traffic grows with points)."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
+                        "mixed_gemm_kernel_counts_4x.md")
+    if density != 4 or not os.path.exists(path):
+        return None
+    m = re.search(r"traffic_bytes_per_point:\s*([0-9.]+)", open(path).read())
+    return float(m.group(1)) * points if m else None
 
 
 def main():
