@@ -119,6 +119,26 @@ int y3b_sel_function(const y3b_selfunc_config* cfg, const y3b_mor* mor,
                      const y3b_plob* plob, double* lnm_out, double* z_out,
                      double* S_out);
 
+/* The same S_stack producer for callers that cannot allocate device memory
+ * (no counterpart in the reference).  Such callers -- a sampler that has
+ * reserved all of its device memory up front in its own pool, or a host
+ * whose device allocations belong to another runtime's allocator and where
+ * a cudaMalloc would synchronise the device mid-run -- pass device buffers
+ * lnm_dev[n_lnm], z_dev[n_z], S_dev[n_bins][n_z][n_lnm]; the configuration
+ * and the projection table stay in host memory.  Scratch (GL nodes, edge and
+ * bin tables, the copied configuration) lives in one fixed file-scope device
+ * array of 43 KiB, so the call allocates nothing and rejects N_q > 1024,
+ * n_bins > 256 or more than 256 projection-table nodes with Y3B_ERR_INVALID.
+ * The array is shared by every call on a device and keeps the last call's
+ * contents: calls that overlap on the GPU (other streams or threads) race on
+ * it and must be serialised by the caller.  The first call on each device
+ * looks the array's device address up (cudaGetSymbolAddress); make that
+ * first call before any stream capture.  Asynchronous on `stream` (a
+ * cudaStream_t, NULL = the legacy default stream). */
+int y3b_sel_function_noalloc(const y3b_selfunc_config* cfg, const y3b_mor* mor,
+                             const y3b_plob* plob, double* lnm_dev, double* z_dev,
+                             double* S_dev, void* stream);
+
 /* ---------------------------------------------------------------------- */
 /* SelGLCore: fixed-GL z-contracted mass weights and the two evaluators.  */
 

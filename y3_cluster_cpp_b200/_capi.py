@@ -150,6 +150,8 @@ def _declare(L):
     L.y3b_engine_sync.argtypes = [VP, VP]
     L.y3b_engine_weights.argtypes = [VP, I, PD]
     L.y3b_selftest_wait_timeout.argtypes = [I]
+    L.y3b_sel_function_noalloc.argtypes = [C.POINTER(SelFuncConfig), C.POINTER(Mor),
+                                           C.POINTER(Plob), VP, VP, VP, VP]
     L.y3b_engine_profile.argtypes = [VP, I]
     L.y3b_engine_profile_read.argtypes = [VP, PD, PI]
 
@@ -181,5 +183,5 @@ EXPORTED = [
     "y3b_engine_table_stride", "y3b_engine_table_offsets", "y3b_engine_n_bins",
     "y3b_engine_device_bytes", "y3b_engine_eval", "y3b_engine_eval_device",
     "y3b_engine_sync", "y3b_engine_weights", "y3b_selftest_wait_timeout",
-    "y3b_engine_profile", "y3b_engine_profile_read",
+    "y3b_engine_profile", "y3b_engine_profile_read", "y3b_sel_function_noalloc",
 ]

@@ -812,3 +812,173 @@ y3b_nfw_mis(int which, int n, const double* r, const double* rmis, const double*
   Y3B_CUDA(cudaStreamSynchronize(s));
   return Y3B_OK;
 }
+
+// ===========================================================================
+// y3b_sel_function_noalloc: the S_stack producer for callers that cannot
+// allocate device memory.  Everything the kernel needs besides the caller's
+// output buffers (Gauss-Legendre nodes, the unique richness edges and their
+// bin pairing, the per-bin photo-z edges and widths, the projection table)
+// lives in one file-scope __device__ array of fixed size that every call
+// shares.
+#include <mutex>
+
+namespace y3b {
+
+constexpr int kNoAllocMaxQ = 1024;      // N_q
+constexpr int kNoAllocMaxBins = 256;    // bins
+constexpr int kNoAllocMaxPlob = 256;    // projection-table z nodes
+constexpr size_t kNoAllocScratchDoubles =
+  2 * kNoAllocMaxQ + kMaxEdges + 3 * kNoAllocMaxBins + 9 * kNoAllocMaxPlob +
+  (2 * kMaxPairs + kNoAllocMaxBins);    // last term holds the int tables
+static __device__ __align__(256) double g_selfunc_scratch[kNoAllocScratchDoubles];
+
+// Device address of g_selfunc_scratch, looked up once per device (host code
+// may not use the symbol itself: it names a host-side stand-in).
+static std::mutex g_scratch_mu;
+static void* g_scratch_addr[128];
+
+static int
+scratch_address(double** out)
+{
+  int dev = 0;
+  Y3B_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) {
+    set_error("y3b_sel_function_noalloc: device index %d out of range", dev);
+    return Y3B_ERR_INVALID;
+  }
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_selfunc_scratch);
+    if (e != cudaSuccess || !p) {
+      set_error("cudaGetSymbolAddress(g_selfunc_scratch): %s", cudaGetErrorString(e));
+      return Y3B_ERR_CUDA;
+    }
+    g_scratch_addr[dev] = p;
+  }
+  *out = static_cast<double*>(g_scratch_addr[dev]);
+  return Y3B_OK;
+}
+
+}  // namespace y3b
+
+extern "C" int
+y3b_sel_function_noalloc(const y3b_selfunc_config* cfg, const y3b_mor* mor,
+                         const y3b_plob* plob, double* lnm_dev, double* z_dev, double* S_dev,
+                         void* stream)
+{
+  using namespace y3b;
+  clear_error();
+  if (!cfg || !mor || !plob || !lnm_dev || !z_dev || !S_dev || !plob->z || !plob->coef ||
+      !cfg->lam_min || !cfg->lam_max || !cfg->zob_min || !cfg->zob_max || !cfg->sigma_z) {
+    set_error("y3b_sel_function_noalloc: null argument");
+    return Y3B_ERR_INVALID;
+  }
+  if (cfg->n_bins <= 0 || cfg->n_lnm <= 0 || cfg->n_z <= 0 || cfg->n_q <= 0 || plob->n < 1 ||
+      (mor->kind != Y3B_MOR_HOD && mor->kind != Y3B_MOR_LOGNORMAL)) {
+    set_error("y3b_sel_function_noalloc: invalid sizes or MOR kind");
+    return Y3B_ERR_INVALID;
+  }
+  if (cfg->n_q > kNoAllocMaxQ || cfg->n_bins > kNoAllocMaxBins || plob->n > kNoAllocMaxPlob) {
+    set_error("y3b_sel_function_noalloc: sizes exceed the fixed scratch (N_q <= %d, "
+              "n_bins <= %d, projection-table nodes <= %d); use y3b_sel_function",
+              kNoAllocMaxQ, kNoAllocMaxBins, kNoAllocMaxPlob);
+    return Y3B_ERR_INVALID;
+  }
+  Y3B_TRY(require_device());
+  const int nb = cfg->n_bins;
+  std::vector<double> edges;
+  for (int k = 0; k < nb; ++k) {
+    edges.push_back(cfg->lam_min[k]);
+    edges.push_back(cfg->lam_max[k]);
+  }
+  std::sort(edges.begin(), edges.end());
+  edges.erase(std::unique(edges.begin(), edges.end()), edges.end());
+  if ((int)edges.size() > kMaxEdges) {
+    set_error("y3b_sel_function_noalloc: more than %d unique richness edges", kMaxEdges);
+    return Y3B_ERR_UNSUPPORTED;
+  }
+  std::vector<int> ints;  // pair_lo | pair_hi | bin_pair
+  std::vector<int> plo, phi_, bin_pair(nb);
+  for (int k = 0; k < nb; ++k) {
+    int lo = int(std::lower_bound(edges.begin(), edges.end(), cfg->lam_min[k]) - edges.begin());
+    int hi = int(std::lower_bound(edges.begin(), edges.end(), cfg->lam_max[k]) - edges.begin());
+    int p = 0;
+    for (; p < (int)plo.size(); ++p)
+      if (plo[p] == lo && phi_[p] == hi) break;
+    if (p == (int)plo.size()) {
+      plo.push_back(lo);
+      phi_.push_back(hi);
+    }
+    bin_pair[k] = p;
+  }
+  if ((int)plo.size() > kMaxPairs) {
+    set_error("y3b_sel_function_noalloc: more than %d distinct richness bins", kMaxPairs);
+    return Y3B_ERR_UNSUPPORTED;
+  }
+  double* scratch = nullptr;
+  Y3B_TRY(scratch_address(&scratch));
+  // Scratch layout (doubles, then ints).
+  const int nq = cfg->n_q, np = plob->n;
+  double* d_glt = scratch;
+  double* d_glw = d_glt + nq;
+  double* d_edges = d_glw + nq;
+  double* d_zmin = d_edges + edges.size();
+  double* d_zmax = d_zmin + nb;
+  double* d_sz = d_zmax + nb;
+  double* d_pz = d_sz + nb;
+  double* d_pc = d_pz + np;
+  int* d_ints = reinterpret_cast<int*>(d_pc + 8 * (size_t)np);
+  int* d_plo = d_ints;
+  int* d_phi = d_plo + plo.size();
+  int* d_bp = d_phi + phi_.size();
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  auto put = [&](void* dst, const void* src, size_t bytes) {
+    return cuda_status(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s),
+                       "y3b_sel_function_noalloc: copy to scratch");
+  };
+  Y3B_TRY(put(d_edges, edges.data(), edges.size() * sizeof(double)));
+  Y3B_TRY(put(d_zmin, cfg->zob_min, nb * sizeof(double)));
+  Y3B_TRY(put(d_zmax, cfg->zob_max, nb * sizeof(double)));
+  Y3B_TRY(put(d_sz, cfg->sigma_z, nb * sizeof(double)));
+  Y3B_TRY(put(d_pz, plob->z, np * sizeof(double)));
+  Y3B_TRY(put(d_pc, plob->coef, 8 * (size_t)np * sizeof(double)));
+  Y3B_TRY(put(d_plo, plo.data(), plo.size() * sizeof(int)));
+  Y3B_TRY(put(d_phi, phi_.data(), phi_.size() * sizeof(int)));
+  Y3B_TRY(put(d_bp, bin_pair.data(), nb * sizeof(int)));
+  Y3B_TRY(gl_nodes_device(-1.0, 1.0, nq, d_glt, d_glw, s));
+
+  SelFuncArgs a;
+  a.n_lnm = cfg->n_lnm;
+  a.n_z = cfg->n_z;
+  a.n_q = nq;
+  a.n_bins = nb;
+  a.n_edges = (int)edges.size();
+  a.n_pairs = (int)plo.size();
+  a.lnm_low = cfg->lnm_low;
+  a.lnm_high = cfg->lnm_high;
+  a.zt_low = cfg->zt_low;
+  a.zt_high = cfg->zt_high;
+  a.mor_kind = mor->kind;
+  for (int i = 0; i < 8; ++i) a.mor[i] = mor->p[i];
+  a.n_plob = np;
+  a.plob_z = d_pz;
+  a.plob_coef = d_pc;
+  a.edges = d_edges;
+  a.pair_lo = d_plo;
+  a.pair_hi = d_phi;
+  a.bin_pair = d_bp;
+  a.zob_min = d_zmin;
+  a.zob_max = d_zmax;
+  a.sigma_z = d_sz;
+  a.gl_t = d_glt;
+  a.gl_w = d_glw;
+  a.lnm_out = lnm_dev;
+  a.z_out = z_dev;
+  a.S_out = S_dev;
+  long long warps = (long long)cfg->n_lnm * cfg->n_z;
+  int blocks = (int)((warps * 32 + 127) / 128);
+  sel_function_kernel<<<blocks, 128, 0, s>>>(a);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "sel_function_kernel (noalloc)");
+}
