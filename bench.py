@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--density", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=2, help="points in the CPU baseline sample")
+    ap.add_argument("--serve-requests", type=int, default=256,
+                    help="requests in the serving stream (0: skip the serving measurement)")
     return ap.parse_args()
 
 
@@ -176,6 +178,78 @@ def run_reference(a):
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def serving_run(a, rank, dev):
+    """Serving workload: a Poisson request stream (mean gap 2 ms) of requests
+    of 1..1024 points (log-uniform), points from the batched-config prior at
+    mixed 1x/2x/4x densities, each with its own tables; counts at 1e-4.
+    Runs the stream through the continuous-batching server and, for
+    comparison, the plain per-request FP64 form (each request evaluated by
+    itself in arrival order, queueing included).  Latency = completion -
+    arrival."""
+    import numpy as np
+    import torch
+
+    from y3_cluster_cpp_b200 import _capi, engine, serve, synthetic
+
+    n_req = a.serve_requests
+    dens = (1, 2, 4)
+    grids = [synthetic.grid(d) for d in dens]
+    gi = {d: i for i, d in enumerate(dens)}
+    pool = synthetic.walkers(96, seed=2 + 1000 * rank, densities=dens)
+    t0 = pool[0].tables
+    pz, pc = synthetic.plob_baseline()
+    eng = engine.Engine(grids, len(t0["hmf_m_h"]), len(t0["hmf_z"]), len(t0["dist_z"]),
+                        (pz, pc), max_points=2048, n_sci=len(t0["sci_z"]))
+    tab_pool = eng.pack(pool)
+    sizes = serve.request_sizes(n_req, seed=2 + rank)
+    arrivals = serve.poisson_arrivals(n_req, 0.002, seed=2 + rank)
+    rng = np.random.default_rng(3 + rank)
+    total = int(sizes.sum())
+    tables_h = torch.empty((total, eng.stride), dtype=torch.float64, pin_memory=True).numpy()
+    reqs, o = [], 0
+    for n in sizes:
+        idx = rng.integers(0, len(pool), n)
+        tables_h[o:o + n] = tab_pool[idx]
+        pts = eng.points_array([pool[i] for i in idx], grid_of=lambda p: gi[p.density])
+        reqs.append((pts, tables_h[o:o + n]))
+        o += n
+
+    # plain per-request FP64 GPU form, in arrival order (one request at a time)
+    lib = engine.lib()
+    fp64_counts, finish, lat64 = [], 0.0, []
+    for (pts, tab), t_arr in zip(reqs, arrivals):
+        out = np.empty((len(pts), eng.n_bins))
+        t_s = time.perf_counter()
+        engine.check(lib.y3b_engine_eval(eng.handle, engine.FP64, len(pts), pts,
+                                         _capi.ptr(tab), _capi.ptr(out), None))
+        svc = time.perf_counter() - t_s
+        finish = max(finish, t_arr) + svc
+        lat64.append(finish - t_arr)
+        fp64_counts.append(out)
+    fp64_tp = total / finish
+
+    # warm the server path once, then the timed stream
+    with serve.Server(eng, pool_points=8192, max_batch=2048, precision=engine.MIXED) as srv:
+        srv.wait(srv.submit(*reqs[0]))
+        s0 = srv.stats()
+        run = serve.run_stream(srv, reqs, arrivals)
+        s1 = srv.stats()
+    eng.close()
+    err = max(float(np.max(np.abs(r["counts"] / c - 1)))
+              for r, c in zip(run["results"], fp64_counts))
+    launches = s1["launches"] - s0["launches"]
+    return {"requests": n_req, "points": total,
+            "arrivals": "Poisson, mean gap 2 ms", "sizes": "round(exp(U[0, ln 1024]))",
+            "densities": "1x/2x/4x in thirds per point", "tables": "per point, pinned host",
+            "throughput": total / run["wall_s"], "unit": UNIT,
+            **serve.percentiles_ms(run["latency_s"]),
+            "launches": launches, "mean_launch_points": total / max(launches, 1),
+            "max_launch_points": s1["max_launch_points"],
+            "max_rel_err_vs_fp64": err,
+            "fp64_per_request": {"throughput": fp64_tp, "unit": UNIT,
+                                 **serve.percentiles_ms(np.asarray(lat64))}}
 
 
 def run_ours(a):
@@ -314,6 +388,11 @@ def run_ours(a):
     h2d = B * (C.sizeof(_capi.Point) + eng.stride * 8)
     d2h = B * n_bins * 8
 
+    eng.close()
+    serving = None
+    if a.serve_requests > 0:
+        serving = serving_run(a, rank, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline(a.density, a.cpu_sample)
@@ -349,10 +428,11 @@ def run_ours(a):
             "gpu_launches": launches,
             "clocks": clk,
         }
+        if serving is not None:
+            line["serving"] = serving
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
-    eng.close()
     if world > 1:
         torch.distributed.destroy_process_group()
 

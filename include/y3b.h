@@ -272,6 +272,15 @@ int y3b_engine_eval(y3b_engine* e, int precision, int n,
 int y3b_engine_eval_device(y3b_engine* e, int precision, int n,
                            const y3b_point* pts_dev, const double* tables_dev,
                            double* counts_dev, double* shear_dev, void* stream);
+/* As y3b_engine_eval_device, but point i reads its table block from a
+ * resident pool: pool_dev + slot_dev[i] * y3b_engine_table_stride(e)
+ * doubles (device pointers; the pool 16-byte aligned).  Lets tables stay on
+ * the device across evaluations (the request server keeps them there).
+ * Points are not checked on the device: their grid must be valid. */
+int y3b_engine_eval_pooled(y3b_engine* e, int precision, int n,
+                           const y3b_point* pts_dev, const double* pool_dev,
+                           const int* slot_dev, double* counts_dev,
+                           double* shear_dev, void* stream);
 /* Wait for the engine's work on `stream` and report device-side errors. */
 int y3b_engine_sync(y3b_engine* e, void* stream);
 /* Optional: the mass weights W_b(lnM_k) of the last eval ([n][n_bins][n_m]
@@ -291,6 +300,81 @@ int y3b_engine_profile_read(y3b_engine* e, double* ms, int* n_evals);
  * barrier nobody arrives at for ~`usec` microseconds and must come back
  * with Y3B_ERR_TIMEOUT (the context stays usable). */
 int y3b_selftest_wait_timeout(int usec);
+
+/* ---------------------------------------------------------------------- */
+/* Request server: continuous batching of likelihood-evaluation requests   */
+/* from a running sampler over one engine.  The reference evaluates one     */
+/* point per CosmoSIS execute() call and has no counterpart.                */
+/*                                                                          */
+/* A request is n points with their own table blocks (host memory, packed   */
+/* as for y3b_engine_eval).  Its tables are copied once into a device table */
+/* pool when the pool has room (admission in arrival order, bounded by the  */
+/* HBM budget); every launch evaluates up to max_batch points drawn from    */
+/* all admitted requests, oldest first, splitting large requests across     */
+/* launches, with up to max_inflight launches queued on the device.  The    */
+/* server's worker thread owns the engine: do not evaluate on that engine   */
+/* while the server exists.                                                 */
+
+typedef struct {
+  int pool_points;     /* table-pool slots, one per resident point (0: what the
+                          budget allows, at most 65536) */
+  size_t hbm_budget;   /* bytes for engine + launch buffers + pool (0: 150 GiB) */
+  int max_batch;       /* points per launch (0: the engine's max_points) */
+  int precision;       /* Y3B_MIXED or Y3B_FP64 */
+  int with_shear;      /* also return DeltaSigma (engine created with_shear) */
+  int max_inflight;    /* launches queued on the device at once, 1..4 (0: 2) */
+} y3b_server_config;
+
+typedef struct {
+  long long requests_done, points_done, launches;
+  int max_launch_points;
+  int pool_points, pool_free_points;
+  int waiting;         /* submitted, not yet admitted to the pool */
+  int unscheduled;     /* admitted, with points not yet in a launch */
+} y3b_server_stats;
+
+typedef struct y3b_server y3b_server;
+
+int y3b_server_create(y3b_engine* e, const y3b_server_config* cfg,
+                      y3b_server** out);
+/* Queues a request and returns at once with its ticket.  pts, tables,
+ * counts ([n][n_bins]) and shear ([n][n_bins][n_R], with_shear only) are
+ * host buffers that must stay valid until y3b_server_wait has returned for
+ * the ticket; pinned tables upload fastest.  Points and their distance
+ * tables are checked here (Y3B_ERR_INVALID / Y3B_ERR_DOMAIN); a request
+ * larger than the whole pool gets Y3B_ERR_BUDGET. */
+int y3b_server_submit(y3b_server* s, int n, const y3b_point* pts,
+                      const double* tables, double* counts, double* shear,
+                      long long* ticket);
+/* Blocks until the request is complete (timeout_s < 0: no limit) and
+ * returns its status; Y3B_ERR_TIMEOUT leaves it running and the ticket
+ * valid.  latency_s (optional) = completion - submission.  One waiter per
+ * ticket; a ticket is collected by the wait that returns its status. */
+int y3b_server_wait(y3b_server* s, long long ticket, double timeout_s,
+                    double* latency_s);
+int y3b_server_stats_read(y3b_server* s, y3b_server_stats* out);
+/* Finishes every submitted request, then frees the server (not the engine). */
+void y3b_server_destroy(y3b_server* s);
+
+/* The server's scheduling policy on its own (host only, no device): FIFO
+ * admission of requests into contiguous runs of pool slots, launches of up
+ * to max_batch points, slots released when a request completes.  For
+ * capacity planning and tests of the policy. */
+typedef struct y3b_planner y3b_planner;
+int y3b_planner_create(int pool_points, int max_batch, y3b_planner** out);
+void y3b_planner_destroy(y3b_planner* p);
+int y3b_planner_submit(y3b_planner* p, long long id, int n_points);
+/* Admits waiting requests in order while they fit: ids[i] gets slot0[i]. */
+int y3b_planner_admit(y3b_planner* p, long long* ids, int* slot0, int cap,
+                      int* n_out);
+/* Next launch: up to cap chunks (request id, first point, count, slot). */
+int y3b_planner_next_batch(y3b_planner* p, long long* ids, int* first,
+                           int* count, int* slot, int cap, int* n_chunks,
+                           int* n_points);
+/* count points of request id came back; *finished = 1 when it completed. */
+int y3b_planner_complete(y3b_planner* p, long long id, int count,
+                         int* finished);
+int y3b_planner_free_points(const y3b_planner* p);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -101,6 +101,17 @@ class Point(C.Structure):
                 ("grid", I), ("reserved", I)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("pool_points", I), ("hbm_budget", C.c_size_t), ("max_batch", I),
+                ("precision", I), ("with_shear", I), ("max_inflight", I)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("requests_done", C.c_longlong), ("points_done", C.c_longlong),
+                ("launches", C.c_longlong), ("max_launch_points", I), ("pool_points", I),
+                ("pool_free_points", I), ("waiting", I), ("unscheduled", I)]
+
+
 _lib = None
 
 
@@ -152,6 +163,22 @@ def _declare(L):
     L.y3b_selftest_wait_timeout.argtypes = [I]
     L.y3b_sel_function_noalloc.argtypes = [C.POINTER(SelFuncConfig), C.POINTER(Mor),
                                            C.POINTER(Plob), VP, VP, VP, VP]
+    L.y3b_engine_eval_pooled.argtypes = [VP, I, I, VP, VP, VP, VP, VP, VP]
+    L.y3b_server_create.argtypes = [VP, C.POINTER(ServerConfig), C.POINTER(VP)]
+    L.y3b_server_submit.argtypes = [VP, I, VP, VP, VP, VP, C.POINTER(C.c_longlong)]
+    L.y3b_server_wait.argtypes = [VP, C.c_longlong, D, PD]
+    L.y3b_server_stats_read.argtypes = [VP, C.POINTER(ServerStats)]
+    L.y3b_server_destroy.argtypes = [VP]
+    L.y3b_server_destroy.restype = None
+    PLL = C.POINTER(C.c_longlong)
+    L.y3b_planner_create.argtypes = [I, I, C.POINTER(VP)]
+    L.y3b_planner_destroy.argtypes = [VP]
+    L.y3b_planner_destroy.restype = None
+    L.y3b_planner_submit.argtypes = [VP, C.c_longlong, I]
+    L.y3b_planner_admit.argtypes = [VP, PLL, PI, I, PI]
+    L.y3b_planner_next_batch.argtypes = [VP, PLL, PI, PI, PI, I, PI, PI]
+    L.y3b_planner_complete.argtypes = [VP, C.c_longlong, I, PI]
+    L.y3b_planner_free_points.argtypes = [VP]
     L.y3b_engine_profile.argtypes = [VP, I]
     L.y3b_engine_profile_read.argtypes = [VP, PD, PI]
 
@@ -184,4 +211,8 @@ EXPORTED = [
     "y3b_engine_device_bytes", "y3b_engine_eval", "y3b_engine_eval_device",
     "y3b_engine_sync", "y3b_engine_weights", "y3b_selftest_wait_timeout",
     "y3b_engine_profile", "y3b_engine_profile_read", "y3b_sel_function_noalloc",
+    "y3b_engine_eval_pooled", "y3b_server_create", "y3b_server_submit", "y3b_server_wait",
+    "y3b_server_stats_read", "y3b_server_destroy", "y3b_planner_create",
+    "y3b_planner_destroy", "y3b_planner_submit", "y3b_planner_admit",
+    "y3b_planner_next_batch", "y3b_planner_complete", "y3b_planner_free_points",
 ]

@@ -16,6 +16,7 @@
 //     (mixed_gemm.cu) with FP32 integrands and FP64 final sums.
 // Reductions are fixed-order trees; reruns are bit-identical.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -86,6 +87,7 @@ struct PrepArgs {
   const GridDev* grids;
   const PointDev* pts;
   const double* tables;
+  const int* slot;  // table block of point p: tables + slot[p] * stride (null: p)
   TableLayout lay;
   int mixed;
   double* s64;
@@ -161,7 +163,7 @@ prep_kernel(PrepArgs a)
   __shared__ int timed_out;
   __shared__ double red[2];
 
-  const double* src = a.tables + (size_t)p * L.stride;
+  const double* src = a.tables + (size_t)(a.slot ? a.slot[p] : p) * L.stride;
   const uint32_t bytes = (uint32_t)(L.stride * sizeof(double));
   if (tid == 0) {
     timed_out = 0;
@@ -547,6 +549,7 @@ struct y3b_engine {
   size_t prep_smem = 0, direct_smem = 0;
   size_t device_bytes = 0;
   int last_n = 0;
+  std::vector<std::array<double, 2>> zt_node_range;  // per grid: min, max z_t node
   // stage timing (y3b_engine_profile)
   bool prof = false;
   int prof_evals = 0;
@@ -620,6 +623,14 @@ build_grid(y3b_engine* e, int gi)
   Y3B_TRY(b->omz.alloc(g.n_z));
   Y3B_TRY(gl_nodes_device(in.lnm_lo, in.lnm_hi, g.n_m, b->xm.get(), b->wm.get(), s));
   Y3B_TRY(gl_nodes_device(in.zt_lo, in.zt_hi, g.n_z, b->xz.get(), b->wz.get(), s));
+  {
+    std::vector<double> xz(g.n_z);
+    Y3B_CUDA(cudaMemcpyAsync(xz.data(), b->xz.get(), g.n_z * sizeof(double),
+                             cudaMemcpyDeviceToHost, s));
+    Y3B_CUDA(cudaStreamSynchronize(s));
+    e->zt_node_range[gi][0] = *std::min_element(xz.begin(), xz.end());
+    e->zt_node_range[gi][1] = *std::max_element(xz.begin(), xz.end());
+  }
   Y3B_TRY(gl_nodes_device(g.ll_lo, g.ll_hi, g.n_t, b->xl.get(), b->wl.get(), s));
   for (int i = 0; i < g.nI; ++i)
     Y3B_TRY(gl_nodes_device(in.lam_edges[i], in.lam_edges[i + 1], g.n_o, b->lo_x.get() + i * g.n_o,
@@ -799,6 +810,7 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
   e->cfg.plob.coef = e->plob_coef.data();
   e->grids_in.assign(grids, grids + n_grids);
   e->grids.resize(n_grids);
+  e->zt_node_range.resize(n_grids);
   for (int g = 0; g < n_grids; ++g) e->gbufs.push_back(new (std::nothrow) GridBufs());
   int rc = cuda_status(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking),
                        "cudaStreamCreate");
@@ -957,12 +969,12 @@ struct StageTimer {
 
 static int
 enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_tables,
-        double* d_counts, double* d_shear, cudaStream_t s, int grid_mask)
+        const int* d_slot, double* d_counts, double* d_shear, cudaStream_t s, int grid_mask)
 {
   Y3B_CUDA(cudaMemsetAsync(e->status.get(), 0, sizeof(int), s));
   if (e->prof) ++e->prof_evals;
-  PrepArgs pa{e->d_grids.get(), d_pts, d_tables, e->lay, prec == Y3B_MIXED, e->s64.get(),
-              e->s32.get(), e->status.get(), grid_mask};
+  PrepArgs pa{e->d_grids.get(), d_pts, d_tables, d_slot, e->lay, prec == Y3B_MIXED,
+              e->s64.get(), e->s32.get(), e->status.get(), grid_mask};
   {
     StageTimer t(e, s, 0);
     prep_kernel<<<n, 256, e->prep_smem, s>>>(pa);
@@ -1044,7 +1056,84 @@ y3b_engine_eval_device(y3b_engine* e, int precision, int n, const y3b_point* pts
   cudaStream_t s = stream ? (cudaStream_t)stream : e->stream;
   int mask = (1 << (int)e->grids.size()) - 1;
   return enqueue(e, precision, n, reinterpret_cast<const PointDev*>(pts_dev), tables_dev,
-                 counts_dev, shear_dev, s, mask);
+                 nullptr, counts_dev, shear_dev, s, mask);
+}
+
+extern "C" int
+y3b_engine_eval_pooled(y3b_engine* e, int precision, int n, const y3b_point* pts_dev,
+                       const double* pool_dev, const int* slot_dev, double* counts_dev,
+                       double* shear_dev, void* stream)
+{
+  clear_error();
+  if (!e || n < 1 || n > e->cfg.max_points || !pts_dev || !pool_dev || !slot_dev ||
+      !counts_dev || (precision != Y3B_FP64 && precision != Y3B_MIXED)) {
+    set_error("y3b_engine_eval_pooled: invalid arguments (1 <= n <= max_points)");
+    return Y3B_ERR_INVALID;
+  }
+  if (((uintptr_t)pool_dev & 15u) != 0) {
+    set_error("y3b_engine_eval_pooled: the table pool must be 16-byte aligned");
+    return Y3B_ERR_INVALID;
+  }
+  cudaStream_t s = stream ? (cudaStream_t)stream : e->stream;
+  int mask = (1 << (int)e->grids.size()) - 1;
+  return enqueue(e, precision, n, reinterpret_cast<const PointDev*>(pts_dev), pool_dev,
+                 slot_dev, counts_dev, shear_dev, s, mask);
+}
+
+int
+y3b::engine_check_points(const y3b_engine* e, int n, const y3b_point* pts, int* mask)
+{
+  *mask = 0;
+  for (int i = 0; i < n; ++i) {
+    const y3b_point& p = pts[i];
+    if (p.grid < 0 || p.grid >= (int)e->grids.size()) {
+      set_error("point %d has grid %d outside [0, %d)", i, p.grid, (int)e->grids.size());
+      return Y3B_ERR_INVALID;
+    }
+    if (!(p.sigma > 0.0) || !(p.Mpiv > 0.0) || !(p.cosmo.om - p.cosmo.onu > 0.0) ||
+        !(p.cosmo.h0 > 0.0)) {
+      set_error("point %d has non-positive sigma, Mpiv, h0 or omega_M - omega_nu", i);
+      return Y3B_ERR_INVALID;
+    }
+    *mask |= 1 << p.grid;
+  }
+  return Y3B_OK;
+}
+
+int
+y3b::engine_check_tables(const y3b_engine* e, int n, const y3b_point* pts, const double* tables)
+{
+  const size_t st = e->lay.stride;
+  const int nd = e->lay.n_dist;
+  for (int i = 0; i < n; ++i) {
+    const double* dz = tables + (size_t)i * st + e->lay.off[3];
+    const auto& zr = e->zt_node_range[pts[i].grid];
+    if (!(dz[0] <= zr[0] && zr[1] <= dz[nd - 1])) {
+      set_error("point %d: distances/z [%g, %g] does not cover the z_t nodes [%g, %g] of its "
+                "grid", i, dz[0], dz[nd - 1], zr[0], zr[1]);
+      return Y3B_ERR_DOMAIN;
+    }
+  }
+  return Y3B_OK;
+}
+
+void
+y3b::engine_info(const y3b_engine* e, EngineInfo* out)
+{
+  out->n_grids = (int)e->grids.size();
+  out->n_bins = e->nB_max;
+  out->n_R = e->cfg.with_shear ? e->shear.n_R : 0;
+  out->with_shear = e->cfg.with_shear;
+  out->max_points = e->cfg.max_points;
+  out->stride = e->lay.stride;
+  out->device_bytes = e->device_bytes;
+}
+
+int
+y3b::engine_status_to_host(y3b_engine* e, int* host, cudaStream_t s)
+{
+  Y3B_CUDA(cudaMemcpyAsync(host, e->status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+  return Y3B_OK;
 }
 
 extern "C" int
@@ -1070,27 +1159,13 @@ y3b_engine_eval(y3b_engine* e, int precision, int n, const y3b_point* pts,
     return Y3B_ERR_INVALID;
   }
   int mask = 0;
-  for (int i = 0; i < n; ++i) {
-    const y3b_point& p = pts[i];
-    if (p.grid < 0 || p.grid >= (int)e->grids.size()) {
-      set_error("y3b_engine_eval: point %d has grid %d outside [0, %d)", i, p.grid,
-                (int)e->grids.size());
-      return Y3B_ERR_INVALID;
-    }
-    if (!(p.sigma > 0.0) || !(p.Mpiv > 0.0) || !(p.cosmo.om - p.cosmo.onu > 0.0) ||
-        !(p.cosmo.h0 > 0.0)) {
-      set_error("y3b_engine_eval: point %d has non-positive sigma, Mpiv, h0 or omega_M - omega_nu",
-                i);
-      return Y3B_ERR_INVALID;
-    }
-    mask |= 1 << p.grid;
-  }
+  Y3B_TRY(y3b::engine_check_points(e, n, pts, &mask));
   cudaStream_t s = e->stream;
   Y3B_CUDA(cudaMemcpyAsync(e->pts.get(), pts, n * sizeof(y3b_point), cudaMemcpyHostToDevice, s));
   Y3B_CUDA(cudaMemcpyAsync(e->tables.get(), tables, n * e->lay.stride * sizeof(double),
                            cudaMemcpyHostToDevice, s));
   const bool want_shear = e->cfg.with_shear && shear;
-  Y3B_TRY(enqueue(e, precision, n, e->pts.get(), e->tables.get(), e->counts.get(),
+  Y3B_TRY(enqueue(e, precision, n, e->pts.get(), e->tables.get(), nullptr, e->counts.get(),
                   want_shear ? e->shear_out.get() : nullptr, s, mask));
   Y3B_CUDA(cudaMemcpyAsync(counts, e->counts.get(), (size_t)n * e->nB_max * sizeof(double),
                            cudaMemcpyDeviceToHost, s));

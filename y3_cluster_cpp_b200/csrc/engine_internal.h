@@ -10,6 +10,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "../../include/y3b.h"
+
 namespace y3b {
 
 constexpr int kMaxLamBins = 8;
@@ -85,6 +87,25 @@ struct MixedLaunch {
 };
 
 int launch_mixed_gemm(const MixedLaunch& L);
+
+// Enqueues a copy of the engine's device status word (the result of the
+// device-side checks of the evaluations enqueued before it on `s`) to `host`.
+int engine_status_to_host(::y3b_engine* e, int* host, cudaStream_t s);
+
+struct EngineInfo {
+  int n_grids, n_bins, n_R, with_shear, max_points;
+  size_t stride;        // doubles per point's table block
+  size_t device_bytes;  // what the engine holds
+};
+void engine_info(const ::y3b_engine* e, EngineInfo* out);
+
+// Host-side checks of points (grid index, positive sigma, Mpiv, h0 and
+// omega_M - omega_nu); sets the error message.  *mask gets the grids used.
+int engine_check_points(const ::y3b_engine* e, int n, const y3b_point* pts, int* mask);
+
+// Host-side copy of the device domain check: every z_t node of a point's grid
+// must lie inside its distances/z table (host tables).  Y3B_ERR_DOMAIN if not.
+int engine_check_tables(const ::y3b_engine* e, int n, const y3b_point* pts, const double* tables);
 size_t mixed_gemm_smem_bytes(int ncp, int n_z, int n_t_pad, int nJ, int nIc);
 
 }  // namespace y3b
