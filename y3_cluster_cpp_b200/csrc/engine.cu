@@ -144,7 +144,10 @@ prep_kernel(PrepArgs a)
   extern __shared__ __align__(16) double psh[];
   const int p = blockIdx.x;
   const PointDev pt = a.pts[p];
-  if (!((a.grid_mask >> pt.grid) & 1)) return;
+  if (!grid_in_mask(a.grid_mask, pt.grid)) {
+    if (threadIdx.x == 0) set_err(a.status, kDevShape);  // no such grid
+    return;
+  }
   const GridDev* __restrict__ Gp = a.grids + pt.grid;
   const int n_m = Gp->n_m, n_z = Gp->n_z, n_m_pad = Gp->n_m_pad, tid = threadIdx.x;
   const TableLayout& L = a.lay;
@@ -388,7 +391,7 @@ direct_main_kernel(const GridDev* grids, const PointDev* pts, double* s64all, in
   extern __shared__ double dsh[];
   const int p = blockIdx.y, q = blockIdx.x;
   const PointDev pt = pts[p];
-  if (!((grid_mask >> pt.grid) & 1)) return;
+  if (!grid_in_mask(grid_mask, pt.grid)) return;
   const GridDev& G = grids[pt.grid];
   if (q >= G.n_z) return;
   const int n_t = G.n_t, nI = G.nI;
@@ -425,7 +428,7 @@ direct_wreduce_kernel(const GridDev* grids, const PointDev* pts, const double* s
 {
   const int p = blockIdx.x;
   const PointDev pt = pts[p];
-  if (!((grid_mask >> pt.grid) & 1)) return;
+  if (!grid_in_mask(grid_mask, pt.grid)) return;
   const GridDev& G = grids[pt.grid];
   const double* s64 = s64all + (size_t)p * G.s64_stride;
   for (int k = threadIdx.x; k < G.n_m; k += blockDim.x) {
@@ -470,7 +473,7 @@ shear_phi_kernel(const GridDev* grids, const PointDev* pts, int n_points, int w_
   const int iR = (int)(r % sh.n_R);
   const int i = (int)(r / sh.n_R);
   const PointDev pt = pts[p];
-  if (!((grid_mask >> pt.grid) & 1)) return;
+  if (!grid_in_mask(grid_mask, pt.grid)) return;
   const GridDev& G = grids[pt.grid];
   if (i >= G.nI || k >= G.n_m) return;
   const double lnM = G.xm[k];
@@ -497,7 +500,7 @@ finalize_kernel(const GridDev* grids, const PointDev* pts, const double* W, cons
 {
   const int p = blockIdx.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const PointDev pt = pts[p];
-  if (!((grid_mask >> pt.grid) & 1)) return;
+  if (!grid_in_mask(grid_mask, pt.grid)) return;
   const GridDev& G = grids[pt.grid];
   const int nw = blockDim.x >> 5;
   for (int b = warp; b < G.nB; b += nw) {
@@ -543,7 +546,9 @@ struct y3b_engine {
   y3b::DevBuf<y3b::PointDev> pts;
   y3b::DevBuf<double> tables, s64, W, Wg, Phi, counts, shear_out;
   y3b::DevBuf<float> s32;
-  y3b::DevBuf<int> status;
+  y3b::DevBuf<int> status, order, tile_start, tile_list;
+  int max_tiles_pp = 0;
+  y3b::ContractShape cshape{};
   size_t s64_stride = 0, s32_stride = 0;
   int w_stride = 0, nB_max = 0, nI_max = 0, nz_max = 0, nt_max = 0;
   size_t prep_smem = 0, direct_smem = 0;
@@ -600,6 +605,7 @@ build_grid(y3b_engine* e, int gi)
   g.nIc = std::max(1, std::min(g.nI, 256 / g.n_z));
   g.n_bg = (g.nI + g.nIc - 1) / g.nIc;
   g.ncp_c = (g.nIc * g.n_z + 15) / 16 * 16;
+  g.tiles_pp = (g.n_m_pad / kGemmRows) * g.n_bg;
   g.lnm_lo = in.lnm_lo;
   g.lnm_hi = in.lnm_hi;
   g.zt_lo = in.zt_lo;
@@ -668,7 +674,6 @@ build_grid(y3b_engine* e, int gi)
           g.uk_zindep = 0;
           break;
         }
-    if ((size_t)g.nIc * g.n_t_pad * 4 > 16384) g.uk_zindep = 0;
   }
   g.xm = b->xm.get();
   g.wm = b->wm.get();
@@ -854,12 +859,32 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
     set_error("y3b_engine_create: per-point tables too large for shared-memory staging");
     return fail(Y3B_ERR_UNSUPPORTED);
   }
-  for (int g = 0; g < n_grids; ++g) {
-    const GridDev& gd = e->grids[g];
-    if (mixed_gemm_smem_bytes(gd.ncp_c, gd.n_z, gd.n_t_pad, gd.nJ, gd.nIc) > 227 * 1024) {
-      set_error("y3b_engine_create: grid %d needs more shared memory than one CTA has", g);
-      return fail(Y3B_ERR_UNSUPPORTED);
+  {
+    ContractShape& c = e->cshape;
+    c.nJ = e->grids[0].nJ;
+    c.nz_max = e->nz_max;
+    c.ntp_max = 0;
+    c.uk_max = 0;
+    for (const auto& g : e->grids) {
+      c.ntp_max = std::max(c.ntp_max, g.n_t_pad);
+      if (g.uk_zindep) c.uk_max = std::max(c.uk_max, g.nIc * g.n_t_pad);
     }
+    if (c.uk_max > 4096) c.uk_max = 0;  // larger per-tile slices are read from global memory
+  }
+  if (contract_stages(e->cshape) == 0) {
+    set_error("y3b_engine_create: the contraction needs more shared memory than one CTA has");
+    return fail(Y3B_ERR_UNSUPPORTED);
+  }
+  // Contraction schedule: grids with the most expensive tiles (lam_t steps x
+  // accumulator columns) first, ties by index.
+  {
+    std::vector<int> idx(n_grids);
+    for (int g = 0; g < n_grids; ++g) idx[g] = g;
+    auto cost = [&](int g) { return (long long)e->grids[g].n_t_pad * e->grids[g].ncp_c; };
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return cost(a) > cost(b); });
+    for (int r = 0; r < n_grids; ++r) e->grids[idx[r]].cost_rank = r;
+    e->max_tiles_pp = 0;
+    for (const auto& g : e->grids) e->max_tiles_pp = std::max(e->max_tiles_pp, g.tiles_pp);
   }
   // Shear options.
   ShearDev& sh = e->shear;
@@ -880,7 +905,8 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
   const size_t N = cfg->max_points;
   size_t bytes = N * sizeof(PointDev) + N * L.stride * 8 + N * e->s64_stride * 8 +
                  N * e->s32_stride * 4 + 2 * N * e->nB_max * (size_t)e->w_stride * 8 +
-                 N * e->nB_max * 8;
+                 N * e->nB_max * 8 + (2 * N + 1) * sizeof(int) +
+                 N * (size_t)e->max_tiles_pp * sizeof(int);
   if (cfg->with_shear)
     bytes += N * (size_t)e->nI_max * sh.n_R * e->w_stride * 8 + N * e->nB_max * sh.n_R * 8;
   const size_t budget = cfg->hbm_budget ? cfg->hbm_budget : (size_t)150 << 30;
@@ -894,7 +920,9 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
       (rc = e->s64.alloc(N * e->s64_stride)) || (rc = e->s32.alloc(N * e->s32_stride)) ||
       (rc = e->W.alloc(N * e->nB_max * (size_t)e->w_stride)) ||
       (rc = e->Wg.alloc(N * e->nB_max * (size_t)e->w_stride)) ||
-      (rc = e->counts.alloc(N * e->nB_max)) || (rc = e->status.alloc(1)))
+      (rc = e->counts.alloc(N * e->nB_max)) || (rc = e->status.alloc(1)) ||
+      (rc = e->order.alloc(N)) || (rc = e->tile_start.alloc(N + 1)) ||
+      (rc = e->tile_list.alloc(N * (size_t)e->max_tiles_pp)))
     return fail(rc);
   if (cfg->with_shear) {
     if ((rc = e->Phi.alloc(N * (size_t)e->nI_max * sh.n_R * e->w_stride)) ||
@@ -993,16 +1021,15 @@ enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_t
     count_launch();
     Y3B_CUDA(cudaGetLastError());
   } else {
-    for (int g = 0; g < (int)e->grids.size(); ++g) {
-      if (!((grid_mask >> g) & 1)) continue;
-      MixedLaunch L{e->d_grids.get(), d_pts, g, n, &e->grids[g], e->s32.get(), e->W.get(),
-                    e->Wg.get(), e->w_stride, e->status.get(), s,
-                    e->cfg.with_shear && d_shear != nullptr};
-      int rc = launch_mixed_gemm(L);
-      if (rc) {
-        delete tc;
-        return rc;
-      }
+    ContractLaunch L{e->d_grids.get(), (int)e->grids.size(), grid_mask, d_pts, n,
+                     e->order.get(), e->tile_start.get(), e->tile_list.get(),
+                     (long long)n * e->max_tiles_pp, e->cshape, e->s32.get(), e->W.get(),
+                     e->Wg.get(),
+                     e->w_stride, e->status.get(), s, e->cfg.with_shear && d_shear != nullptr};
+    const int rc = launch_contract(L);
+    if (rc) {
+      delete tc;
+      return rc;
     }
   }
   delete tc;

@@ -31,6 +31,8 @@ struct GridDev {
   int nIc;         // richness bins per tensor-core CTA (nIc * n_z <= 256 columns)
   int n_bg;        // bin groups = ceil(nI / nIc)
   int ncp_c;       // TMEM columns per CTA: nIc * n_z padded to 16
+  int tiles_pp;    // contraction tiles per point: (n_m_pad / kGemmRows) * n_bg
+  int cost_rank;   // 0 = the grid with the most expensive tiles (scheduled first)
   double lnm_lo, lnm_hi, zt_lo, zt_hi, ll_lo, ll_hi, sz0;
   const double* xm;   // [n_m]  lnM nodes
   const double* wm;
@@ -71,12 +73,24 @@ struct ShearDev {
   double c0, c_slope, c_pivot;
 };
 
-struct MixedLaunch {
+// Shared-memory shape of the contraction, fixed per engine.
+struct ContractShape {
+  int nJ;       // z_obs bins (shared by all grids)
+  int nz_max;   // largest n_z
+  int ntp_max;  // largest n_t_pad
+  int uk_max;   // floats of staged u_t K_i(t) per tile (0: read from global)
+};
+
+struct ContractLaunch {
   const GridDev* grids;     // device array
+  int n_grids, grid_mask;   // points of grids outside the mask get no tiles
   const PointDev* pts;      // device array
-  int grid_id;              // only points of this grid do work
   int n_points;
-  const GridDev* g_host;    // host copy of grids[grid_id] (dims)
+  int* order;               // [n_points] device scratch: points by grid cost
+  int* tile_start;          // [n_points + 1] device scratch: tile offsets
+  int* tile_list;           // [max_tiles] device scratch: (point << 8) | local tile
+  long long max_tiles;      // upper bound of the launch's tiles (grid size)
+  ContractShape shape;
   float* s32;               // FP32 scratch base
   double* W;                // [n][nB][w_stride]
   double* Wg;
@@ -86,7 +100,11 @@ struct MixedLaunch {
   bool shear;               // also accumulate the Sigma_crit-weighted W^g
 };
 
-int launch_mixed_gemm(const MixedLaunch& L);
+// One launch of the tile planner and one persistent contraction launch over
+// the points of every grid.
+int launch_contract(const ContractLaunch& L);
+size_t contract_smem_bytes(const ContractShape& c);  // (size_t)-1 if it does not fit
+int contract_stages(const ContractShape& c);
 
 // Enqueues a copy of the engine's device status word (the result of the
 // device-side checks of the evaluations enqueued before it on `s`) to `host`.
@@ -106,6 +124,12 @@ int engine_check_points(const ::y3b_engine* e, int n, const y3b_point* pts, int*
 // Host-side copy of the device domain check: every z_t node of a point's grid
 // must lie inside its distances/z table (host tables).  Y3B_ERR_DOMAIN if not.
 int engine_check_tables(const ::y3b_engine* e, int n, const y3b_point* pts, const double* tables);
-size_t mixed_gemm_smem_bytes(int ncp, int n_z, int n_t_pad, int nJ, int nIc);
+
+// A point's grid index is valid and selected.
+__host__ __device__ inline bool
+grid_in_mask(int mask, int g)
+{
+  return (unsigned)g < 31u && ((mask >> g) & 1);
+}
 
 }  // namespace y3b

@@ -18,11 +18,14 @@
 // and contracts z_t with the FP32 weights C_j(q) = v_q dV Omega K_j(q) into
 // FP64 mass weights W_ij(k) (and the Sigma_crit-weighted W^gamma_ij(k)).
 //
-// A persistent CTA per SM walks the (point, 128-row lnM tile, richness-bin
-// group) tiles: warps 1-11 generate operands into a 4-stage shared-memory
-// ring, warp 0 issues the MMAs into one of two TMEM accumulators, warps 12-15
-// drain the other; full/empty mbarriers (empty signalled by tcgen05.commit)
-// order the ring and the accumulators, and every wait is bounded.
+// One launch covers the points of every grid: a planner kernel orders the
+// points by the cost of their grid's tiles and a persistent CTA per SM walks
+// the (point, 128-row lnM tile, richness-bin group) tiles in that order:
+// warps 1-8 generate F and warps 9-16 generate the other operand into an
+// 8-stage shared-memory ring, warp 0 issues the MMAs into one of two TMEM
+// accumulators, warps 17-24 drain the other; full/empty mbarriers (empty
+// signalled by tcgen05.commit) order the ring and the accumulators, and every
+// wait is bounded.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -155,19 +158,22 @@ tmem_ld16(uint32_t taddr, float* v)
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Split 8 FP32 values into bf16 hi + lo and store one 16-byte core-matrix
-// row of each.
+// Split 8 FP32 values (4 pairs) into bf16 hi (round to nearest) + bf16 lo
+// (round to nearest of v - hi, which is exact in FP32) and store one 16-byte
+// core-matrix row of each.  Packed FP32x2 arithmetic: 5 instructions a pair.
 __device__ __forceinline__ void
-store_split8(uint8_t* hi, uint8_t* lo, const float* v)
+store_split8(uint8_t* hi, uint8_t* lo, const float2* v)
 {
   uint32_t h[4], l[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    __nv_bfloat162 hb = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
-    float2 hf = __bfloat1622float2(hb);
-    __nv_bfloat162 lb = __floats2bfloat162_rn(v[2 * k] - hf.x, v[2 * k + 1] - hf.y);
-    h[k] = *reinterpret_cast<uint32_t*>(&hb);
-    l[k] = *reinterpret_cast<uint32_t*>(&lb);
+    const __nv_bfloat162 hb = __float22bfloat162_rn(v[k]);
+    const uint32_t hu = *reinterpret_cast<const uint32_t*>(&hb);
+    const float2 hf = make_float2(__uint_as_float(hu << 16), __uint_as_float(hu & 0xFFFF0000u));
+    const float2 r = __ffma2_rn(hf, make_float2(-1.f, -1.f), v[k]);
+    const __nv_bfloat162 lb = __float22bfloat162_rn(r);
+    h[k] = hu;
+    l[k] = *reinterpret_cast<const uint32_t*>(&lb);
   }
   *reinterpret_cast<uint4*>(hi) = make_uint4(h[0], h[1], h[2], h[3]);
   *reinterpret_cast<uint4*>(lo) = make_uint4(l[0], l[1], l[2], l[3]);
@@ -175,33 +181,22 @@ store_split8(uint8_t* hi, uint8_t* lo, const float* v)
 
 constexpr long long kWaitBudget = 2000000000LL;  // SM cycles (~1 s)
 constexpr int kMmaWarp = 0;        // issues tcgen05.mma
-constexpr int kProdWarp0 = 1;      // warps 1..8 generate operands (one F and one A item each)
-constexpr int kProdWarps = 8;
-constexpr int kEpiWarp0 = 9;       // warps 9..16 drain TMEM (warp w reads lanes 32 (w % 4)..)
+constexpr int kFWarp0 = 1;         // warps 1..8: F(t, k), thread -> (row, half of the k-step)
+constexpr int kFWarps = 8;
+constexpr int kAWarp0 = 9;         // warps 9..16: A((i, q), t), thread -> (q, half, bin pair)
+constexpr int kAWarps = 8;
+constexpr int kProdWarps = kFWarps + kAWarps;
+constexpr int kEpiWarp0 = 17;      // warps 17..24 drain TMEM (warp w reads lanes 32 (w % 4)..)
 constexpr int kEpiWarps = 8;
-constexpr int kThreads = 32 * (1 + kProdWarps + kEpiWarps);  // 544
+constexpr int kLoadWarp = 25;      // stages the next tile's factor vectors in shared memory
+constexpr int kThreads = 32 * (2 + kProdWarps + kEpiWarps);  // 832
 constexpr int kStageK = 16;        // lam_t nodes per pipeline stage (one MMA k-step)
-constexpr int kStages = 4;
+constexpr int kMaxStages = 8;      // ring depth: what shared memory leaves, at most 8
 constexpr int kAccCols = 256;      // TMEM columns per accumulator buffer (2 buffers)
-
-__host__ __device__ inline uint32_t
-stage_bytes(int ncp)
-{
-  return 2u * kGemmRows * kStageK * 2u + 2u * (uint32_t)ncp * kStageK * 2u;
-}
-
-// shared memory: stage ring | producer floats | epilogue floats | control
-__host__ __device__ inline uint32_t
-prod_floats(int n_z, int n_t_pad, int nIc)
-{
-  return kGemmRows + n_z + n_t_pad + nIc * n_t_pad;
-}
-
-__host__ __device__ inline uint32_t
-epi_floats(int n_z, int nJ)
-{
-  return 2 * nJ * n_z;
-}
+constexpr uint32_t kFPlane = kGemmRows * kStageK * 2;        // one bf16 plane of F: 4 KB
+constexpr uint32_t kAPlane = kAccCols * kStageK * 2;         // one bf16 plane of A: 8 KB
+constexpr uint32_t kStageBytes = 2 * kFPlane + 2 * kAPlane;  // hi + lo of both: 24 KB
+constexpr uint32_t kLboF = kGemmRows * 16;                   // K-adjacent core matrices of F
 
 __device__ __forceinline__ void
 mbar_arrive(uint32_t addr)
@@ -224,7 +219,7 @@ mbar_wait_or_abort(uint32_t addr, uint32_t parity, volatile int* abort_flag)
   return true;
 }
 
-// Named barrier over `count` threads (the producer or the epilogue group).
+// Named barrier over `count` threads (the epilogue group).
 __device__ __forceinline__ void
 group_sync(int id, int count)
 {
@@ -240,80 +235,202 @@ warp_wait(uint32_t addr, uint32_t parity, volatile int* abort_flag, int lane)
   return __shfl_sync(0xffffffffu, ok, 0) != 0;
 }
 
-struct TileIdx {
-  int p, mtile, bg;
+// Position in the operand ring: stage s and the parity of its current use.
+struct RingPos {
+  int s = 0;
+  uint32_t ph = 0;
+  __device__ __forceinline__ void next(int n)
+  {
+    if (++s == n) {
+      s = 0;
+      ph ^= 1u;
+    }
+  }
 };
 
-__device__ __forceinline__ TileIdx
-tile_of(int t, int n_mt, int n_bg)
+// Untiled bulk copy global -> shared completing on mbarrier `mbar` (16-byte
+// aligned addresses, size a multiple of 16).
+__device__ __forceinline__ void
+bulk_g2s(void* dst, const void* src, uint32_t bytes, uint32_t mbar)
 {
-  TileIdx r;
-  r.bg = t % n_bg;
-  t /= n_bg;
-  r.mtile = t % n_mt;
-  r.p = t / n_mt;
+  asm volatile(
+    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+      smem_u32(dst)),
+    "l"(src), "r"(bytes), "r"(mbar)
+    : "memory");
+}
+
+// Tile t of the launch: tile_list[t] = (point << 8) | local tile, local
+// tiles of a point with the richness-bin groups varying fastest.
+__host__ __device__ inline int
+vec_slot_floats(int nz_max, int ntp_max, int uk_max)
+{
+  return 4 + kGemmRows + nz_max + ntp_max + uk_max;
+}
+
+struct Tile {
+  int p, mtile, bg;
+  const GridDev* G;
+};
+
+__device__ __forceinline__ Tile
+decode_tile(int t, const int* __restrict__ tile_list, const PointDev* __restrict__ pts,
+            const GridDev* __restrict__ grids)
+{
+  const int v = __ldg(tile_list + t);
+  Tile T;
+  T.p = v >> 8;
+  const int local = v & 255;
+  T.G = grids + pts[T.p].grid;
+  const int n_bg = T.G->n_bg;
+  T.bg = local % n_bg;
+  T.mtile = local / n_bg;
+  return T;
+}
+
+// Exclusive prefix sum over the 1024 threads of a block; *total = the sum.
+__device__ __forceinline__ int
+block_excl_scan(int v, int* sh, int* total)
+{
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sh[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    const int y = sh[lane];
+    int z = y;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, z, o);
+      if (lane >= o) z += u;
+    }
+    sh[lane] = z - y;
+    if (lane == 31) sh[32] = z;
+  }
+  __syncthreads();
+  const int r = sh[w] + x - v;
+  *total = sh[32];
+  __syncthreads();
   return r;
 }
 
 }  // namespace
 
-// Persistent kernel: one CTA per SM loops over tiles (point, 128-row lnM
-// tile, richness-bin group).  A tile's accumulator is nIc n_z <= 256 TMEM
+// Orders the points by the cost of their grid's tiles (most expensive grid
+// first, stable inside a grid) and writes the tiles of the launch in that
+// order: tile_start[i] = tiles of order[0..i), tile_start[n] = all tiles,
+// tile_list[t] = (point << 8) | tile inside the point.  One
+// block of 1024 threads, each owning a contiguous chunk of points.  Points
+// whose grid is not in the mask are put last with no tiles.
+__global__ void __launch_bounds__(1024)
+tile_plan_kernel(const GridDev* __restrict__ grids, int n_grids, int grid_mask,
+                 const PointDev* __restrict__ pts, int n, int* __restrict__ order,
+                 int* __restrict__ tile_start, int* __restrict__ tile_list)
+{
+  __shared__ int sh[33];
+  const int C = (n + 1023) / 1024;
+  const int b = min(n, (int)threadIdx.x * C), e = min(n, b + C);
+  int base = 0;
+  for (int r = 0; r <= n_grids; ++r) {  // r == n_grids: points outside the mask
+    int c = 0;
+    for (int i = b; i < e; ++i) {
+      const int g = pts[i].grid;
+      const int key = grid_in_mask(grid_mask, g) ? grids[g].cost_rank : n_grids;
+      c += key == r;
+    }
+    int tot;
+    int pos = base + block_excl_scan(c, sh, &tot);
+    for (int i = b; i < e; ++i) {
+      const int g = pts[i].grid;
+      const int key = grid_in_mask(grid_mask, g) ? grids[g].cost_rank : n_grids;
+      if (key == r) order[pos++] = i;
+    }
+    base += tot;
+  }
+  __syncthreads();
+  int c = 0;
+  for (int i = b; i < e; ++i) {
+    const int g = pts[order[i]].grid;
+    c += grid_in_mask(grid_mask, g) ? grids[g].tiles_pp : 0;
+  }
+  int tot;
+  int off = block_excl_scan(c, sh, &tot);
+  for (int i = b; i < e; ++i) {
+    tile_start[i] = off;
+    const int p = order[i], g = pts[p].grid;
+    const int nt = grid_in_mask(grid_mask, g) ? grids[g].tiles_pp : 0;
+    for (int l = 0; l < nt; ++l) tile_list[off + l] = (p << 8) | l;
+    off += nt;
+  }
+  if (threadIdx.x == 0) tile_start[n] = tot;
+}
+
+// Persistent contraction: one CTA per SM walks the launch's tiles (point,
+// 128-row lnM tile, richness-bin group), points of every grid in one launch,
+// most expensive grid first.  A tile's accumulator is nIc n_z <= 256 TMEM
 // columns; two buffers let the epilogue of tile j overlap the MMAs of tile
-// j+1.  Roles: warp 0 issues MMAs; warps 1-11 fill a 4-stage shared-memory
-// ring (full/empty mbarriers, empty signalled by tcgen05.commit); warps 12-15
-// read TMEM, apply Y(k,q) and the z-bin weights and write W_ij(k) in FP64.
+// j+1.  Roles: warp 0 issues the MMAs; warps 1-8 generate F and warps 9-16
+// generate A into an n_stages-deep shared-memory ring (full/empty mbarriers,
+// empty signalled by tcgen05.commit), each thread reading its point's factor
+// vectors straight from global memory, so no producer waits on another;
+// warps 17-24 read TMEM, apply Y(k,q) and the z-bin weights and write
+// W_ij(k) in FP64.  The tile's block of Y (n_z rows of 128 lnM values) is
+// brought into shared memory by bulk async copies issued while the tile's
+// MMAs run.
 template <int NJ, bool SHEAR>
 __global__ void __launch_bounds__(kThreads, 1)
-mixed_gemm_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ pts,
-                  int n_points, int grid_id, const float* __restrict__ s32,
-                  double* __restrict__ Wout, double* __restrict__ Wgout, int w_stride,
-                  int* status)
+contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ pts,
+                const int* __restrict__ tile_start, const int* __restrict__ tile_list,
+                int n_points, int nz_max, int ntp_max, int uk_max, int n_stages,
+                const float* __restrict__ s32, double* __restrict__ Wout,
+                double* __restrict__ Wgout, int w_stride, int* status)
 {
-  const GridDev* Gp = grids + grid_id;
-  const int n_m = Gp->n_m, n_z = Gp->n_z, n_t_pad = Gp->n_t_pad, nI = Gp->nI, nB = Gp->nB;
-  const int nIc = Gp->nIc, ncp = Gp->ncp_c, n_m_pad = Gp->n_m_pad, n_bg = Gp->n_bg;
-  const int n_mt = n_m_pad / kGemmRows;
-  const int n_tiles = n_points * n_mt * n_bg;
-  const bool uk_smem = Gp->uk_zindep != 0;
-  const float* __restrict__ UK = Gp->UK;
-  const size_t s32_stride = Gp->s32_stride;
-  const size_t f_a = Gp->f_a, f_b = Gp->f_b, f_delta = Gp->f_delta, f_scal = Gp->f_scal;
-  const size_t f_CN = Gp->f_CN, f_CG = Gp->f_CG, f_Yt = Gp->f_Yt;
-  const int nk = n_t_pad / kStageK;
-  const uint32_t SB = stage_bytes(ncp);
-  const uint32_t lboA = (uint32_t)ncp * 16u;
-  const uint32_t lboF = kGemmRows * 16u;
-
   extern __shared__ __align__(1024) uint8_t smem[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  float* a_s = reinterpret_cast<float*>(smem + kStages * SB);
-  float* b_s = a_s + kGemmRows;
-  float* d_s = b_s + n_z;
-  float* UK_s = d_s + n_t_pad;
-  float* CN_s = a_s + prod_floats(n_z, n_t_pad, nIc);
-  float* CG_s = CN_s + NJ * n_z;
-  uint32_t ctl = kStages * SB + 4u * (prod_floats(n_z, n_t_pad, nIc) + epi_floats(n_z, NJ));
+  const int n_tiles = __ldg(tile_start + n_points);
+  const int nst = n_stages;
+  float* Ys = reinterpret_cast<float*>(smem + nst * kStageBytes);  // [n_z][128]
+  float* CN_s = Ys + (size_t)nz_max * kGemmRows;
+  float* CG_s = CN_s + NJ * nz_max;
+  // Two slots of per-tile factor vectors: scal[4] | a[128] | b[nz_max] |
+  // delta[ntp_max] | u_t K_i(t)[uk_max] (all 16-byte aligned).
+  const int vec_floats = vec_slot_floats(nz_max, ntp_max, uk_max);
+  float* vec_s = CG_s + NJ * nz_max;
+  uint32_t ctl = nst * kStageBytes +
+                 4u * ((uint32_t)nz_max * kGemmRows + 2u * NJ * nz_max + 2u * vec_floats);
   ctl = (ctl + 15u) & ~15u;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + ctl);
-  uint64_t* empty = full + kStages;
-  uint64_t* acc_full = empty + kStages;
+  uint64_t* empty = full + kMaxStages;
+  uint64_t* acc_full = empty + kMaxStages;
   uint64_t* acc_empty = acc_full + 2;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
+  uint64_t* ybar = acc_empty + 2;
+  uint64_t* vec_full = ybar + 1;
+  uint64_t* vec_empty = vec_full + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(vec_empty + 2);
   volatile int* abort_s = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
-  // Zero the operand ring once: padded rows/columns stay zero throughout.
-  for (uint32_t i = tid * 16u; i < kStages * SB; i += kThreads * 16u)
+  // Zero the operand ring once: columns a tile does not write stay finite.
+  for (uint32_t i = tid * 16u; i < nst * kStageBytes; i += kThreads * 16u)
     *reinterpret_cast<uint4*>(smem + i) = make_uint4(0u, 0u, 0u, 0u);
   if (warp == kMmaWarp) tmem_alloc(smem_u32(tmem_slot), 2 * kAccCols);
   if (tid == 0) {
-    for (int i = 0; i < kStages; ++i) {
+    for (int i = 0; i < nst; ++i) {
       mbar_init(smem_u32(&full[i]), kProdWarps);
       mbar_init(smem_u32(&empty[i]), 1);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(smem_u32(&acc_full[b]), 1);
       mbar_init(smem_u32(&acc_empty[b]), kEpiWarps);
+    }
+    mbar_init(smem_u32(ybar), 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&vec_full[b]), 1);
+      mbar_init(smem_u32(&vec_empty[b]), kProdWarps);
     }
     *abort_s = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -326,34 +443,36 @@ mixed_gemm_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict_
   if (warp == kMmaWarp) {
     // ---------------- MMA issuer ----------------
     if (lane == 0) {
-      int chunk = 0, j = 0, last_stage = -1, last_parity = 0;
+      RingPos rp;
+      int j = 0, last_stage = -1, last_parity = 0;
       for (int t = blockIdx.x; t < n_tiles && !*abort_s; t += gridDim.x) {
-        const TileIdx ti = tile_of(t, n_mt, n_bg);
-        if (pts[ti.p].grid != grid_id || ti.bg * nIc >= nI) continue;
+        const Tile T = decode_tile(t, tile_list, pts, grids);
+        const int ncp = T.G->ncp_c, nk = T.G->n_t_pad / kStageK;
         const int buf = j & 1;
         if (j >= 2 && !mbar_wait_or_abort(smem_u32(&acc_empty[buf]), ((j >> 1) - 1) & 1, abort_s))
           break;
         tc_fence_after();
         const uint32_t dacc = tmem + (uint32_t)(buf * kAccCols);
+        const uint32_t idesc = umma_idesc_bf16(kGemmRows, ncp);
+        const uint32_t lboA = (uint32_t)ncp * 16u;
         bool broke = false;
-        for (int kc = 0; kc < nk; ++kc, ++chunk) {
-          const int s = chunk % kStages;
-          if (!mbar_wait_or_abort(smem_u32(&full[s]), (chunk / kStages) & 1, abort_s)) {
+        for (int kc = 0; kc < nk; ++kc, rp.next(nst)) {
+          const int s = rp.s;
+          if (!mbar_wait_or_abort(smem_u32(&full[s]), rp.ph, abort_s)) {
             broke = true;
             break;
           }
           tc_fence_after();
-          const uint32_t fh = smem_u32(smem + s * SB), fl = fh + lboF * 2;
-          const uint32_t ah = fl + lboF * 2, al = ah + lboA * 2;
-          const uint64_t dfh = umma_desc(fh, lboF, 128), dfl = umma_desc(fl, lboF, 128);
-          const uint32_t idesc = umma_idesc_bf16(kGemmRows, ncp);
+          const uint32_t fh = smem_u32(smem + s * kStageBytes), fl = fh + kFPlane;
+          const uint32_t ah = fh + 2 * kFPlane, al = ah + kAPlane;
+          const uint64_t dfh = umma_desc(fh, kLboF, 128), dfl = umma_desc(fl, kLboF, 128);
           const uint64_t dah = umma_desc(ah, lboA, 128), dal = umma_desc(al, lboA, 128);
           umma_bf16(dacc, dfh, dah, idesc, kc != 0);
           umma_bf16(dacc, dfh, dal, idesc, 1u);
           umma_bf16(dacc, dfl, dah, idesc, 1u);
           umma_commit(smem_u32(&empty[s]));
           last_stage = s;
-          last_parity = (chunk / kStages) & 1;
+          last_parity = (int)rp.ph;
         }
         if (broke) break;
         umma_commit(smem_u32(&acc_full[buf]));  // tile j's accumulator is complete
@@ -370,95 +489,127 @@ mixed_gemm_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict_
       }
     }
     __syncwarp();
-  } else if (warp < kEpiWarp0) {
-    // ---------------- operand producers ----------------
-    const int ptid = tid - kProdWarp0 * 32;
-    constexpr int kP = kProdWarps * 32;
-    int chunk = 0, last_grid_loaded = 0;
-    // Every producer runs every tile iteration (named barriers stay matched);
-    // after an abort the waits return at once and the work is skipped.
-    for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
-      const TileIdx ti = tile_of(t, n_mt, n_bg);
-      if (pts[ti.p].grid != grid_id || ti.bg * nIc >= nI) continue;
-      const int i0 = ti.bg * nIc, nIh = min(nIc, nI - i0);
-      const float* __restrict__ sp = s32 + (size_t)ti.p * s32_stride;
-      // Per-tile vectors (all producers have finished the previous tile's
-      // generation before they are overwritten).
-      group_sync(1, kP);
-      const float c1 = sp[f_scal], c2 = sp[f_scal + 1];
-      const float sc1 = sqrtf(c1);
-      for (int m = ptid; m < kGemmRows; m += kP) {
-        const int row = ti.mtile * kGemmRows + m;
-        a_s[m] = row < n_m ? sp[f_a + row] * sc1 : 0.f;
-      }
-      for (int q = ptid; q < n_z; q += kP) b_s[q] = sp[f_b + q] * c2;
-      for (int u = ptid; u < n_t_pad; u += kP) d_s[u] = sp[f_delta + u] * sc1;
-      if (uk_smem && (last_grid_loaded == 0 || last_grid_loaded != i0 + 1)) {
-        for (int u = ptid; u < nIh * n_t_pad; u += kP) {
-          const int il = u / n_t_pad, tt = u - il * n_t_pad;
-          UK_s[u] = UK[((size_t)(i0 + il) * n_z) * n_t_pad + tt];  // the q = 0 slice
-        }
-        last_grid_loaded = i0 + 1;
-      }
-      group_sync(1, kP);
-      const float inv_sc1 = 1.0f / sc1;
-      for (int kc = 0; kc < nk; ++kc, ++chunk) {
-        const int s = chunk % kStages;
-        if (chunk >= kStages &&
-            !warp_wait(smem_u32(&empty[s]), ((chunk / kStages) - 1) & 1, abort_s, lane))
+  } else if (warp < kAWarp0) {
+    // ---------------- F(t, k) = 2^-((delta_t - a_k) sqrt(c1))^2 ----------------
+    const int f = tid - kFWarp0 * 32;
+    const int m = f & (kGemmRows - 1), g = f >> 7;
+    int chunk = 0, jt = 0;
+    RingPos rp;
+    for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++jt) {
+      const Tile T = decode_tile(t, tile_list, pts, grids);
+      const GridDev* G = T.G;
+      const int nk = G->n_t_pad / kStageK;
+      const int slot = jt & 1;
+      const float* vs = vec_s + slot * vec_floats;
+      if (!warp_wait(smem_u32(&vec_full[slot]), (jt >> 1) & 1, abort_s, lane)) continue;
+      const float sc1 = sqrtf(vs[0]);
+      const bool valid = T.mtile * kGemmRows + m < G->n_m;
+      // Rows past n_m get an offset so large that F = 2^-(x^2) is exactly 0.
+      const float am = valid ? vs[4 + m] * sc1 : 1e18f;
+      const float2 sc2 = make_float2(sc1, sc1), nam2 = make_float2(-am, -am);
+      const float* dsm = vs + 132 + nz_max + g * 8;
+      for (int kc = 0; kc < nk; ++kc, ++chunk, rp.next(nst)) {
+        const int s = rp.s;
+        if (chunk >= nst && !warp_wait(smem_u32(&empty[s]), rp.ph ^ 1u, abort_s, lane))
           continue;
         if (*abort_s) continue;
-        uint8_t* st = smem + s * SB;
-        uint8_t* Fhi = st;
-        uint8_t* Flo = st + lboF * 2;
-        uint8_t* Ahi = Flo + lboF * 2;
-        uint8_t* Alo = Ahi + lboA * 2;
-        // F(t, k) = 2^-((delta_t - a_k) sqrt(c1))^2: thread -> (row m, kgroup g).
-        {
-          const int m = ptid & (kGemmRows - 1), g = ptid >> 7;
-          const int t0 = kc * kStageK + g * 8;
-          const float am = a_s[m];
-          const float4 d0 = *reinterpret_cast<const float4*>(d_s + t0);
-          const float4 d1 = *reinterpret_cast<const float4*>(d_s + t0 + 4);
-          const float dd[8] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w};
-          float v[8];
+        uint8_t* st = smem + s * kStageBytes;
+        const float4 d0 = *reinterpret_cast<const float4*>(dsm + kc * kStageK);
+        const float4 d1 = *reinterpret_cast<const float4*>(dsm + kc * kStageK + 4);
+        const float2 dd[4] = {make_float2(d0.x, d0.y), make_float2(d0.z, d0.w),
+                              make_float2(d1.x, d1.y), make_float2(d1.z, d1.w)};
+        float2 v[4];
 #pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            const float d = dd[u] - am;
-            v[u] = fast_exp2(-d * d);
-          }
-          if (ti.mtile * kGemmRows + m >= n_m) {
-#pragma unroll
-            for (int u = 0; u < 8; ++u) v[u] = 0.f;
-          }
-          store_split8(Fhi + g * lboF + m * 16, Flo + g * lboF + m * 16, v);
+        for (int u = 0; u < 4; ++u) {
+          const float2 x = __ffma2_rn(dd[u], sc2, nam2);
+          const float2 e = __fmul2_rn(x, x);
+          v[u] = make_float2(fast_exp2(-e.x), fast_exp2(-e.y));
         }
-        // A((i, q), t) = u_t K_i(t, q) 2^(delta_t c2 b_q): thread -> (q, kgroup).
-        for (int ia = ptid; ia < 2 * n_z; ia += kP) {
-          const int g = ia >= n_z ? 1 : 0;
-          const int q = ia - g * n_z;
-          const int t0 = kc * kStageK + g * 8;
-          const float bq = b_s[q] * inv_sc1;  // d_s carries sqrt(c1)
-          const float4 d0 = *reinterpret_cast<const float4*>(d_s + t0);
-          const float4 d1 = *reinterpret_cast<const float4*>(d_s + t0 + 4);
-          const float dd[8] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w};
-          float gq[8];
+        store_split8(st + g * kLboF + m * 16, st + kFPlane + g * kLboF + m * 16, v);
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&full[s]));
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&vec_empty[slot]));  // done with this slot
+    }
+  } else if (warp < kEpiWarp0) {
+    // ---------------- A((i, q), t) = u_t K_i(t, q) 2^(delta_t b_q c2) ----------------
+    const int a = tid - kAWarp0 * 32;
+    constexpr int kA = kAWarps * 32;
+    int chunk = 0, jt = 0;
+    RingPos rp;
+    for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++jt) {
+      const Tile T = decode_tile(t, tile_list, pts, grids);
+      const GridDev* G = T.G;
+      const int nk = G->n_t_pad / kStageK, n_z = G->n_z, ntp = G->n_t_pad;
+      const int i0 = T.bg * G->nIc, nIh = min(G->nIc, G->nI - i0);
+      const int items = 2 * n_z * ((nIh + 1) >> 1);
+      const int slot = jt & 1;
+      const float* vs = vec_s + slot * vec_floats;
+      if (!warp_wait(smem_u32(&vec_full[slot]), (jt >> 1) & 1, abort_s, lane)) continue;
+      const float c2 = vs[1];
+      const float* bsm = vs + 4 + kGemmRows;
+      const float* dsm = vs + 132 + nz_max;
+      // u_t K_i(t): the staged copy when P(lam_o | lam_t) has no z dependence,
+      // else the per-(i, q) rows in global memory.
+      const bool uks = G->uk_zindep != 0 && nIh * ntp <= uk_max;
+      const float* uksm = dsm + ntp_max;
+      const float* __restrict__ UK = G->UK;
+      const uint32_t lboA = (uint32_t)G->ncp_c * 16u;
+      // This thread's items (q, k half, bin pair) of the tile: at most two,
+      // since items <= 2 * 256.
+      int item_q[2], item_g[2], item_il[2], item_ok = 0;
 #pragma unroll
-          for (int u = 0; u < 8; ++u) gq[u] = fast_exp2(dd[u] * bq);
-          for (int il = 0; il < nIh; ++il) {
+      for (int r = 0; r < 2; ++r) {
+        const int it = a + r * kA;
+        const int q = it % n_z, rest = it / n_z;
+        item_q[r] = q;
+        item_g[r] = rest & 1;
+        item_il[r] = (rest >> 1) * 2;
+        if (it < items) item_ok |= 1 << r;
+      }
+      for (int kc = 0; kc < nk; ++kc, ++chunk, rp.next(nst)) {
+        const int s = rp.s;
+        if (chunk >= nst && !warp_wait(smem_u32(&empty[s]), rp.ph ^ 1u, abort_s, lane))
+          continue;
+        if (*abort_s) continue;
+        uint8_t* Ahi = smem + s * kStageBytes + 2 * kFPlane;
+        uint8_t* Alo = Ahi + kAPlane;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          if (!(item_ok & (1 << r))) continue;
+          const int q = item_q[r], g = item_g[r], il0 = item_il[r];
+          const int t0 = kc * kStageK + g * 8;
+          const float bq = bsm[q] * c2;
+          const float2 bq2 = make_float2(bq, bq);
+          const float4 d0 = *reinterpret_cast<const float4*>(dsm + t0);
+          const float4 d1 = *reinterpret_cast<const float4*>(dsm + t0 + 4);
+          const float2 dd[4] = {make_float2(d0.x, d0.y), make_float2(d0.z, d0.w),
+                                make_float2(d1.x, d1.y), make_float2(d1.z, d1.w)};
+          float2 gq[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const float2 x = __fmul2_rn(dd[u], bq2);
+            gq[u] = make_float2(fast_exp2(x.x), fast_exp2(x.y));
+          }
+          const int il1 = min(il0 + 2, nIh);
+          for (int il = il0; il < il1; ++il) {
             float4 u0, u1;
-            if (uk_smem) {
-              const float4* uk = reinterpret_cast<const float4*>(UK_s + il * n_t_pad + t0);
+            if (uks) {
+              const float4* uk = reinterpret_cast<const float4*>(uksm + il * ntp + t0);
               u0 = uk[0];
               u1 = uk[1];
             } else {
               const float4* uk = reinterpret_cast<const float4*>(
-                UK + ((size_t)((i0 + il) * n_z + q)) * n_t_pad + t0);
+                UK + ((size_t)((i0 + il) * n_z + q)) * ntp + t0);
               u0 = __ldg(uk);
               u1 = __ldg(uk + 1);
             }
-            float v[8] = {u0.x * gq[0], u0.y * gq[1], u0.z * gq[2], u0.w * gq[3],
-                          u1.x * gq[4], u1.y * gq[5], u1.z * gq[6], u1.w * gq[7]};
+            const float2 v[4] = {__fmul2_rn(make_float2(u0.x, u0.y), gq[0]),
+                                 __fmul2_rn(make_float2(u0.z, u0.w), gq[1]),
+                                 __fmul2_rn(make_float2(u1.x, u1.y), gq[2]),
+                                 __fmul2_rn(make_float2(u1.z, u1.w), gq[3])};
             const int row = il * n_z + q;
             store_split8(Ahi + g * lboA + row * 16, Alo + g * lboA + row * 16, v);
           }
@@ -467,7 +618,50 @@ mixed_gemm_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict_
         __syncwarp();
         if (lane == 0) mbar_arrive(smem_u32(&full[s]));
       }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&vec_empty[slot]));  // done with this slot
     }
+  } else if (warp == kLoadWarp) {
+    // ---------------- per-tile factor vectors, one tile ahead ----------------
+    if (lane == 0) {
+      int j = 0, issued = -1;
+      for (int t = blockIdx.x; t < n_tiles && !*abort_s; t += gridDim.x, ++j) {
+        const int slot = j & 1;
+        if (j >= 2 && !mbar_wait_or_abort(smem_u32(&vec_empty[slot]), ((j >> 1) - 1) & 1, abort_s))
+          break;
+        const Tile T = decode_tile(t, tile_list, pts, grids);
+        const GridDev* G = T.G;
+        const int n_z = G->n_z, ntp = G->n_t_pad;
+        const int i0 = T.bg * G->nIc, nIh = min(G->nIc, G->nI - i0);
+        const bool uks = G->uk_zindep != 0 && nIh * ntp <= uk_max;
+        const float* sp = s32 + (size_t)T.p * G->s32_stride;
+        float* vs = vec_s + slot * vec_floats;
+        const uint32_t bytes = 4u * (4 + kGemmRows + n_z + ntp + (uks ? nIh * ntp : 0));
+        const uint32_t vb = smem_u32(&vec_full[slot]);
+        fence_proxy_async_smem();  // the producers' reads of this slot come first
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(vb),
+                     "r"(bytes)
+                     : "memory");
+        bulk_g2s(vs, sp + G->f_scal, 16u, vb);
+        bulk_g2s(vs + 4, sp + G->f_a + (size_t)T.mtile * kGemmRows, 4u * kGemmRows, vb);
+        bulk_g2s(vs + 4 + kGemmRows, sp + G->f_b, 4u * n_z, vb);
+        bulk_g2s(vs + 132 + nz_max, sp + G->f_delta, 4u * ntp, vb);
+        if (uks)
+          for (int il = 0; il < nIh; ++il)
+            bulk_g2s(vs + 132 + nz_max + ntp_max + il * ntp,
+                     G->UK + (size_t)(i0 + il) * n_z * ntp, 4u * ntp, vb);
+        issued = j;
+      }
+      // Copies still in flight (after an abort) must land before the CTA's
+      // shared memory is released: wait for the last two issued (bounded).
+      for (int jj = max(0, issued - 1); jj <= issued; ++jj) {
+        long long t0 = clock64();
+        while (!mbar_try_wait(smem_u32(&vec_full[jj & 1]), (jj >> 1) & 1) &&
+               clock64() - t0 < kWaitBudget) {
+        }
+      }
+    }
+    __syncwarp();
   } else {
     // ---------------- epilogue ----------------
     const int etid = tid - kEpiWarp0 * 32;
@@ -476,25 +670,43 @@ mixed_gemm_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict_
     const int eg = (warp - kEpiWarp0) >> 2;   // which half of the bins
     constexpr int kEG = kEpiWarps / 4;
     const uint32_t lane_base = (uint32_t)(lq * 32) << 16;
-    int j = 0;
+    int j = 0, y_pending = 0;
     for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
-      const TileIdx ti = tile_of(t, n_mt, n_bg);
-      if (pts[ti.p].grid != grid_id || ti.bg * nIc >= nI) continue;
-      const int i0 = ti.bg * nIc, nIh = min(nIc, nI - i0);
-      const float* __restrict__ sp = s32 + (size_t)ti.p * s32_stride;
-      group_sync(2, kE);
+      const Tile T = decode_tile(t, tile_list, pts, grids);
+      const GridDev* G = T.G;
+      const int n_z = G->n_z, n_m = G->n_m, n_m_pad = G->n_m_pad, nI = G->nI, nB = G->nB;
+      const int i0 = T.bg * G->nIc, nIh = min(G->nIc, nI - i0);
+      const float* __restrict__ sp = s32 + (size_t)T.p * G->s32_stride;
+      group_sync(2, kE);  // the previous tile's Y and weights are no longer read
+      if (warp == kEpiWarp0 && !*abort_s) {
+        // Y rows q of this tile: 128 lnM values each, one bulk copy per row.
+        const uint32_t yb = smem_u32(ybar);
+        if (lane == 0) {
+          fence_proxy_async_smem();
+          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(yb),
+                       "r"((uint32_t)n_z * kGemmRows * 4u)
+                       : "memory");
+        }
+        __syncwarp();
+        const float* ysrc = sp + G->f_Yt + (size_t)T.mtile * kGemmRows;
+        for (int q = lane; q < n_z; q += 32)
+          bulk_g2s(Ys + (size_t)q * kGemmRows, ysrc + (size_t)q * n_m_pad, 4u * kGemmRows, yb);
+        y_pending = 1;
+      }
       for (int u = etid; u < NJ * n_z; u += kE) {
-        CN_s[u] = sp[f_CN + u];
-        if (SHEAR) CG_s[u] = sp[f_CG + u];
+        CN_s[u] = sp[G->f_CN + u];
+        if (SHEAR) CG_s[u] = sp[G->f_CG + u];
       }
       group_sync(2, kE);
       const int buf = j & 1;
       ++j;
       if (!warp_wait(smem_u32(&acc_full[buf]), ((j - 1) >> 1) & 1, abort_s, lane)) continue;
+      if (!warp_wait(smem_u32(ybar), (j - 1) & 1, abort_s, lane)) continue;
+      y_pending = 0;
       tc_fence_after();
-      const int row = ti.mtile * kGemmRows + lq * 32 + lane;
+      const int rl = lq * 32 + lane;  // row inside the tile
+      const int row = T.mtile * kGemmRows + rl;
       const bool valid = row < n_m;
-      const float* __restrict__ Yr = sp + f_Yt + (valid ? row : 0);
       const uint32_t tbase = tmem + lane_base + (uint32_t)(buf * kAccCols);
       for (int il = eg; il < nIh; il += kEG) {
         const int i = i0 + il;
@@ -504,30 +716,36 @@ mixed_gemm_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict_
         for (int qc = 0; qc < n_z; qc += 16) {
           float v[16];
           tmem_ld16(tbase + (uint32_t)(il * n_z + qc), v);
-          float pN[NJ], pG[NJ];
+          // Even and odd z nodes summed side by side (packed FP32x2), then
+          // added in FP64.
+          float2 pN[NJ], pG[NJ];
 #pragma unroll
-          for (int jj = 0; jj < NJ; ++jj) pN[jj] = pG[jj] = 0.f;
-          const float* __restrict__ yq = Yr + (size_t)qc * n_m_pad;
+          for (int jj = 0; jj < NJ; ++jj) pN[jj] = pG[jj] = make_float2(0.f, 0.f);
 #pragma unroll
-          for (int u = 0; u < 16; ++u) {
+          for (int u = 0; u < 16; u += 2) {
             const int q = qc + u;
-            const float e = v[u] * __ldg(yq + (size_t)u * n_m_pad);
+            const float2 e = __fmul2_rn(make_float2(v[u], v[u + 1]),
+                                        make_float2(Ys[q * kGemmRows + rl],
+                                                    Ys[(q + 1) * kGemmRows + rl]));
 #pragma unroll
             for (int jj = 0; jj < NJ; ++jj) {
-              pN[jj] = fmaf(CN_s[jj * n_z + q], e, pN[jj]);
-              if (SHEAR) pG[jj] = fmaf(CG_s[jj * n_z + q], e, pG[jj]);
+              pN[jj] = __ffma2_rn(*reinterpret_cast<const float2*>(CN_s + jj * n_z + q), e,
+                                  pN[jj]);
+              if (SHEAR)
+                pG[jj] = __ffma2_rn(*reinterpret_cast<const float2*>(CG_s + jj * n_z + q), e,
+                                    pG[jj]);
             }
           }
 #pragma unroll
           for (int jj = 0; jj < NJ; ++jj) {
-            accN[jj] += (double)pN[jj];
-            if (SHEAR) accG[jj] += (double)pG[jj];
+            accN[jj] += (double)pN[jj].x + (double)pN[jj].y;
+            if (SHEAR) accG[jj] += (double)pG[jj].x + (double)pG[jj].y;
           }
         }
         if (valid) {
 #pragma unroll
           for (int jj = 0; jj < NJ; ++jj) {
-            const size_t o = ((size_t)ti.p * nB + i + nI * jj) * w_stride + row;
+            const size_t o = ((size_t)T.p * nB + i + nI * jj) * w_stride + row;
             Wout[o] = accN[jj];
             if (SHEAR) Wgout[o] = accG[jj];
           }
@@ -538,6 +756,13 @@ mixed_gemm_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict_
       __syncwarp();
       if (lane == 0) mbar_arrive(smem_u32(&acc_empty[buf]));
     }
+    // After an abort a Y copy may still be in flight: wait for it (bounded)
+    // before the CTA's shared memory is released.
+    if (warp == kEpiWarp0 && y_pending && lane == 0) {
+      long long t0 = clock64();
+      while (!mbar_try_wait(smem_u32(ybar), (j - 1) & 1) && clock64() - t0 < kWaitBudget) {
+      }
+    }
   }
   __syncthreads();
   if (*abort_s && tid == 0) set_err(status, kDevTimeout);
@@ -547,38 +772,57 @@ mixed_gemm_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict_
   }
 }
 
-size_t
-mixed_gemm_smem_bytes(int ncp, int n_z, int n_t_pad, int nJ, int nIc)
+// Shared memory of the contraction with `stages` ring stages.
+static size_t
+contract_smem_at(int stages, const ContractShape& c)
 {
-  size_t b = kStages * (size_t)stage_bytes(ncp) +
-             4u * (prod_floats(n_z, n_t_pad, nIc) + epi_floats(n_z, nJ));
+  size_t b = (size_t)stages * kStageBytes +
+             4u * ((size_t)c.nz_max * kGemmRows + 2u * c.nJ * c.nz_max +
+                   2u * vec_slot_floats(c.nz_max, c.ntp_max, c.uk_max));
   b = (b + 15) & ~size_t(15);
-  return b + 8 * (2 * kStages + 4) + 16;
+  return b + 8 * (2 * kMaxStages + 9) + 16;
+}
+
+// Ring depth: as many stages (<= 8) as fit next to the Y block and the
+// vector slots; 0 if not even 2 do.
+int
+contract_stages(const ContractShape& c)
+{
+  for (int st = kMaxStages; st >= 2; --st)
+    if (contract_smem_at(st, c) <= 227 * 1024) return st;
+  return 0;
+}
+
+size_t
+contract_smem_bytes(const ContractShape& c)
+{
+  const int st = contract_stages(c);
+  return st ? contract_smem_at(st, c) : (size_t)-1;
 }
 
 template <int NJ, bool SHEAR>
 static int
-launch_nj(const MixedLaunch& L, size_t smem)
+launch_nj(const ContractLaunch& L, size_t smem)
 {
-  auto k = mixed_gemm_kernel<NJ, SHEAR>;
+  auto k = contract_kernel<NJ, SHEAR>;
   Y3B_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const GridDev& g = *L.g_host;
   int dev = 0, n_sm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-  const long long tiles = (long long)L.n_points * (g.n_m_pad / kGemmRows) * g.n_bg;
-  const int blocks = (int)std::min<long long>(tiles, n_sm);
-  k<<<blocks, kThreads, smem, L.stream>>>(L.grids, L.pts, L.n_points, L.grid_id, L.s32, L.W,
-                                          L.Wg, L.w_stride, L.status);
+  const int blocks = (int)std::min<long long>(std::max<long long>(L.max_tiles, 1), n_sm);
+  k<<<blocks, kThreads, smem, L.stream>>>(L.grids, L.pts, L.tile_start, L.tile_list, L.n_points,
+                                          L.shape.nz_max, L.shape.ntp_max, L.shape.uk_max,
+                                          contract_stages(L.shape), L.s32, L.W, L.Wg, L.w_stride,
+                                          L.status);
   count_launch();
-  return cuda_status(cudaGetLastError(), "mixed_gemm_kernel");
+  return cuda_status(cudaGetLastError(), "contract_kernel");
 }
 
 template <bool SHEAR>
 static int
-launch_shear(const MixedLaunch& L, size_t smem)
+launch_shear(const ContractLaunch& L, size_t smem)
 {
-  switch (L.g_host->nJ) {
+  switch (L.shape.nJ) {
     case 1: return launch_nj<1, SHEAR>(L, smem);
     case 2: return launch_nj<2, SHEAR>(L, smem);
     case 3: return launch_nj<3, SHEAR>(L, smem);
@@ -588,16 +832,19 @@ launch_shear(const MixedLaunch& L, size_t smem)
     case 7: return launch_nj<7, SHEAR>(L, smem);
     case 8: return launch_nj<8, SHEAR>(L, smem);
     default:
-      set_error("mixed_gemm: n_z_bins must be 1..8");
+      set_error("contract: n_z_bins must be 1..8");
       return Y3B_ERR_UNSUPPORTED;
   }
 }
 
 int
-launch_mixed_gemm(const MixedLaunch& L)
+launch_contract(const ContractLaunch& L)
 {
-  const GridDev& g = *L.g_host;
-  size_t smem = mixed_gemm_smem_bytes(g.ncp_c, g.n_z, g.n_t_pad, g.nJ, g.nIc);
+  tile_plan_kernel<<<1, 1024, 0, L.stream>>>(L.grids, L.n_grids, L.grid_mask, L.pts, L.n_points,
+                                             L.order, L.tile_start, L.tile_list);
+  count_launch();
+  Y3B_CUDA(cudaGetLastError());
+  const size_t smem = contract_smem_bytes(L.shape);
   return L.shear ? launch_shear<true>(L, smem) : launch_shear<false>(L, smem);
 }
 
