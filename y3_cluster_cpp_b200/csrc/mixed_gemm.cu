@@ -158,22 +158,24 @@ tmem_ld16(uint32_t taddr, float* v)
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Split 8 FP32 values (4 pairs) into bf16 hi (round to nearest) + bf16 lo
-// (round to nearest of v - hi, which is exact in FP32) and store one 16-byte
-// core-matrix row of each.  Packed FP32x2 arithmetic: 5 instructions a pair.
+// Split 8 FP32 values (4 pairs) into bf16 hi + bf16 lo and store one 16-byte
+// core-matrix row of each.  hi rounds to nearest (ties away) on the bit
+// pattern, lo = v - hi is exact in FP32 and keeps its top 16 bits, so
+// |v - hi - lo| <= 2^-16 |v|; the products hi*hi + hi*lo + lo*hi then carry a
+// relative error of a few 2^-17.  Integer and packed-FP32 instructions only:
+// the conversion unit stays free for the exponentials.
 __device__ __forceinline__ void
 store_split8(uint8_t* hi, uint8_t* lo, const float2* v)
 {
   uint32_t h[4], l[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    const __nv_bfloat162 hb = __float22bfloat162_rn(v[k]);
-    const uint32_t hu = *reinterpret_cast<const uint32_t*>(&hb);
-    const float2 hf = make_float2(__uint_as_float(hu << 16), __uint_as_float(hu & 0xFFFF0000u));
-    const float2 r = __ffma2_rn(hf, make_float2(-1.f, -1.f), v[k]);
-    const __nv_bfloat162 lb = __float22bfloat162_rn(r);
-    h[k] = hu;
-    l[k] = *reinterpret_cast<const uint32_t*>(&lb);
+    const uint32_t hx = (__float_as_uint(v[k].x) + 0x8000u) & 0xFFFF0000u;
+    const uint32_t hy = (__float_as_uint(v[k].y) + 0x8000u) & 0xFFFF0000u;
+    const float2 r =
+      __ffma2_rn(make_float2(__uint_as_float(hx), __uint_as_float(hy)), make_float2(-1.f, -1.f), v[k]);
+    h[k] = __byte_perm(hx, hy, 0x7632);
+    l[k] = __byte_perm(__float_as_uint(r.x), __float_as_uint(r.y), 0x7632);
   }
   *reinterpret_cast<uint4*>(hi) = make_uint4(h[0], h[1], h[2], h[3]);
   *reinterpret_cast<uint4*>(lo) = make_uint4(l[0], l[1], l[2], l[3]);
@@ -508,27 +510,44 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
       const float am = valid ? vs[4 + m] * sc1 : 1e18f;
       const float2 sc2 = make_float2(sc1, sc1), nam2 = make_float2(-am, -am);
       const float* dsm = vs + 132 + nz_max + g * 8;
-      for (int kc = 0; kc < nk; ++kc, ++chunk, rp.next(nst)) {
-        const int s = rp.s;
-        if (chunk >= nst && !warp_wait(smem_u32(&empty[s]), rp.ph ^ 1u, abort_s, lane))
+      // Two ring stages per iteration (nk is even): twice the independent
+      // work between waits, one fence for both.
+      for (int kc = 0; kc < nk; kc += 2, chunk += 2) {
+        int sp2[2];
+        uint32_t ph2[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          sp2[h] = rp.s;
+          ph2[h] = rp.ph;
+          rp.next(nst);
+        }
+        if (chunk >= nst && !warp_wait(smem_u32(&empty[sp2[0]]), ph2[0] ^ 1u, abort_s, lane))
+          continue;
+        if (chunk + 1 >= nst && !warp_wait(smem_u32(&empty[sp2[1]]), ph2[1] ^ 1u, abort_s, lane))
           continue;
         if (*abort_s) continue;
-        uint8_t* st = smem + s * kStageBytes;
-        const float4 d0 = *reinterpret_cast<const float4*>(dsm + kc * kStageK);
-        const float4 d1 = *reinterpret_cast<const float4*>(dsm + kc * kStageK + 4);
-        const float2 dd[4] = {make_float2(d0.x, d0.y), make_float2(d0.z, d0.w),
-                              make_float2(d1.x, d1.y), make_float2(d1.z, d1.w)};
-        float2 v[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const float2 x = __ffma2_rn(dd[u], sc2, nam2);
-          const float2 e = __fmul2_rn(x, x);
-          v[u] = make_float2(fast_exp2(-e.x), fast_exp2(-e.y));
+        for (int h = 0; h < 2; ++h) {
+          uint8_t* st = smem + sp2[h] * kStageBytes;
+          const float4 d0 = *reinterpret_cast<const float4*>(dsm + (kc + h) * kStageK);
+          const float4 d1 = *reinterpret_cast<const float4*>(dsm + (kc + h) * kStageK + 4);
+          const float2 dd[4] = {make_float2(d0.x, d0.y), make_float2(d0.z, d0.w),
+                                make_float2(d1.x, d1.y), make_float2(d1.z, d1.w)};
+          float2 v[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const float2 x = __ffma2_rn(dd[u], sc2, nam2);
+            const float2 e = __fmul2_rn(x, x);
+            v[u] = make_float2(fast_exp2(-e.x), fast_exp2(-e.y));
+          }
+          store_split8(st + g * kLboF + m * 16, st + kFPlane + g * kLboF + m * 16, v);
         }
-        store_split8(st + g * kLboF + m * 16, st + kFPlane + g * kLboF + m * 16, v);
         fence_proxy_async_smem();
         __syncwarp();
-        if (lane == 0) mbar_arrive(smem_u32(&full[s]));
+        if (lane == 0) {
+          mbar_arrive(smem_u32(&full[sp2[0]]));
+          mbar_arrive(smem_u32(&full[sp2[1]]));
+        }
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(smem_u32(&vec_empty[slot]));  // done with this slot
@@ -569,18 +588,28 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
         item_il[r] = (rest >> 1) * 2;
         if (it < items) item_ok |= 1 << r;
       }
-      for (int kc = 0; kc < nk; ++kc, ++chunk, rp.next(nst)) {
-        const int s = rp.s;
-        if (chunk >= nst && !warp_wait(smem_u32(&empty[s]), rp.ph ^ 1u, abort_s, lane))
+      for (int kc = 0; kc < nk; kc += 2, chunk += 2) {
+        int sp2[2];
+        uint32_t ph2[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          sp2[h] = rp.s;
+          ph2[h] = rp.ph;
+          rp.next(nst);
+        }
+        if (chunk >= nst && !warp_wait(smem_u32(&empty[sp2[0]]), ph2[0] ^ 1u, abort_s, lane))
+          continue;
+        if (chunk + 1 >= nst && !warp_wait(smem_u32(&empty[sp2[1]]), ph2[1] ^ 1u, abort_s, lane))
           continue;
         if (*abort_s) continue;
-        uint8_t* Ahi = smem + s * kStageBytes + 2 * kFPlane;
-        uint8_t* Alo = Ahi + kAPlane;
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
+        for (int hr = 0; hr < 4; ++hr) {
+          const int h = hr & 1, r = hr >> 1;
           if (!(item_ok & (1 << r))) continue;
+          uint8_t* Ahi = smem + sp2[h] * kStageBytes + 2 * kFPlane;
+          uint8_t* Alo = Ahi + kAPlane;
           const int q = item_q[r], g = item_g[r], il0 = item_il[r];
-          const int t0 = kc * kStageK + g * 8;
+          const int t0 = (kc + h) * kStageK + g * 8;
           const float bq = bsm[q] * c2;
           const float2 bq2 = make_float2(bq, bq);
           const float4 d0 = *reinterpret_cast<const float4*>(dsm + t0);
@@ -616,7 +645,10 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
         }
         fence_proxy_async_smem();
         __syncwarp();
-        if (lane == 0) mbar_arrive(smem_u32(&full[s]));
+        if (lane == 0) {
+          mbar_arrive(smem_u32(&full[sp2[0]]));
+          mbar_arrive(smem_u32(&full[sp2[1]]));
+        }
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(smem_u32(&vec_empty[slot]));  // done with this slot
