@@ -128,9 +128,9 @@ mor_norm(double a, double b)
 //         Y = n H / (sqrt(2 pi) s D) in FP32 (D in FP64 where not exactly 1).
 // Shared memory: table block | FP32 dn/dlnM | per-k and per-q vectors.
 __host__ __device__ inline size_t
-prep_smem_bytes(size_t stride, int n_hz, int n_hm, int n_m, int n_z)
+prep_smem_bytes(const TableLayout& L, int n_hz, int n_hm, int n_m, int n_z)
 {
-  size_t b = stride * 8;                                   // table block
+  size_t b = (L.off[2] + L.stride - L.off[3]) * 8;         // table block without dn/dlnM
   b += (((size_t)n_hz * n_hm * 4) + 15) & ~size_t(15);     // FP32 dn/dlnM
   b += (size_t)n_m * (8 + 8 + 8 + 4 + 4);                  // alpha, t, kf, xi, pad
   b += (size_t)n_z * (8 + 8 + 4 + 4);                      // beta, u, yi, pad
@@ -138,7 +138,7 @@ prep_smem_bytes(size_t stride, int n_hz, int n_hm, int n_m, int n_z)
   return b + 64;
 }
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
 prep_kernel(PrepArgs a)
 {
   extern __shared__ __align__(16) double psh[];
@@ -152,8 +152,13 @@ prep_kernel(PrepArgs a)
   const int n_m = Gp->n_m, n_z = Gp->n_z, n_m_pad = Gp->n_m_pad, tid = threadIdx.x;
   const TableLayout& L = a.lay;
   const int n_hm = L.n_hm, n_hz = L.n_hz;
-  double* tab = psh;                                                  // [stride]
-  float* h32 = reinterpret_cast<float*>(tab + L.stride);              // [n_hz n_hm]
+  // The small tables (HMF axes, distances, Sigma_crit) are staged in shared
+  // memory; the n_hz x n_hm HMF grid is read once from global memory (FP32
+  // copy for the mixed form), which keeps a CTA small enough for several to
+  // share an SM.
+  const size_t head = L.off[2], tail = L.stride - L.off[3];
+  double* tab = psh;                                                  // [head + tail]
+  float* h32 = reinterpret_cast<float*>(tab + head + tail);           // [n_hz n_hm]
   double* k_alpha = reinterpret_cast<double*>(
     reinterpret_cast<uint8_t*>(h32) + ((((size_t)n_hz * n_hm * 4) + 15) & ~size_t(15)));
   double* k_t = k_alpha + n_m;
@@ -167,7 +172,7 @@ prep_kernel(PrepArgs a)
   __shared__ double red[2];
 
   const double* src = a.tables + (size_t)(a.slot ? a.slot[p] : p) * L.stride;
-  const uint32_t bytes = (uint32_t)(L.stride * sizeof(double));
+  const uint32_t bytes = (uint32_t)((head + tail) * sizeof(double));
   if (tid == 0) {
     timed_out = 0;
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar)) : "memory");
@@ -181,8 +186,14 @@ prep_kernel(PrepArgs a)
     asm volatile(
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
         "r"(smem_addr(tab)),
-      "l"(src), "r"(bytes), "r"(smem_addr(&bar))
+      "l"(src), "r"((uint32_t)(head * sizeof(double))), "r"(smem_addr(&bar))
       : "memory");
+    if (tail)
+      asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+        "[%3];" ::"r"(smem_addr(tab + head)),
+        "l"(src + L.off[3]), "r"((uint32_t)(tail * sizeof(double))), "r"(smem_addr(&bar))
+        : "memory");
   }
   {
     long long t0 = clock64();
@@ -207,15 +218,15 @@ prep_kernel(PrepArgs a)
   }
   double* mh = tab + L.off[0];
   const double* hz = tab + L.off[1];
-  const double* dn = tab + L.off[2];
-  const double* dz = tab + L.off[3];
-  const double* da = tab + L.off[4];
-  const double* sz = tab + L.off[5];
-  const double* sv = tab + L.off[6];
+  const double* __restrict__ dn = src + L.off[2];  // global
+  const double* dz = tab + head;
+  const double* da = tab + head + (L.off[4] - L.off[3]);
+  const double* sz = tab + head + (L.off[5] - L.off[3]);
+  const double* sv = tab + head + (L.off[6] - L.off[3]);
   // HMF mass axis ln(m_h (Omega_M - Omega_nu)) (hmf_t.hh:15-25), in place.
   for (int i = tid; i < n_hm; i += blockDim.x) mh[i] = log(mh[i] * (pt.om - pt.onu));
   if (a.mixed)
-    for (int i = tid; i < n_hz * n_hm; i += blockDim.x) h32[i] = (float)dn[i];
+    for (int i = tid; i < n_hz * n_hm; i += blockDim.x) h32[i] = (float)__ldg(dn + i);
   __syncthreads();
   double* s64 = a.s64 + (size_t)p * Gp->s64_stride;
   float* s32 = a.s32 + (size_t)p * Gp->s32_stride;
@@ -853,7 +864,7 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
     g.s64_stride = e->s64_stride;
     g.s32_stride = e->s32_stride;
   }
-  e->prep_smem = prep_smem_bytes(L.stride, L.n_hz, L.n_hm, e->w_stride, e->nz_max);
+  e->prep_smem = prep_smem_bytes(L, L.n_hz, L.n_hm, e->w_stride, e->nz_max);
   e->direct_smem = ((size_t)e->nI_max * e->nt_max + e->nt_max) * 8;
   if (e->prep_smem > 200 * 1024 || e->direct_smem > 200 * 1024) {
     set_error("y3b_engine_create: per-point tables too large for shared-memory staging");
