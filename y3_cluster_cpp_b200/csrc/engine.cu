@@ -104,10 +104,11 @@ struct PrepArgs {
 __device__ __noinline__ double
 mor_norm_slow(double a, double b)
 {
+  constexpr double kInvSqrt2 = 0.70710678118654752440;
   if (a < -8.5)  // low tail closed: D = Phi(b)
-    return b < 0.0 ? 0.5 * erfc(-b / kSqrt2) : 1.0 - 0.5 * erfc(b / kSqrt2);
+    return b < 0.0 ? 0.5 * erfc(-b * kInvSqrt2) : 1.0 - 0.5 * erfc(b * kInvSqrt2);
   if (b > 8.5)  // high tail closed: D = Phi(-a)
-    return a > 0.0 ? 0.5 * erfc(a / kSqrt2) : 1.0 - 0.5 * erfc(-a / kSqrt2);
+    return a > 0.0 ? 0.5 * erfc(a * kInvSqrt2) : 1.0 - 0.5 * erfc(-a * kInvSqrt2);
   return phi_diff(a, b);
 }
 
@@ -117,6 +118,13 @@ mor_norm(double a, double b)
   if (a < -8.5 && b > 8.5) return 1.0;
   return mor_norm_slow(a, b);
 }
+
+// The mixed form reads D(mu) from a per-point FP64 table: D and dD/dmu at
+// kDTab equally spaced mu over the point's range of alpha_k + beta_q, cubic
+// Hermite interpolation (absolute error ~1e-9 for sigma-scaled spacing 0.03;
+// below D = 1e-3 the direct FP64 value is used, so the relative error stays
+// small in deep tails).
+constexpr int kDTab = 1024;
 
 // Per-point prep, one CTA per point.  The point's packed tables are staged
 // into shared memory with one bulk (TMA) copy completing on an mbarrier;
@@ -135,6 +143,7 @@ prep_smem_bytes(const TableLayout& L, int n_hz, int n_hm, int n_m, int n_z)
   b += (size_t)n_m * (8 + 8 + 8 + 4 + 4);                  // alpha, t, kf, xi, pad
   b += (size_t)n_z * (8 + 8 + 4 + 4);                      // beta, u, yi, pad
   b += (size_t)n_m * 12;                                   // FP32 t, kf, alpha - A0
+  b += 8 + 2 * (size_t)kDTab * 8;                          // D(mu) table (mixed form)
   return b + 64;
 }
 
@@ -169,7 +178,7 @@ prep_kernel(PrepArgs a)
   int* q_y = k_x + n_m;
   __shared__ __align__(8) uint64_t bar;
   __shared__ int timed_out;
-  __shared__ double red[2];
+  __shared__ double red[4];
 
   const double* src = a.tables + (size_t)(a.slot ? a.slot[p] : p) * L.stride;
   const uint32_t bytes = (uint32_t)((head + tail) * sizeof(double));
@@ -307,6 +316,8 @@ prep_kernel(PrepArgs a)
       }
       red[0] = 0.5 * (amin + amax);
       red[1] = 0.5 * (bmin + bmax);
+      red[2] = amin + bmin;  // range of mu = alpha_k + beta_q
+      red[3] = amax + bmax;
       s64[Gp->o_scal] = red[0];
       s64[Gp->o_scal + 1] = red[1];
     }
@@ -361,6 +372,19 @@ prep_kernel(PrepArgs a)
     kf_f[k] = (float)k_f[k];
     ka_f[k] = (float)(k_alpha[k] - A0);
   }
+  // D(mu) and h dD/dmu = h (phi(a) - phi(b)) / s on the table nodes.
+  double* dtab = reinterpret_cast<double*>(
+    (reinterpret_cast<uintptr_t>(ka_f + n_m) + 7) & ~uintptr_t(7));  // [2 kDTab]
+  const double mu0 = red[2];
+  const double hmu = red[3] > red[2] ? (red[3] - red[2]) / (kDTab - 1) : 1.0;
+  const double inv_hmu = 1.0 / hmu;
+  for (int j = tid; j < kDTab; j += blockDim.x) {
+    const double mu = mu0 + j * hmu;
+    const double aa = (ll_lo - mu) * inv_s, bb = (ll_hi - mu) * inv_s;
+    dtab[j] = mor_norm(aa, bb);
+    dtab[kDTab + j] =
+      hmu * inv_s * (exp(-0.5 * aa * aa) - exp(-0.5 * bb * bb)) / kSqrt2Pi;
+  }
   __syncthreads();
   // One warp per z row; lanes over lnM (no divides, FP32 in the common path).
   const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
@@ -384,7 +408,14 @@ prep_kernel(PrepArgs a)
         float scale = norm0f;
         if (!(mu_rel > mu_sat_lo && mu_rel < mu_sat_hi)) {
           const double mu = k_alpha[k] + q_beta[q];
-          scale = (float)(norm0 / mor_norm_slow((ll_lo - mu) * inv_s, (ll_hi - mu) * inv_s));
+          const double uu = (mu - mu0) * inv_hmu;
+          const int j = min(max((int)uu, 0), kDTab - 2);
+          const double t = uu - j, t2 = t * t, t3 = t2 * t;
+          double D = (2.0 * t3 - 3.0 * t2 + 1.0) * dtab[j] + (t3 - 2.0 * t2 + t) * dtab[kDTab + j] +
+                     (3.0 * t2 - 2.0 * t3) * dtab[j + 1] + (t3 - t2) * dtab[kDTab + j + 1];
+          if (D < 1e-3) D = mor_norm_slow((ll_lo - mu) * inv_s, (ll_hi - mu) * inv_s);
+          // Y is FP32, so is the quotient.
+          scale = norm0f * __frcp_rn((float)D);
         }
         y = n * H * scale;
       }
