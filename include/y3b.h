@@ -281,6 +281,12 @@ int y3b_engine_eval_pooled(y3b_engine* e, int precision, int n,
                            const y3b_point* pts_dev, const double* pool_dev,
                            const int* slot_dev, double* counts_dev,
                            double* shear_dev, void* stream);
+/* CUDA graphs (mode 1, the default): an evaluation whose arguments (precision,
+ * n, the device buffers) repeat a recent call is captured once into a CUDA
+ * graph and replayed from then on, one host launch for the whole sequence of
+ * kernels.  Stage timing (y3b_engine_profile) bypasses the graphs.  mode 0
+ * turns them off and frees the captured graphs. */
+int y3b_engine_set_graphs(y3b_engine* e, int mode);
 /* Wait for the engine's work on `stream` and report device-side errors. */
 int y3b_engine_sync(y3b_engine* e, void* stream);
 /* Optional: the mass weights W_b(lnM_k) of the last eval ([n][n_bins][n_m]

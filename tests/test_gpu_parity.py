@@ -276,3 +276,33 @@ def test_engine_rejects_bad_arguments(gpu):
     with pytest.raises(E.A.Y3BError) as e:
         E.Engine([synthetic.grid(1, n_z=40)], 100, 50, 200, synthetic.plob_baseline())
     assert e.value.status == 7
+
+
+def test_engine_graph_replay_matches_direct_launches(gpu):
+    """Repeated device evaluations are captured once into a CUDA graph and
+    replayed; the replayed results equal those of plain launches bitwise and
+    the launch accounting counts the graph's kernels on every replay."""
+    import ctypes as C
+    import torch
+    g = synthetic.grid(1)
+    eng = _engine([g], n_max=8)
+    pts = synthetic.walkers(6, seed=31, densities=(1,))
+    parr = eng.points_array(pts, grid_of=lambda _: 0)
+    ph = torch.empty(C.sizeof(parr), dtype=torch.uint8)
+    C.memmove(ph.data_ptr(), C.addressof(parr), C.sizeof(parr))
+    pd = ph.cuda()
+    tab = torch.tensor(eng.pack(pts)).cuda()
+    out = torch.empty((6, eng.n_bins), dtype=torch.float64, device="cuda")
+    res, launches = [], []
+    for mode in (0, 1):
+        eng.set_graphs(bool(mode))
+        for _ in range(4):                     # 1st plain, 2nd captured, 3rd/4th replayed
+            l0 = E.launch_count()
+            eng.eval_device(E.MIXED, 6, pd.data_ptr(), tab.data_ptr(), out.data_ptr())
+            eng.sync()
+            launches.append(E.launch_count() - l0)
+            res.append(out.cpu().numpy().copy())
+    for r in res[1:]:
+        np.testing.assert_array_equal(r, res[0])
+    assert len(set(launches)) == 1 and launches[0] >= 3
+    eng.close()

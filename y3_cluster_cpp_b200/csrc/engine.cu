@@ -591,6 +591,28 @@ struct y3b_engine {
   y3b::DevBuf<int> status, order, tile_start, tile_list;
   int max_tiles_pp = 0;
   y3b::ContractShape cshape{};
+  int cstages = 0, n_ctas = 0;  // contraction ring depth and persistent CTAs
+  // CUDA graphs of whole evaluations, keyed by their arguments: an
+  // evaluation seen before replays its graph (one launch from the host).
+  struct GraphKey {
+    int prec, n, mask;
+    const void *pts, *tables, *slot, *counts, *shear;
+    bool operator==(const GraphKey& o) const
+    {
+      return prec == o.prec && n == o.n && mask == o.mask && pts == o.pts &&
+             tables == o.tables && slot == o.slot && counts == o.counts && shear == o.shear;
+    }
+  };
+  struct GraphEntry {
+    GraphKey key;
+    cudaGraphExec_t exec;
+    unsigned long long kernels;  // kernel launches the graph holds
+    unsigned long long used;
+  };
+  int graph_mode = 1;                 // 0: off, 1: capture a repeated evaluation
+  std::vector<GraphEntry> graphs;     // at most kMaxGraphs
+  std::vector<GraphKey> seen;         // recent evaluations without a graph
+  unsigned long long graph_clock = 0;
   size_t s64_stride = 0, s32_stride = 0;
   int w_stride = 0, nB_max = 0, nI_max = 0, nz_max = 0, nt_max = 0;
   size_t prep_smem = 0, direct_smem = 0;
@@ -612,6 +634,7 @@ struct y3b_engine {
       cudaEventDestroy(p.a);
       cudaEventDestroy(p.b);
     }
+    for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
     for (auto* g : gbufs) delete g;
     if (stream) cudaStreamDestroy(stream);
   }
@@ -917,6 +940,15 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
     set_error("y3b_engine_create: the contraction needs more shared memory than one CTA has");
     return fail(Y3B_ERR_UNSUPPORTED);
   }
+  e->cstages = contract_stages(e->cshape);
+  {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if ((rc = cuda_status(cudaDeviceGetAttribute(&e->n_ctas, cudaDevAttrMultiProcessorCount, dev),
+                          "cudaDeviceGetAttribute")))
+      return fail(rc);
+  }
+  if ((rc = contract_prepare(e->cshape))) return fail(rc);
   // Contraction schedule: grids with the most expensive tiles (lam_t steps x
   // accumulator columns) first, ties by index.
   {
@@ -1065,9 +1097,9 @@ enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_t
   } else {
     ContractLaunch L{e->d_grids.get(), (int)e->grids.size(), grid_mask, d_pts, n,
                      e->order.get(), e->tile_start.get(), e->tile_list.get(),
-                     (long long)n * e->max_tiles_pp, e->cshape, e->s32.get(), e->W.get(),
-                     e->Wg.get(),
-                     e->w_stride, e->status.get(), s, e->cfg.with_shear && d_shear != nullptr};
+                     (long long)n * e->max_tiles_pp, e->cshape, e->cstages, e->n_ctas,
+                     e->s32.get(), e->W.get(), e->Wg.get(), e->w_stride, e->status.get(), s,
+                     e->cfg.with_shear && d_shear != nullptr};
     const int rc = launch_contract(L);
     if (rc) {
       delete tc;
@@ -1104,6 +1136,68 @@ enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_t
   return Y3B_OK;
 }
 
+constexpr size_t kMaxGraphs = 16;
+constexpr size_t kSeenKeys = 32;
+
+// Runs one evaluation on `s`.  With graphs on (and stage timing off), an
+// evaluation whose arguments were seen before is captured once into a CUDA
+// graph and replayed from then on: one host launch for the whole sequence
+// (status reset, prep, planner, contraction, profiles, final sums).  The
+// graph holds the device pointers of the call, so the buffers must be the
+// same ones (same addresses) when it is replayed, as they are for a repeated
+// call.
+static int
+run(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_tables,
+    const int* d_slot, double* d_counts, double* d_shear, cudaStream_t s, int grid_mask)
+{
+  if (e->graph_mode == 0 || e->prof)
+    return enqueue(e, prec, n, d_pts, d_tables, d_slot, d_counts, d_shear, s, grid_mask);
+  const y3b_engine::GraphKey key{prec, n, grid_mask, d_pts, d_tables, d_slot, d_counts, d_shear};
+  ++e->graph_clock;
+  for (auto& g : e->graphs)
+    if (g.key == key) {
+      g.used = e->graph_clock;
+      Y3B_CUDA(cudaGraphLaunch(g.exec, s));
+      count_launch((unsigned)g.kernels);
+      e->last_n = n;
+      return Y3B_OK;
+    }
+  bool repeated = false;
+  for (const auto& k : e->seen) repeated |= k == key;
+  if (!repeated) {
+    if (e->seen.size() >= kSeenKeys) e->seen.erase(e->seen.begin());
+    e->seen.push_back(key);
+    return enqueue(e, prec, n, d_pts, d_tables, d_slot, d_counts, d_shear, s, grid_mask);
+  }
+  // Capture.  The kernels counted while capturing are the ones the first
+  // replay below runs.
+  const unsigned long long before = g_launches.load();
+  Y3B_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  const int rc = enqueue(e, prec, n, d_pts, d_tables, d_slot, d_counts, d_shear, s, grid_mask);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+  if (rc != Y3B_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  Y3B_CUDA(ce);
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  Y3B_CUDA(ie);
+  if (e->graphs.size() >= kMaxGraphs) {  // evict the least recently used
+    size_t lru = 0;
+    for (size_t i = 1; i < e->graphs.size(); ++i)
+      if (e->graphs[i].used < e->graphs[lru].used) lru = i;
+    cudaGraphExecDestroy(e->graphs[lru].exec);
+    e->graphs.erase(e->graphs.begin() + lru);
+  }
+  e->graphs.push_back({key, exec, g_launches.load() - before, e->graph_clock});
+  Y3B_CUDA(cudaGraphLaunch(exec, s));
+  e->last_n = n;
+  return Y3B_OK;
+}
+
 }  // namespace y3b
 
 extern "C" int
@@ -1124,7 +1218,7 @@ y3b_engine_eval_device(y3b_engine* e, int precision, int n, const y3b_point* pts
   static_assert(sizeof(y3b_point) == sizeof(PointDev), "y3b_point layout");
   cudaStream_t s = stream ? (cudaStream_t)stream : e->stream;
   int mask = (1 << (int)e->grids.size()) - 1;
-  return enqueue(e, precision, n, reinterpret_cast<const PointDev*>(pts_dev), tables_dev,
+  return run(e, precision, n, reinterpret_cast<const PointDev*>(pts_dev), tables_dev,
                  nullptr, counts_dev, shear_dev, s, mask);
 }
 
@@ -1145,7 +1239,7 @@ y3b_engine_eval_pooled(y3b_engine* e, int precision, int n, const y3b_point* pts
   }
   cudaStream_t s = stream ? (cudaStream_t)stream : e->stream;
   int mask = (1 << (int)e->grids.size()) - 1;
-  return enqueue(e, precision, n, reinterpret_cast<const PointDev*>(pts_dev), pool_dev,
+  return run(e, precision, n, reinterpret_cast<const PointDev*>(pts_dev), pool_dev,
                  slot_dev, counts_dev, shear_dev, s, mask);
 }
 
@@ -1206,6 +1300,24 @@ y3b::engine_status_to_host(y3b_engine* e, int* host, cudaStream_t s)
 }
 
 extern "C" int
+y3b_engine_set_graphs(y3b_engine* e, int mode)
+{
+  clear_error();
+  if (!e || (mode != 0 && mode != 1)) {
+    set_error("y3b_engine_set_graphs: mode must be 0 (off) or 1 (on)");
+    return Y3B_ERR_INVALID;
+  }
+  e->graph_mode = mode;
+  if (mode == 0) {
+    Y3B_CUDA(cudaStreamSynchronize(e->stream));
+    for (auto& g : e->graphs) cudaGraphExecDestroy(g.exec);
+    e->graphs.clear();
+    e->seen.clear();
+  }
+  return Y3B_OK;
+}
+
+extern "C" int
 y3b_engine_sync(y3b_engine* e, void* stream)
 {
   clear_error();
@@ -1234,8 +1346,8 @@ y3b_engine_eval(y3b_engine* e, int precision, int n, const y3b_point* pts,
   Y3B_CUDA(cudaMemcpyAsync(e->tables.get(), tables, n * e->lay.stride * sizeof(double),
                            cudaMemcpyHostToDevice, s));
   const bool want_shear = e->cfg.with_shear && shear;
-  Y3B_TRY(enqueue(e, precision, n, e->pts.get(), e->tables.get(), nullptr, e->counts.get(),
-                  want_shear ? e->shear_out.get() : nullptr, s, mask));
+  Y3B_TRY(run(e, precision, n, e->pts.get(), e->tables.get(), nullptr, e->counts.get(),
+              want_shear ? e->shear_out.get() : nullptr, s, mask));
   Y3B_CUDA(cudaMemcpyAsync(counts, e->counts.get(), (size_t)n * e->nB_max * sizeof(double),
                            cudaMemcpyDeviceToHost, s));
   if (want_shear)

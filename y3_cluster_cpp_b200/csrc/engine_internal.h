@@ -91,6 +91,8 @@ struct ContractLaunch {
   int* tile_list;           // [max_tiles] device scratch: (point << 8) | local tile
   long long max_tiles;      // upper bound of the launch's tiles (grid size)
   ContractShape shape;
+  int stages;               // ring depth, 2..contract_stages(shape)
+  int n_ctas;               // persistent CTAs (at most one per SM)
   float* s32;               // FP32 scratch base
   double* W;                // [n][nB][w_stride]
   double* Wg;
@@ -105,6 +107,8 @@ struct ContractLaunch {
 int launch_contract(const ContractLaunch& L);
 size_t contract_smem_bytes(const ContractShape& c);  // (size_t)-1 if it does not fit
 int contract_stages(const ContractShape& c);
+// Sets the kernels' shared-memory limit once, outside any stream capture.
+int contract_prepare(const ContractShape& c);
 
 // Enqueues a copy of the engine's device status word (the result of the
 // device-side checks of the evaluations enqueued before it on `s`) to `host`.

@@ -834,18 +834,22 @@ contract_smem_bytes(const ContractShape& c)
 
 template <int NJ, bool SHEAR>
 static int
+set_attr_nj(size_t smem)
+{
+  Y3B_CUDA(cudaFuncSetAttribute(contract_kernel<NJ, SHEAR>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  return Y3B_OK;
+}
+
+template <int NJ, bool SHEAR>
+static int
 launch_nj(const ContractLaunch& L, size_t smem)
 {
   auto k = contract_kernel<NJ, SHEAR>;
-  Y3B_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int dev = 0, n_sm = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-  const int blocks = (int)std::min<long long>(std::max<long long>(L.max_tiles, 1), n_sm);
+  const int blocks = (int)std::min<long long>(std::max<long long>(L.max_tiles, 1), L.n_ctas);
   k<<<blocks, kThreads, smem, L.stream>>>(L.grids, L.pts, L.tile_start, L.tile_list, L.n_points,
                                           L.shape.nz_max, L.shape.ntp_max, L.shape.uk_max,
-                                          contract_stages(L.shape), L.s32, L.W, L.Wg, L.w_stride,
-                                          L.status);
+                                          L.stages, L.s32, L.W, L.Wg, L.w_stride, L.status);
   count_launch();
   return cuda_status(cudaGetLastError(), "contract_kernel");
 }
@@ -870,13 +874,38 @@ launch_shear(const ContractLaunch& L, size_t smem)
 }
 
 int
+contract_prepare(const ContractShape& c)
+{
+  const size_t smem = contract_smem_bytes(c);
+  if (smem == (size_t)-1) {
+    set_error("contract: the grids need more shared memory than one CTA has");
+    return Y3B_ERR_UNSUPPORTED;
+  }
+  switch (c.nJ) {
+#define Y3B_ATTR(n) \
+  case n: Y3B_TRY((set_attr_nj<n, false>(smem))); return set_attr_nj<n, true>(smem);
+    Y3B_ATTR(1) Y3B_ATTR(2) Y3B_ATTR(3) Y3B_ATTR(4) Y3B_ATTR(5) Y3B_ATTR(6) Y3B_ATTR(7)
+    Y3B_ATTR(8)
+#undef Y3B_ATTR
+    default:
+      set_error("contract: n_z_bins must be 1..8");
+      return Y3B_ERR_UNSUPPORTED;
+  }
+}
+
+int
 launch_contract(const ContractLaunch& L)
 {
+  if (L.stages < 2 || L.stages > contract_stages(L.shape) || L.n_ctas < 1) {
+    set_error("contract: ring depth %d outside [2, %d] or no CTAs", L.stages,
+              contract_stages(L.shape));
+    return Y3B_ERR_INVALID;
+  }
   tile_plan_kernel<<<1, 1024, 0, L.stream>>>(L.grids, L.n_grids, L.grid_mask, L.pts, L.n_points,
                                              L.order, L.tile_start, L.tile_list);
   count_launch();
   Y3B_CUDA(cudaGetLastError());
-  const size_t smem = contract_smem_bytes(L.shape);
+  const size_t smem = contract_smem_at(L.stages, L.shape);
   return L.shear ? launch_shear<true>(L, smem) : launch_shear<false>(L, smem);
 }
 

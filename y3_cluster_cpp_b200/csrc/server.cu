@@ -324,6 +324,13 @@ y3b_server_create(y3b_engine* e, const y3b_server_config* cfg_in, y3b_server** o
   }
   y3b_server* S = new (std::nothrow) y3b_server;
   if (!S) return Y3B_ERR_NOMEM;
+  int rc0;
+  // Launch sizes vary from launch to launch, so captured graphs would rarely
+  // be replayed: the server's launches go straight to the stream.
+  if ((rc0 = y3b_engine_set_graphs(e, 0))) {
+    delete S;
+    return rc0;
+  }
   S->e = e;
   S->cfg = cfg;
   S->info = info;

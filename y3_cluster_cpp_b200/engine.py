@@ -271,6 +271,10 @@ class Engine:
                                            C.c_void_p(shear_dev or None),
                                            C.c_void_p(stream or None)))
 
+    def set_graphs(self, on=True):
+        """CUDA-graph replay of repeated evaluations (on by default)."""
+        check(lib().y3b_engine_set_graphs(self._h, 1 if on else 0))
+
     def profile(self, enable=True):
         check(lib().y3b_engine_profile(self._h, 1 if enable else 0))
 
