@@ -287,6 +287,17 @@ int y3b_engine_eval_pooled(y3b_engine* e, int precision, int n,
  * kernels.  Stage timing (y3b_engine_profile) bypasses the graphs.  mode 0
  * turns them off and frees the captured graphs. */
 int y3b_engine_set_graphs(y3b_engine* e, int mode);
+/* Autotuner: times the tensor-core contraction on the caller's batch (device
+ * buffers as for y3b_engine_eval_device, mixed form) for ring depths 2..8
+ * (what shared memory allows) and, grid by grid, 1/2/4/8 richness bins per
+ * tile (at most 256 accumulator columns), and keeps the fastest for the
+ * engine's life.  Results of different settings differ only by FP32
+ * rounding; once tuned, an engine's results are fixed.  best_ms (optional):
+ * the contraction time of the chosen setting.  Synchronous. */
+int y3b_engine_autotune(y3b_engine* e, int n, const y3b_point* pts_dev,
+                        const double* tables_dev, double* counts_dev, double* best_ms);
+/* The current setting: ring depth and bins per tile of each grid (cap >= grids). */
+int y3b_engine_tuning(const y3b_engine* e, int* stages, int* bins_per_tile, int cap);
 /* Wait for the engine's work on `stream` and report device-side errors. */
 int y3b_engine_sync(y3b_engine* e, void* stream);
 /* Optional: the mass weights W_b(lnM_k) of the last eval ([n][n_bins][n_m]

@@ -306,3 +306,30 @@ def test_engine_graph_replay_matches_direct_launches(gpu):
         np.testing.assert_array_equal(r, res[0])
     assert len(set(launches)) == 1 and launches[0] >= 3
     eng.close()
+
+
+def test_engine_autotune_keeps_results_within_tolerance(gpu):
+    """The autotuner picks a ring depth and bins per tile from its candidate
+    set; the tuned engine still meets the 1e-4 bar against FP64 and gives a
+    point the same counts alone and in a mixed-density batch."""
+    import ctypes as C
+    import torch
+    grids = [synthetic.grid(1), synthetic.grid(2)]
+    eng = _engine(grids, n_max=16)
+    pts = synthetic.walkers(12, seed=41, densities=(1, 2))
+    gof = {1: 0, 2: 1}
+    parr = eng.points_array(pts, grid_of=lambda p: gof[p.density])
+    ph = torch.empty(C.sizeof(parr), dtype=torch.uint8)
+    C.memmove(ph.data_ptr(), C.addressof(parr), C.sizeof(parr))
+    pd = ph.cuda()
+    tab = torch.tensor(eng.pack(pts)).cuda()
+    out = torch.empty((12, eng.n_bins), dtype=torch.float64, device="cuda")
+    t = eng.autotune(12, pd.data_ptr(), tab.data_ptr(), out.data_ptr())
+    assert 2 <= t["stages"] <= 8 and t["contraction_ms"] > 0
+    assert all(b in (1, 2, 4, 8) for b in t["bins_per_tile"])
+    r64 = eng.eval(pts, E.FP64, grid_of=lambda p: gof[p.density])["counts"]
+    rmx = eng.eval(pts, E.MIXED, grid_of=lambda p: gof[p.density])["counts"]
+    assert np.max(np.abs(rmx / r64 - 1)) <= TOLMIX
+    alone = eng.eval(pts[5:6], E.MIXED, grid_of=lambda p: gof[p.density])["counts"]
+    np.testing.assert_array_equal(alone[0], rmx[5])
+    eng.close()

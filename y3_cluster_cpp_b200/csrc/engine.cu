@@ -589,7 +589,7 @@ struct y3b_engine {
   y3b::DevBuf<double> tables, s64, W, Wg, Phi, counts, shear_out;
   y3b::DevBuf<float> s32;
   y3b::DevBuf<int> status, order, tile_start, tile_list;
-  int max_tiles_pp = 0;
+  int max_tiles_pp = 0, tile_cap_pp = 0;
   y3b::ContractShape cshape{};
   int cstages = 0, n_ctas = 0;  // contraction ring depth and persistent CTAs
   // CUDA graphs of whole evaluations, keyed by their arguments: an
@@ -648,6 +648,31 @@ pad2(size_t n)
   return (n + 1) & ~size_t(1);
 }
 
+// Richness bins per contraction tile (nIc n_z <= 256 accumulator columns)
+// and what follows from it.
+static void
+set_bins_per_tile(GridDev& g, int nIc)
+{
+  g.nIc = nIc;
+  g.n_bg = (g.nI + g.nIc - 1) / g.nIc;
+  g.ncp_c = (g.nIc * g.n_z + 15) / 16 * 16;
+  g.tiles_pp = (g.n_m_pad / kGemmRows) * g.n_bg;
+}
+
+// Most expensive tiles (lam_t steps x accumulator columns) first, ties by index.
+static void
+rank_grids(y3b_engine* e)
+{
+  const int n_grids = (int)e->grids.size();
+  std::vector<int> idx(n_grids);
+  for (int g = 0; g < n_grids; ++g) idx[g] = g;
+  auto cost = [&](int g) { return (long long)e->grids[g].n_t_pad * e->grids[g].ncp_c; };
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return cost(a) > cost(b); });
+  for (int r = 0; r < n_grids; ++r) e->grids[idx[r]].cost_rank = r;
+  e->max_tiles_pp = 0;
+  for (const auto& g : e->grids) e->max_tiles_pp = std::max(e->max_tiles_pp, g.tiles_pp);
+}
+
 static int
 build_grid(y3b_engine* e, int gi)
 {
@@ -667,10 +692,7 @@ build_grid(y3b_engine* e, int gi)
   g.n_t_pad = (g.n_t + kKChunk - 1) / kKChunk * kKChunk;
   g.n_cols = g.nI * g.n_z;
   g.n_cols_pad = (g.n_cols + 15) / 16 * 16;
-  g.nIc = std::max(1, std::min(g.nI, 256 / g.n_z));
-  g.n_bg = (g.nI + g.nIc - 1) / g.nIc;
-  g.ncp_c = (g.nIc * g.n_z + 15) / 16 * 16;
-  g.tiles_pp = (g.n_m_pad / kGemmRows) * g.n_bg;
+  set_bins_per_tile(g, std::max(1, std::min(g.nI, 256 / g.n_z)));
   g.lnm_lo = in.lnm_lo;
   g.lnm_hi = in.lnm_hi;
   g.zt_lo = in.zt_lo;
@@ -949,17 +971,12 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
       return fail(rc);
   }
   if ((rc = contract_prepare(e->cshape))) return fail(rc);
-  // Contraction schedule: grids with the most expensive tiles (lam_t steps x
-  // accumulator columns) first, ties by index.
-  {
-    std::vector<int> idx(n_grids);
-    for (int g = 0; g < n_grids; ++g) idx[g] = g;
-    auto cost = [&](int g) { return (long long)e->grids[g].n_t_pad * e->grids[g].ncp_c; };
-    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return cost(a) > cost(b); });
-    for (int r = 0; r < n_grids; ++r) e->grids[idx[r]].cost_rank = r;
-    e->max_tiles_pp = 0;
-    for (const auto& g : e->grids) e->max_tiles_pp = std::max(e->max_tiles_pp, g.tiles_pp);
-  }
+  // Contraction schedule: grids with the most expensive tiles first.  The
+  // tile list holds the most tiles any tuning can give (one bin per tile).
+  rank_grids(e);
+  e->tile_cap_pp = 0;
+  for (const auto& g : e->grids)
+    e->tile_cap_pp = std::max(e->tile_cap_pp, (g.n_m_pad / kGemmRows) * g.nI);
   // Shear options.
   ShearDev& sh = e->shear;
   std::memset(&sh, 0, sizeof(sh));
@@ -980,7 +997,7 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
   size_t bytes = N * sizeof(PointDev) + N * L.stride * 8 + N * e->s64_stride * 8 +
                  N * e->s32_stride * 4 + 2 * N * e->nB_max * (size_t)e->w_stride * 8 +
                  N * e->nB_max * 8 + (2 * N + 1) * sizeof(int) +
-                 N * (size_t)e->max_tiles_pp * sizeof(int);
+                 N * (size_t)e->tile_cap_pp * sizeof(int);
   if (cfg->with_shear)
     bytes += N * (size_t)e->nI_max * sh.n_R * e->w_stride * 8 + N * e->nB_max * sh.n_R * 8;
   const size_t budget = cfg->hbm_budget ? cfg->hbm_budget : (size_t)150 << 30;
@@ -996,7 +1013,7 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
       (rc = e->Wg.alloc(N * e->nB_max * (size_t)e->w_stride)) ||
       (rc = e->counts.alloc(N * e->nB_max)) || (rc = e->status.alloc(1)) ||
       (rc = e->order.alloc(N)) || (rc = e->tile_start.alloc(N + 1)) ||
-      (rc = e->tile_list.alloc(N * (size_t)e->max_tiles_pp)))
+      (rc = e->tile_list.alloc(N * (size_t)e->tile_cap_pp)))
     return fail(rc);
   if (cfg->with_shear) {
     if ((rc = e->Phi.alloc(N * (size_t)e->nI_max * sh.n_R * e->w_stride)) ||
@@ -1405,5 +1422,121 @@ y3b_engine_profile_read(y3b_engine* e, double* ms, int* n_evals)
   e->pending.clear();
   for (int i = 0; i < 4; ++i) ms[i] = e->prof_ms[i];
   if (n_evals) *n_evals = e->prof_evals;
+  return Y3B_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner: ring depth of the contraction and richness bins per tile of each
+// grid, chosen by timing the contraction stage on the caller's batch.
+
+namespace y3b {
+
+// Mean contraction milliseconds of `reps` evaluations with the current
+// settings (one untimed evaluation first).
+static int
+time_contraction(y3b_engine* e, int n, const PointDev* d_pts, const double* d_tables,
+                 double* d_counts, cudaStream_t s, int reps, double* ms)
+{
+  Y3B_TRY(enqueue(e, Y3B_MIXED, n, d_pts, d_tables, nullptr, d_counts, nullptr, s,
+                  (1 << (int)e->grids.size()) - 1));
+  Y3B_TRY(y3b_engine_profile(e, 1));
+  for (int r = 0; r < reps; ++r)
+    Y3B_TRY(enqueue(e, Y3B_MIXED, n, d_pts, d_tables, nullptr, d_counts, nullptr, s,
+                    (1 << (int)e->grids.size()) - 1));
+  double st[4];
+  int ne = 0;
+  const int rc = y3b_engine_profile_read(e, st, &ne);
+  y3b_engine_profile(e, 0);
+  Y3B_TRY(rc);
+  Y3B_TRY(read_device_status(e->status.get(), s));
+  *ms = st[1] / std::max(ne, 1);
+  return Y3B_OK;
+}
+
+static int
+upload_grids(y3b_engine* e)
+{
+  rank_grids(e);
+  Y3B_TRY(e->d_grids.upload(e->grids.data(), e->grids.size(), e->stream));
+  Y3B_CUDA(cudaStreamSynchronize(e->stream));
+  return Y3B_OK;
+}
+
+}  // namespace y3b
+
+extern "C" int
+y3b_engine_autotune(y3b_engine* e, int n, const y3b_point* pts_dev, const double* tables_dev,
+                    double* counts_dev, double* best_ms)
+{
+  using namespace y3b;
+  clear_error();
+  if (!e || n < 1 || n > e->cfg.max_points || !pts_dev || !tables_dev || !counts_dev ||
+      ((uintptr_t)tables_dev & 15u) != 0) {
+    set_error("y3b_engine_autotune: invalid arguments (1 <= n <= max_points, 16-byte aligned "
+              "tables)");
+    return Y3B_ERR_INVALID;
+  }
+  // Tuning changes kernel arguments that captured graphs hold: drop them.
+  const int mode = e->graph_mode;
+  Y3B_TRY(y3b_engine_set_graphs(e, 0));
+  const PointDev* pts = reinterpret_cast<const PointDev*>(pts_dev);
+  cudaStream_t s = e->stream;
+  constexpr int kReps = 3;
+  double best = 0.0;
+  int rc = time_contraction(e, n, pts, tables_dev, counts_dev, s, kReps, &best);
+  // 1. ring depth
+  const int st_max = contract_stages(e->cshape);
+  int best_st = e->cstages;
+  for (int st : {2, 3, 4, 6, 8}) {
+    if (rc || st > st_max || st == best_st) continue;
+    const int keep = e->cstages;
+    e->cstages = st;
+    double ms = 0.0;
+    rc = time_contraction(e, n, pts, tables_dev, counts_dev, s, kReps, &ms);
+    if (!rc && ms < best) {
+      best = ms;
+      best_st = st;
+    } else {
+      e->cstages = keep;
+    }
+  }
+  e->cstages = best_st;
+  // 2. bins per tile, grid by grid
+  for (size_t g = 0; g < e->grids.size() && !rc; ++g) {
+    GridDev& gd = e->grids[g];
+    const int nic_max = std::max(1, std::min(gd.nI, 256 / gd.n_z));
+    int best_nic = gd.nIc;
+    for (int nic : {1, 2, 4, 8}) {
+      if (rc || nic > nic_max || nic == best_nic) continue;
+      set_bins_per_tile(gd, nic);
+      if ((rc = upload_grids(e))) break;
+      double ms = 0.0;
+      rc = time_contraction(e, n, pts, tables_dev, counts_dev, s, kReps, &ms);
+      if (!rc && ms < best) {
+        best = ms;
+        best_nic = nic;
+      }
+    }
+    set_bins_per_tile(gd, best_nic);
+    const int urc = upload_grids(e);
+    if (!rc) rc = urc;
+  }
+  const int grc = y3b_engine_set_graphs(e, mode);
+  if (rc) return rc;
+  Y3B_TRY(grc);
+  if (best_ms) *best_ms = best;
+  return Y3B_OK;
+}
+
+extern "C" int
+y3b_engine_tuning(const y3b_engine* e, int* stages, int* bins_per_tile, int cap)
+{
+  y3b::clear_error();
+  if (!e || !stages || !bins_per_tile || cap < (int)e->grids.size()) {
+    y3b::set_error("y3b_engine_tuning: need room for one entry per grid");
+    return Y3B_ERR_INVALID;
+  }
+  *stages = e->cstages;
+  for (size_t g = 0; g < e->grids.size(); ++g) bins_per_tile[g] = e->grids[g].nIc;
   return Y3B_OK;
 }

@@ -271,6 +271,22 @@ class Engine:
                                            C.c_void_p(shear_dev or None),
                                            C.c_void_p(stream or None)))
 
+    def autotune(self, n, pts_dev, tables_dev, counts_dev):
+        """Tune the contraction (ring depth, bins per tile) on a device batch;
+        returns {"stages", "bins_per_tile", "contraction_ms"}."""
+        ms = C.c_double()
+        check(lib().y3b_engine_autotune(self._h, n, C.c_void_p(pts_dev), C.c_void_p(tables_dev),
+                                        C.c_void_p(counts_dev), C.byref(ms)))
+        out = self.tuning()
+        out["contraction_ms"] = ms.value
+        return out
+
+    def tuning(self):
+        st = C.c_int()
+        nic = (C.c_int * len(self.grids))()
+        check(lib().y3b_engine_tuning(self._h, C.byref(st), nic, len(self.grids)))
+        return {"stages": st.value, "bins_per_tile": list(nic)}
+
     def set_graphs(self, on=True):
         """CUDA-graph replay of repeated evaluations (on by default)."""
         check(lib().y3b_engine_set_graphs(self._h, 1 if on else 0))
