@@ -333,3 +333,30 @@ def test_engine_autotune_keeps_results_within_tolerance(gpu):
     alone = eng.eval(pts[5:6], E.MIXED, grid_of=lambda p: gof[p.density])["counts"]
     np.testing.assert_array_equal(alone[0], rmx[5])
     eng.close()
+
+
+def test_engine_chunked_host_eval_matches_one_launch(gpu):
+    """A large host-buffer evaluation is split into chunks whose copies
+    overlap the previous chunk's kernels; counts and the mass weights equal
+    those of a single device launch over the same batch."""
+    import ctypes as C
+    import torch
+    g = synthetic.grid(1)
+    n = 1100                                  # four chunks
+    eng = _engine([g], n_max=n)
+    uniq = synthetic.walkers(20, seed=51, densities=(1,))
+    pts = [uniq[i % 20] for i in range(n)]
+    tab = eng.pack(pts)
+    r = eng.eval(pts, E.MIXED, tables=tab, grid_of=lambda _: 0, weights=True)
+    parr = eng.points_array(pts, grid_of=lambda _: 0)
+    ph = torch.empty(C.sizeof(parr), dtype=torch.uint8)
+    C.memmove(ph.data_ptr(), C.addressof(parr), C.sizeof(parr))
+    pd, td = ph.cuda(), torch.tensor(tab).cuda()
+    out = torch.empty((n, eng.n_bins), dtype=torch.float64, device="cuda")
+    eng.eval_device(E.MIXED, n, pd.data_ptr(), td.data_ptr(), out.data_ptr())
+    eng.sync()
+    np.testing.assert_array_equal(r["counts"], out.cpu().numpy())
+    W = np.empty_like(r["W"])
+    E.check(E.lib().y3b_engine_weights(eng.handle, n, E.A.ptr(W)))
+    np.testing.assert_array_equal(W, r["W"])
+    eng.close()

@@ -126,6 +126,8 @@ mor_norm(double a, double b)
 // small in deep tails).
 constexpr int kDTab = 1024;
 
+constexpr int kEvalChunks = 4;  // chunks of a large host-buffer evaluation
+
 // Per-point prep, one CTA per point.  The point's packed tables are staged
 // into shared memory with one bulk (TMA) copy completing on an mbarrier;
 // then, per point:
@@ -592,15 +594,22 @@ struct y3b_engine {
   int max_tiles_pp = 0, tile_cap_pp = 0;
   y3b::ContractShape cshape{};
   int cstages = 0, n_ctas = 0;  // contraction ring depth and persistent CTAs
+  // Chunked host-buffer evaluation: copy stream, one event and one pinned
+  // status word per chunk.
+  cudaStream_t xstream = nullptr;
+  cudaEvent_t chunk_ev[y3b::kEvalChunks] = {};
+  int* chunk_status = nullptr;
   // CUDA graphs of whole evaluations, keyed by their arguments: an
   // evaluation seen before replays its graph (one launch from the host).
   struct GraphKey {
     int prec, n, mask;
     const void *pts, *tables, *slot, *counts, *shear;
+    size_t w_off;
     bool operator==(const GraphKey& o) const
     {
       return prec == o.prec && n == o.n && mask == o.mask && pts == o.pts &&
-             tables == o.tables && slot == o.slot && counts == o.counts && shear == o.shear;
+             tables == o.tables && slot == o.slot && counts == o.counts && shear == o.shear &&
+             w_off == o.w_off;
     }
   };
   struct GraphEntry {
@@ -636,6 +645,10 @@ struct y3b_engine {
     }
     for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
     for (auto* g : gbufs) delete g;
+    for (auto ev : chunk_ev)
+      if (ev) cudaEventDestroy(ev);
+    if (chunk_status) cudaFreeHost(chunk_status);
+    if (xstream) cudaStreamDestroy(xstream);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -971,6 +984,15 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
       return fail(rc);
   }
   if ((rc = contract_prepare(e->cshape))) return fail(rc);
+  rc = cuda_status(cudaStreamCreateWithFlags(&e->xstream, cudaStreamNonBlocking), "cudaStreamCreate");
+  for (int c = 0; c < kEvalChunks && !rc; ++c)
+    rc = cuda_status(cudaEventCreateWithFlags(&e->chunk_ev[c], cudaEventDisableTiming),
+                     "cudaEventCreate");
+  if (!rc)
+    rc = cuda_status(cudaHostAlloc((void**)&e->chunk_status, kEvalChunks * sizeof(int),
+                                   cudaHostAllocDefault),
+                     "cudaHostAlloc");
+  if (rc) return fail(rc);
   // Contraction schedule: grids with the most expensive tiles first.  The
   // tile list holds the most tiles any tuning can give (one bin per tile).
   rank_grids(e);
@@ -1086,10 +1108,17 @@ struct StageTimer {
   }
 };
 
+// w_off: index of the call's first point in the engine's W / W^g / Phi
+// buffers (a chunked evaluation keeps every chunk's weights).
 static int
 enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_tables,
-        const int* d_slot, double* d_counts, double* d_shear, cudaStream_t s, int grid_mask)
+        const int* d_slot, double* d_counts, double* d_shear, cudaStream_t s, int grid_mask,
+        size_t w_off = 0)
 {
+  double* W = e->W.get() + w_off * e->nB_max * e->w_stride;
+  double* Wg = e->Wg.get() + w_off * e->nB_max * e->w_stride;
+  double* Phi = e->Phi.get() ? e->Phi.get() + w_off * e->nI_max * e->shear.n_R * e->w_stride
+                             : nullptr;
   Y3B_CUDA(cudaMemsetAsync(e->status.get(), 0, sizeof(int), s));
   if (e->prof) ++e->prof_evals;
   PrepArgs pa{e->d_grids.get(), d_pts, d_tables, d_slot, e->lay, prec == Y3B_MIXED,
@@ -1107,15 +1136,15 @@ enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_t
                                                        grid_mask);
     count_launch();
     Y3B_CUDA(cudaGetLastError());
-    direct_wreduce_kernel<<<n, 256, 0, s>>>(e->d_grids.get(), d_pts, e->s64.get(), e->W.get(),
-                                            e->Wg.get(), e->w_stride, grid_mask);
+    direct_wreduce_kernel<<<n, 256, 0, s>>>(e->d_grids.get(), d_pts, e->s64.get(), W, Wg,
+                                            e->w_stride, grid_mask);
     count_launch();
     Y3B_CUDA(cudaGetLastError());
   } else {
     ContractLaunch L{e->d_grids.get(), (int)e->grids.size(), grid_mask, d_pts, n,
                      e->order.get(), e->tile_start.get(), e->tile_list.get(),
                      (long long)n * e->max_tiles_pp, e->cshape, e->cstages, e->n_ctas,
-                     e->s32.get(), e->W.get(), e->Wg.get(), e->w_stride, e->status.get(), s,
+                     e->s32.get(), W, Wg, e->w_stride, e->status.get(), s,
                      e->cfg.with_shear && d_shear != nullptr};
     const int rc = launch_contract(L);
     if (rc) {
@@ -1131,19 +1160,19 @@ enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_t
     long long blocks = (warps * 32 + 127) / 128;
     if (prec == Y3B_FP64)
       shear_phi_kernel<double><<<(unsigned)blocks, 128, 0, s>>>(
-        e->d_grids.get(), d_pts, n, e->w_stride, e->shear, e->quad.view(), e->Phi.get(),
+        e->d_grids.get(), d_pts, n, e->w_stride, e->shear, e->quad.view(), Phi,
         e->nI_max, grid_mask);
     else
       shear_phi_kernel<float><<<(unsigned)blocks, 128, 0, s>>>(
-        e->d_grids.get(), d_pts, n, e->w_stride, e->shear, e->quad.view(), e->Phi.get(),
+        e->d_grids.get(), d_pts, n, e->w_stride, e->shear, e->quad.view(), Phi,
         e->nI_max, grid_mask);
     count_launch();
     Y3B_CUDA(cudaGetLastError());
   }
   {
     StageTimer t(e, s, 3);
-    finalize_kernel<<<n, 256, 0, s>>>(e->d_grids.get(), d_pts, e->W.get(), e->Wg.get(),
-                                      shear ? e->Phi.get() : nullptr, e->w_stride, e->nB_max,
+    finalize_kernel<<<n, 256, 0, s>>>(e->d_grids.get(), d_pts, W, Wg,
+                                      shear ? Phi : nullptr, e->w_stride, e->nB_max,
                                       e->nI_max, e->shear.n_R, d_counts,
                                       shear ? d_shear : nullptr, grid_mask);
     count_launch();
@@ -1165,11 +1194,13 @@ constexpr size_t kSeenKeys = 32;
 // call.
 static int
 run(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_tables,
-    const int* d_slot, double* d_counts, double* d_shear, cudaStream_t s, int grid_mask)
+    const int* d_slot, double* d_counts, double* d_shear, cudaStream_t s, int grid_mask,
+    size_t w_off = 0)
 {
   if (e->graph_mode == 0 || e->prof)
-    return enqueue(e, prec, n, d_pts, d_tables, d_slot, d_counts, d_shear, s, grid_mask);
-  const y3b_engine::GraphKey key{prec, n, grid_mask, d_pts, d_tables, d_slot, d_counts, d_shear};
+    return enqueue(e, prec, n, d_pts, d_tables, d_slot, d_counts, d_shear, s, grid_mask, w_off);
+  const y3b_engine::GraphKey key{prec,   n,        grid_mask, d_pts, d_tables,
+                                 d_slot, d_counts, d_shear,   w_off};
   ++e->graph_clock;
   for (auto& g : e->graphs)
     if (g.key == key) {
@@ -1184,13 +1215,14 @@ run(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_table
   if (!repeated) {
     if (e->seen.size() >= kSeenKeys) e->seen.erase(e->seen.begin());
     e->seen.push_back(key);
-    return enqueue(e, prec, n, d_pts, d_tables, d_slot, d_counts, d_shear, s, grid_mask);
+    return enqueue(e, prec, n, d_pts, d_tables, d_slot, d_counts, d_shear, s, grid_mask, w_off);
   }
   // Capture.  The kernels counted while capturing are the ones the first
   // replay below runs.
   const unsigned long long before = g_launches.load();
   Y3B_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-  const int rc = enqueue(e, prec, n, d_pts, d_tables, d_slot, d_counts, d_shear, s, grid_mask);
+  const int rc =
+    enqueue(e, prec, n, d_pts, d_tables, d_slot, d_counts, d_shear, s, grid_mask, w_off);
   cudaGraph_t graph = nullptr;
   const cudaError_t ce = cudaStreamEndCapture(s, &graph);
   if (rc != Y3B_OK) {
@@ -1358,20 +1390,60 @@ y3b_engine_eval(y3b_engine* e, int precision, int n, const y3b_point* pts,
   }
   int mask = 0;
   Y3B_TRY(y3b::engine_check_points(e, n, pts, &mask));
-  cudaStream_t s = e->stream;
-  Y3B_CUDA(cudaMemcpyAsync(e->pts.get(), pts, n * sizeof(y3b_point), cudaMemcpyHostToDevice, s));
-  Y3B_CUDA(cudaMemcpyAsync(e->tables.get(), tables, n * e->lay.stride * sizeof(double),
-                           cudaMemcpyHostToDevice, s));
+  // Chunked: chunk c's points and tables are copied on the copy stream while
+  // chunk c-1 is evaluated on the compute stream (with pinned host buffers
+  // the copies overlap the kernels).  Chunks run one after the other on the
+  // compute stream, so they share the per-point scratch; their weights and
+  // outputs land at their own offsets.
+  cudaStream_t s = e->stream, xs = e->xstream;
+  const int chunks = n >= 1024 ? y3b::kEvalChunks : (n >= 256 ? 2 : 1);
+  const int csz = (n + chunks - 1) / chunks;
+  const size_t st = e->lay.stride;
+  const int nB = e->nB_max, nR = e->shear.n_R;
   const bool want_shear = e->cfg.with_shear && shear;
-  Y3B_TRY(run(e, precision, n, e->pts.get(), e->tables.get(), nullptr, e->counts.get(),
-              want_shear ? e->shear_out.get() : nullptr, s, mask));
-  Y3B_CUDA(cudaMemcpyAsync(counts, e->counts.get(), (size_t)n * e->nB_max * sizeof(double),
-                           cudaMemcpyDeviceToHost, s));
-  if (want_shear)
-    Y3B_CUDA(cudaMemcpyAsync(shear, e->shear_out.get(),
-                             (size_t)n * e->nB_max * e->shear.n_R * sizeof(double),
-                             cudaMemcpyDeviceToHost, s));
-  return y3b_engine_sync(e, nullptr);
+  int used = 0;
+  for (int c = 0; c < chunks; ++c) {
+    const int off = c * csz, m = std::min(csz, n - off);
+    if (m <= 0) break;
+    Y3B_CUDA(cudaMemcpyAsync(e->pts.get() + off, pts + off, m * sizeof(y3b_point),
+                             cudaMemcpyHostToDevice, xs));
+    Y3B_CUDA(cudaMemcpyAsync(e->tables.get() + off * st, tables + off * st,
+                             m * st * sizeof(double), cudaMemcpyHostToDevice, xs));
+    Y3B_CUDA(cudaEventRecord(e->chunk_ev[c], xs));
+    used = c + 1;
+  }
+  for (int c = 0; c < used; ++c) {
+    const int off = c * csz, m = std::min(csz, n - off);
+    Y3B_CUDA(cudaStreamWaitEvent(s, e->chunk_ev[c], 0));
+    Y3B_TRY(run(e, precision, m, e->pts.get() + off, e->tables.get() + off * st, nullptr,
+                e->counts.get() + (size_t)off * nB,
+                want_shear ? e->shear_out.get() + (size_t)off * nB * nR : nullptr, s, mask,
+                (size_t)off));
+    Y3B_TRY(y3b::engine_status_to_host(e, e->chunk_status + c, s));
+    Y3B_CUDA(cudaMemcpyAsync(counts + (size_t)off * nB, e->counts.get() + (size_t)off * nB,
+                             (size_t)m * nB * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (want_shear)
+      Y3B_CUDA(cudaMemcpyAsync(shear + (size_t)off * nB * nR,
+                               e->shear_out.get() + (size_t)off * nB * nR,
+                               (size_t)m * nB * nR * sizeof(double), cudaMemcpyDeviceToHost, s));
+  }
+  Y3B_CUDA(cudaStreamSynchronize(s));
+  e->last_n = n;
+  for (int c = 0; c < used; ++c) {
+    const int h = e->chunk_status[c];
+    if (h == y3b::kDevOk) continue;
+    if (h == y3b::kDevDomain) {
+      set_error("y3b engine: a z_t node lies outside distances/z");
+      return Y3B_ERR_DOMAIN;
+    }
+    if (h == y3b::kDevTimeout) {
+      set_error("y3b engine: a bounded device wait ran out");
+      return Y3B_ERR_TIMEOUT;
+    }
+    set_error("y3b engine: device-side check failed (code %d)", h);
+    return Y3B_ERR_INVALID;
+  }
+  return Y3B_OK;
 }
 
 extern "C" int
