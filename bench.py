@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--density", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=2, help="points in the CPU baseline sample")
+    ap.add_argument("--no-extra-workloads", dest="extra_workloads", action="store_false",
+                    help="skip the batched-uneven and DeltaSigma measurements")
     ap.add_argument("--serve-requests", type=int, default=256,
                     help="requests in the serving stream (0: skip the serving measurement)")
     return ap.parse_args()
@@ -178,6 +180,82 @@ def run_reference(a):
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def _device_batch(eng, pts, grid_of, dev):
+    """Packed device buffers (points, tables) of a walker list."""
+    import torch
+    parr = eng.points_array(pts, grid_of=grid_of)
+    ph = torch.empty(C.sizeof(parr), dtype=torch.uint8, pin_memory=True)
+    C.memmove(ph.data_ptr(), C.addressof(parr), C.sizeof(parr))
+    return ph.to(dev), torch.tensor(eng.pack(pts)).to(dev)
+
+
+def workload_run(name, grids, dens, n_points, shear, steps, dev):
+    """One evaluation per step of `n_points` walkers (each with its own HMF,
+    dV/dz and Sigma_crit tables) over `grids`, counts and, with `shear`, the
+    stacked miscentred DeltaSigma; mixed form, device-resident inputs, L2
+    flushed between steps, one CUDA-graph replay per step.  The FP64 form on
+    the same batch gives the relative errors."""
+    import numpy as np
+    import torch
+
+    from y3_cluster_cpp_b200 import engine, synthetic
+
+    gi = {d: i for i, d in enumerate(dens)}
+    pts = synthetic.walkers(n_points, seed=1, densities=dens)
+    t0 = pts[0].tables
+    pz, pc = synthetic.plob_baseline()
+    eng = engine.Engine(grids, len(t0["hmf_m_h"]), len(t0["hmf_z"]), len(t0["dist_z"]),
+                        (pz, pc), max_points=n_points, n_sci=len(t0["sci_z"]), shear=shear)
+    pd, td = _device_batch(eng, pts, lambda p: gi[p.density], dev)
+    nb, nr = eng.n_bins, eng.n_R
+    cd = torch.empty((n_points, nb), dtype=torch.float64, device=dev)
+    sd = torch.empty((n_points, nb, max(nr, 1)), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+
+    def step(prec):
+        eng.eval_device(prec, n_points, pd.data_ptr(), td.data_ptr(), cd.data_ptr(),
+                        sd.data_ptr() if nr else 0, sp)
+
+    tuning = eng.autotune(n_points, pd.data_ptr(), td.data_ptr(), cd.data_ptr())
+    step(engine.FP64)
+    eng.sync(sp)
+    c64, s64 = cd.cpu().numpy().copy(), sd.cpu().numpy().copy()
+    step(engine.MIXED)
+    eng.sync(sp)
+    cmx, smx = cd.cpu().numpy().copy(), sd.cpu().numpy().copy()
+    err_c = float(np.max(np.abs(cmx / c64 - 1)))
+    err_s = float(np.max(np.abs(smx / s64 - 1))) if nr else None
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    for _ in range(3):
+        flush.zero_()
+        step(engine.MIXED)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    torch.cuda.synchronize(dev)
+    for e0, e1 in ev:
+        flush.zero_()
+        e0.record(stream)
+        step(engine.MIXED)
+        e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in ev) / steps
+    eng.profile(True)
+    for _ in range(3):
+        flush.zero_()
+        step(engine.MIXED)
+    prof = eng.profile_read()
+    eng.profile(False)
+    eng.sync(sp)
+    tot = sum(prof[k] for k in ("prep", "contraction", "shear", "final"))
+    eng.close()
+    return {"workload": name, "points_per_step": n_points, "value": n_points / (ms / 1e3),
+            "unit": UNIT, "ms_per_step": ms, "steps": steps,
+            "max_rel_err_counts_vs_fp64": err_c, "max_rel_err_delta_sigma_vs_fp64": err_s,
+            "stage_share": {k: prof[k] / tot for k in ("prep", "contraction", "shear", "final")},
+            "tuning": tuning, "l2": "flushed between steps", "cuda_graph": True}
 
 
 def serving_run(a, rank, dev):
@@ -401,6 +479,19 @@ def run_ours(a):
     serving = None
     if a.serve_requests > 0:
         serving = serving_run(a, rank, dev)
+    extra = None
+    if a.extra_workloads:
+        from y3_cluster_cpp_b200 import synthetic as _syn
+        sh15 = _syn.shear_opts(n_theta=64, n_s=128, n_R=15)
+        extra = [
+            workload_run("batched: 256 walkers, 1x/2x/4x grids in thirds, counts + stacked "
+                         "miscentred DeltaSigma (15 R)",
+                         [_syn.grid(1), _syn.grid(2), _syn.grid(4)], (1, 2, 4), 256, sh15,
+                         a.steps, dev),
+            workload_run("DeltaSigma: stacked miscentred NFW one-halo, 12 bins x 15 R "
+                         "(64 theta x 128 R_mis x 64 lnM x 32 z_t x 64 lam_t), 2048 walkers",
+                         [_syn.grid(1)], (1,), 2048, sh15, a.steps, dev),
+        ]
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -440,6 +531,8 @@ def run_ours(a):
         }
         if serving is not None:
             line["serving"] = serving
+        if extra is not None:
+            line["other_workloads"] = extra
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)

@@ -535,6 +535,73 @@ shear_phi_kernel(const GridDev* grids, const PointDev* pts, int n_points, int w_
   }
 }
 
+// Miscentred profile table for the mixed form.  For a richness bin i and a
+// radius R the ratio x_mis / x = r_mis,i / R does not depend on the point or
+// the mass, so DeltaSigma_mis(x, x_mis) is a smooth function of u = ln x
+// alone: tabulated once per engine in FP64 at kMisNx nodes per (i, R) pair
+// (the same direct quadrature as the FP64 form), read with 4-point Lagrange
+// interpolation in u (relative error ~1e-8 at this spacing).
+constexpr int kMisNx = 2048;
+
+__global__ void __launch_bounds__(128)
+mis_table_kernel(ShearDev sh, MisQuad quad, int n_pairs, double u0, double du, double* tab)
+{
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= (long long)n_pairs * kMisNx) return;
+  const int pair = (int)(w / kMisNx), j = (int)(w % kMisNx);
+  const int i = pair / sh.n_R, iR = pair % sh.n_R;
+  const double ratio = sh.tau_mis * pow(sh.lob[i] / 100.0, 0.2) / sh.R[iR];
+  const double x = exp(u0 + j * du);
+  const double v = warp_sum(mis_partial<double>(quad, x, ratio * x, true, lane));
+  if (lane == 0) tab[w] = v;
+}
+
+// Phi_i(R, k) of the mixed form from the table, one thread per (point, k):
+// c(M), r_s and the normalisation once, the centred profile once per R, the
+// table read once per (i, R).  A point whose x = R / r_s falls outside the
+// table reports a domain error (the table covers Omega_m from 0.01 to 1 over
+// the engine's masses and radii).
+__global__ void __launch_bounds__(128)
+shear_tab_kernel(const GridDev* grids, const PointDev* pts, int n_points, int w_stride,
+                 ShearDev sh, const double* tab, double u0, double inv_du, double* Phi,
+                 int nI_max, int grid_mask, int* status)
+{
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n_points * w_stride) return;
+  const int p = (int)(t / w_stride), k = (int)(t % w_stride);
+  const PointDev pt = pts[p];
+  if (!grid_in_mask(grid_mask, pt.grid)) return;
+  const GridDev& G = grids[pt.grid];
+  if (k >= G.n_m) return;
+  const double lnM = G.xm[k];
+  const double c = sh.c0 * pow(exp(lnM) / sh.c_pivot, sh.c_slope);
+  const double rho = kRhoCrit * pt.om;
+  const double inv_rs = 1.0 / nfw_rs(lnM, c, rho);
+  const double norm = nfw_norm(lnM, c, rho);
+  bool bad = false;
+  for (int iR = 0; iR < sh.n_R; ++iR) {
+    const double x = sh.R[iR] * inv_rs;
+    const double cen = (1.0 - sh.f_mis) * NfwUnit<double>::dsigma(x);
+    const double tt = (log(x) - u0) * inv_du;
+    int j = (int)floor(tt);
+    if (!(tt >= 1.0 && tt <= kMisNx - 2.0)) {
+      bad = true;
+      j = min(max(j, 1), kMisNx - 3);
+    }
+    const double f = tt - j;
+    const double l0 = -f * (f - 1.0) * (f - 2.0) / 6.0, l1 = (f + 1.0) * (f - 1.0) * (f - 2.0) * 0.5;
+    const double l2 = -(f + 1.0) * f * (f - 2.0) * 0.5, l3 = (f + 1.0) * f * (f - 1.0) / 6.0;
+    for (int i = 0; i < G.nI; ++i) {
+      const double* y = tab + ((size_t)i * sh.n_R + iR) * kMisNx + j;
+      const double mis = l0 * y[-1] + l1 * y[0] + l2 * y[1] + l3 * y[2];
+      Phi[(((size_t)p * nI_max + i) * sh.n_R + iR) * w_stride + k] =
+        norm * (cen + sh.f_mis * mis);
+    }
+  }
+  if (bad) set_err(status, kDevDomain);
+}
+
 // N_b = sum_k w_k W_b(k); N_b(R) = sum_k w_k W^g_b(k) Phi_i(R, k).  CTA per
 // point, warp per output, fixed xor-tree order.
 __global__ void __launch_bounds__(256)
@@ -586,6 +653,8 @@ struct y3b_engine {
   y3b::TableLayout lay;
   y3b::ShearDev shear;
   y3b::MisQuadCache quad;
+  y3b::DevBuf<double> mis_tab;          // [nI_max * n_R][kMisNx], mixed form
+  double mis_u0 = 0.0, mis_du = 1.0;
   cudaStream_t stream = nullptr;
   y3b::DevBuf<y3b::PointDev> pts;
   y3b::DevBuf<double> tables, s64, W, Wg, Phi, counts, shear_out;
@@ -1013,6 +1082,30 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
     sh.c_pivot = cfg->shear.c_pivot;
     rc = e->quad.ensure(cfg->shear.n_theta, cfg->shear.n_s, cfg->shear.s_max, e->stream);
     if (rc) return fail(rc);
+    // Table range of x = R / r_s over the grids' masses, the radii and
+    // Omega_m in [0.01, 1], widened by 1.5 on both sides.
+    double x_lo = 1e300, x_hi = 0.0, r_lo = 1e300, r_hi = 0.0;
+    for (int r = 0; r < sh.n_R; ++r) {
+      r_lo = std::min(r_lo, sh.R[r]);
+      r_hi = std::max(r_hi, sh.R[r]);
+    }
+    for (const auto& g : e->grids)
+      for (double lnM : {g.lnm_lo, g.lnm_hi})
+        for (double om : {0.01, 1.0}) {
+          const double M = std::exp(lnM), c = sh.c0 * std::pow(M / sh.c_pivot, sh.c_slope);
+          const double rs = std::cbrt(3.0 * M / (800.0 * kPi * kRhoCrit * om)) / c;
+          x_lo = std::min(x_lo, r_lo / rs);
+          x_hi = std::max(x_hi, r_hi / rs);
+        }
+    e->mis_u0 = std::log(x_lo / 1.5);
+    e->mis_du = (std::log(x_hi * 1.5) - e->mis_u0) / (kMisNx - 1);
+    const int n_pairs = e->nI_max * sh.n_R;
+    if ((rc = e->mis_tab.alloc((size_t)n_pairs * kMisNx))) return fail(rc);
+    const long long threads = (long long)n_pairs * kMisNx * 32;
+    mis_table_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, e->stream>>>(
+      sh, e->quad.view(), n_pairs, e->mis_u0, e->mis_du, e->mis_tab.get());
+    count_launch();
+    if ((rc = cuda_status(cudaGetLastError(), "mis_table_kernel"))) return fail(rc);
   }
   // Device memory against the HBM budget.
   const size_t N = cfg->max_points;
@@ -1163,9 +1256,9 @@ enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_t
         e->d_grids.get(), d_pts, n, e->w_stride, e->shear, e->quad.view(), Phi,
         e->nI_max, grid_mask);
     else
-      shear_phi_kernel<float><<<(unsigned)blocks, 128, 0, s>>>(
-        e->d_grids.get(), d_pts, n, e->w_stride, e->shear, e->quad.view(), Phi,
-        e->nI_max, grid_mask);
+      shear_tab_kernel<<<(unsigned)(((long long)n * e->w_stride + 127) / 128), 128, 0, s>>>(
+        e->d_grids.get(), d_pts, n, e->w_stride, e->shear, e->mis_tab.get(), e->mis_u0,
+        1.0 / e->mis_du, Phi, e->nI_max, grid_mask, e->status.get());
     count_launch();
     Y3B_CUDA(cudaGetLastError());
   }
