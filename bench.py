@@ -518,7 +518,7 @@ def run_ours(a):
             "roofline": {"bound": "tensor", "achieved": achieved_tf, "peak": peak_tf,
                          "unit": "TFLOP/s", "frac": achieved_tf / peak_tf,
                          "traffic": ncu_traffic(a.density, B),
-                         "kernel": "mixed_gemm_kernel",
+                         "kernel": "contract_kernel",
                          "algorithmic_flops_per_launch": flops_alg,
                          "tensor_pipe_flops_per_launch": 3 * flops_alg,
                          "peak_source": f"bf16_tflops ({peak_kind})",
@@ -545,7 +545,7 @@ def ncu_traffic(density, points):
     ncu capture of the 4x kernel, scaled by the points one launch processes
     (each point reads its own operand vectors, so traffic grows with points)."""
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
-                        "mixed_gemm_kernel_counts_4x.md")
+                        "contract_kernel_counts_4x.md")
     if density != 4 or not os.path.exists(path):
         return None
     m = re.search(r"traffic_bytes_per_point:\s*([0-9.]+)", open(path).read())
