@@ -94,6 +94,8 @@ struct PrepArgs {
   float* s32;
   int* status;
   int grid_mask;
+  uint8_t* fbuf;    // mixed form: F(t, k) blocks, f_stride bytes per point
+  size_t f_stride;
 };
 
 // MOR normalisation D = Phi(b) - Phi(a) in FP64, a = (l_lo - mu)/s,
@@ -138,7 +140,7 @@ constexpr int kEvalChunks = 4;  // chunks of a large host-buffer evaluation
 //         Y = n H / (sqrt(2 pi) s D) in FP32 (D in FP64 where not exactly 1).
 // Shared memory: table block | FP32 dn/dlnM | per-k and per-q vectors.
 __host__ __device__ inline size_t
-prep_smem_bytes(const TableLayout& L, int n_hz, int n_hm, int n_m, int n_z)
+prep_smem_bytes(const TableLayout& L, int n_hz, int n_hm, int n_m, int n_z, int n_t_pad)
 {
   size_t b = (L.off[2] + L.stride - L.off[3]) * 8;         // table block without dn/dlnM
   b += (((size_t)n_hz * n_hm * 4) + 15) & ~size_t(15);     // FP32 dn/dlnM
@@ -146,6 +148,7 @@ prep_smem_bytes(const TableLayout& L, int n_hz, int n_hm, int n_m, int n_z)
   b += (size_t)n_z * (8 + 8 + 4 + 4);                      // beta, u, yi, pad
   b += (size_t)n_m * 12;                                   // FP32 t, kf, alpha - A0
   b += 8 + 2 * (size_t)kDTab * 8;                          // D(mu) table (mixed form)
+  b += 16 + (size_t)n_t_pad * 4;                           // FP32 delta_t (mixed form)
   return b + 64;
 }
 
@@ -424,6 +427,37 @@ prep_kernel(PrepArgs a)
       yrow[k] = y;
     }
   }
+  // F(t, k) = 2^-((delta_t - a_k) sqrt(c1))^2 for the contraction, split into
+  // bf16 hi + lo and written in its shared-memory stage layout: block
+  // (lnM tile, stage) of kFStageBytes, hi planes then lo planes, each plane
+  // 8 lam_t nodes x 128 rows of 16 bytes.  Rows past n_m are zero.
+  float* dt_f = reinterpret_cast<float*>(
+    (reinterpret_cast<uintptr_t>(dtab + 2 * kDTab) + 15) & ~uintptr_t(15));  // [n_t_pad]
+  for (int t = tid; t < n_t_pad; t += blockDim.x) dt_f[t] = t < n_t ? (float)(Gp->xl[t] - L0) : 0.f;
+  __syncthreads();
+  const float sc1 = sqrtf((float)(1.4426950408889634 * 0.5 / (sig * sig)));
+  const float2 sc2 = make_float2(sc1, sc1);
+  uint8_t* fb = a.fbuf + (size_t)p * a.f_stride;
+  const int nk = n_t_pad / 16, n_g8 = n_t_pad / 8;
+  for (int it = tid; it < n_m_pad * n_g8; it += blockDim.x) {
+    const int m = it % n_m_pad, t8 = it / n_m_pad;
+    const float am = m < n_m ? ka_f[m] * sc1 : 1e18f;
+    const float2 nam2 = make_float2(-am, -am);
+    const float4 d0 = *reinterpret_cast<const float4*>(dt_f + t8 * 8);
+    const float4 d1 = *reinterpret_cast<const float4*>(dt_f + t8 * 8 + 4);
+    const float2 dd[4] = {make_float2(d0.x, d0.y), make_float2(d0.z, d0.w),
+                          make_float2(d1.x, d1.y), make_float2(d1.z, d1.w)};
+    float2 v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const float2 x = __ffma2_rn(dd[u], sc2, nam2);
+      const float2 e = __fmul2_rn(x, x);
+      v[u] = make_float2(fast_exp2(-e.x), fast_exp2(-e.y));
+    }
+    uint8_t* st = fb + ((size_t)(m >> 7) * nk + (t8 >> 1)) * kFStageBytes + (t8 & 1) * 2048 +
+                  (m & 127) * 16;
+    store_split8(st, st + kFStageBytes / 2, v);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -660,6 +694,8 @@ struct y3b_engine {
   y3b::DevBuf<double> tables, s64, W, Wg, Phi, counts, shear_out;
   y3b::DevBuf<float> s32;
   y3b::DevBuf<int> status, order, tile_start, tile_list;
+  y3b::DevBuf<uint8_t> fbuf;  // F(t, k) stage blocks of the mixed form
+  size_t f_stride = 0;        // bytes per point
   int max_tiles_pp = 0, tile_cap_pp = 0;
   y3b::ContractShape cshape{};
   int cstages = 0, n_ctas = 0;  // contraction ring depth and persistent CTAs
@@ -1022,7 +1058,9 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
     g.s64_stride = e->s64_stride;
     g.s32_stride = e->s32_stride;
   }
-  e->prep_smem = prep_smem_bytes(L, L.n_hz, L.n_hm, e->w_stride, e->nz_max);
+  int ntp_max = 0;
+  for (const auto& g : e->grids) ntp_max = std::max(ntp_max, g.n_t_pad);
+  e->prep_smem = prep_smem_bytes(L, L.n_hz, L.n_hm, e->w_stride, e->nz_max, ntp_max);
   e->direct_smem = ((size_t)e->nI_max * e->nt_max + e->nt_max) * 8;
   if (e->prep_smem > 200 * 1024 || e->direct_smem > 200 * 1024) {
     set_error("y3b_engine_create: per-point tables too large for shared-memory staging");
@@ -1113,6 +1151,10 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
                  N * e->s32_stride * 4 + 2 * N * e->nB_max * (size_t)e->w_stride * 8 +
                  N * e->nB_max * 8 + (2 * N + 1) * sizeof(int) +
                  N * (size_t)e->tile_cap_pp * sizeof(int);
+  for (const auto& g : e->grids)
+    e->f_stride = std::max(e->f_stride, (size_t)(g.n_m_pad / kGemmRows) * (g.n_t_pad / 16) *
+                                          kFStageBytes);
+  bytes += N * e->f_stride;
   if (cfg->with_shear)
     bytes += N * (size_t)e->nI_max * sh.n_R * e->w_stride * 8 + N * e->nB_max * sh.n_R * 8;
   const size_t budget = cfg->hbm_budget ? cfg->hbm_budget : (size_t)150 << 30;
@@ -1128,7 +1170,8 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
       (rc = e->Wg.alloc(N * e->nB_max * (size_t)e->w_stride)) ||
       (rc = e->counts.alloc(N * e->nB_max)) || (rc = e->status.alloc(1)) ||
       (rc = e->order.alloc(N)) || (rc = e->tile_start.alloc(N + 1)) ||
-      (rc = e->tile_list.alloc(N * (size_t)e->tile_cap_pp)))
+      (rc = e->tile_list.alloc(N * (size_t)e->tile_cap_pp)) ||
+      (rc = e->fbuf.alloc(N * e->f_stride)))
     return fail(rc);
   if (cfg->with_shear) {
     if ((rc = e->Phi.alloc(N * (size_t)e->nI_max * sh.n_R * e->w_stride)) ||
@@ -1215,7 +1258,7 @@ enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_t
   Y3B_CUDA(cudaMemsetAsync(e->status.get(), 0, sizeof(int), s));
   if (e->prof) ++e->prof_evals;
   PrepArgs pa{e->d_grids.get(), d_pts, d_tables, d_slot, e->lay, prec == Y3B_MIXED,
-              e->s64.get(), e->s32.get(), e->status.get(), grid_mask};
+              e->s64.get(), e->s32.get(), e->status.get(), grid_mask, e->fbuf.get(), e->f_stride};
   {
     StageTimer t(e, s, 0);
     prep_kernel<<<n, 256, e->prep_smem, s>>>(pa);
@@ -1237,6 +1280,7 @@ enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_t
     ContractLaunch L{e->d_grids.get(), (int)e->grids.size(), grid_mask, d_pts, n,
                      e->order.get(), e->tile_start.get(), e->tile_list.get(),
                      (long long)n * e->max_tiles_pp, e->cshape, e->cstages, e->n_ctas,
+                     e->fbuf.get(), e->f_stride,
                      e->s32.get(), W, Wg, e->w_stride, e->status.get(), s,
                      e->cfg.with_shear && d_shear != nullptr};
     const int rc = launch_contract(L);

@@ -20,6 +20,10 @@ constexpr int kMaxR = 32;
 constexpr int kGemmRows = 128;   // MMA M (lnM rows per CTA)
 constexpr int kKChunk = 32;      // lam_t nodes per pipeline stage
 constexpr int kMaxCols = 512;    // TMEM columns = n_lam_bins * n_z (padded)
+// F(t, k) operand of one contraction stage (16 lam_t nodes x 128 lnM rows),
+// bf16 hi then lo, each as two 2 KB planes of 8 nodes (16-byte rows): the
+// layout of the stage in shared memory, so one bulk copy moves it.
+constexpr int kFStageBytes = 8192;
 
 struct GridDev {
   int n_m, n_z, n_t, n_o, n_zo, nI, nJ, nB;
@@ -93,6 +97,8 @@ struct ContractLaunch {
   ContractShape shape;
   int stages;               // ring depth, 2..contract_stages(shape)
   int n_ctas;               // persistent CTAs (at most one per SM)
+  const uint8_t* fbuf;      // F(t, k) stage blocks written by the prep kernel
+  size_t f_stride;          // bytes per point
   float* s32;               // FP32 scratch base
   double* W;                // [n][nB][w_stride]
   double* Wg;

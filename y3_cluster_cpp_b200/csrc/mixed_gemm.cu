@@ -158,40 +158,16 @@ tmem_ld16(uint32_t taddr, float* v)
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Split 8 FP32 values (4 pairs) into bf16 hi + bf16 lo and store one 16-byte
-// core-matrix row of each.  hi rounds to nearest (ties away) on the bit
-// pattern, lo = v - hi is exact in FP32 and keeps its top 16 bits, so
-// |v - hi - lo| <= 2^-16 |v|; the products hi*hi + hi*lo + lo*hi then carry a
-// relative error of a few 2^-17.  Integer and packed-FP32 instructions only:
-// the conversion unit stays free for the exponentials.
-__device__ __forceinline__ void
-store_split8(uint8_t* hi, uint8_t* lo, const float2* v)
-{
-  uint32_t h[4], l[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const uint32_t hx = (__float_as_uint(v[k].x) + 0x8000u) & 0xFFFF0000u;
-    const uint32_t hy = (__float_as_uint(v[k].y) + 0x8000u) & 0xFFFF0000u;
-    const float2 r =
-      __ffma2_rn(make_float2(__uint_as_float(hx), __uint_as_float(hy)), make_float2(-1.f, -1.f), v[k]);
-    h[k] = __byte_perm(hx, hy, 0x7632);
-    l[k] = __byte_perm(__float_as_uint(r.x), __float_as_uint(r.y), 0x7632);
-  }
-  *reinterpret_cast<uint4*>(hi) = make_uint4(h[0], h[1], h[2], h[3]);
-  *reinterpret_cast<uint4*>(lo) = make_uint4(l[0], l[1], l[2], l[3]);
-}
-
 constexpr long long kWaitBudget = 2000000000LL;  // SM cycles (~1 s)
 constexpr int kMmaWarp = 0;        // issues tcgen05.mma
-constexpr int kFWarp0 = 1;         // warps 1..8: F(t, k), thread -> (row, half of the k-step)
-constexpr int kFWarps = 8;
-constexpr int kAWarp0 = 9;         // warps 9..16: A((i, q), t), thread -> (q, half, bin pair)
-constexpr int kAWarps = 8;
-constexpr int kProdWarps = kFWarps + kAWarps;
+constexpr int kAWarp0 = 1;         // warps 1..16: A((i, q), t), thread -> (q, k half, bin)
+constexpr int kAWarps = 16;
+constexpr int kProdWarps = kAWarps;
 constexpr int kEpiWarp0 = 17;      // warps 17..24 drain TMEM (warp w reads lanes 32 (w % 4)..)
 constexpr int kEpiWarps = 8;
 constexpr int kLoadWarp = 25;      // stages the next tile's factor vectors in shared memory
-constexpr int kThreads = 32 * (2 + kProdWarps + kEpiWarps);  // 832
+constexpr int kFLoadWarp = 26;     // copies every stage's F(t, k) block (prep kernel output)
+constexpr int kThreads = 32 * 27;  // 864
 constexpr int kStageK = 16;        // lam_t nodes per pipeline stage (one MMA k-step)
 constexpr int kMaxStages = 8;      // ring depth: what shared memory leaves, at most 8
 constexpr int kAccCols = 256;      // TMEM columns per accumulator buffer (2 buffers)
@@ -389,6 +365,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ pts,
                 const int* __restrict__ tile_start, const int* __restrict__ tile_list,
                 int n_points, int nz_max, int ntp_max, int uk_max, int n_stages,
+                const uint8_t* __restrict__ fbuf, size_t f_stride,
                 const float* __restrict__ s32, double* __restrict__ Wout,
                 double* __restrict__ Wgout, int w_stride, int* status)
 {
@@ -413,17 +390,20 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
   uint64_t* ybar = acc_empty + 2;
   uint64_t* vec_full = ybar + 1;
   uint64_t* vec_empty = vec_full + 2;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(vec_empty + 2);
+  uint64_t* fbar = vec_empty + 2;  // F block of stage s has landed
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(fbar + kMaxStages);
   volatile int* abort_s = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   // Zero the operand ring once: columns a tile does not write stay finite.
   for (uint32_t i = tid * 16u; i < nst * kStageBytes; i += kThreads * 16u)
     *reinterpret_cast<uint4*>(smem + i) = make_uint4(0u, 0u, 0u, 0u);
+  fence_proxy_async_smem();  // the zeros come before the tensor core's reads and the copies
   if (warp == kMmaWarp) tmem_alloc(smem_u32(tmem_slot), 2 * kAccCols);
   if (tid == 0) {
     for (int i = 0; i < nst; ++i) {
       mbar_init(smem_u32(&full[i]), kProdWarps);
       mbar_init(smem_u32(&empty[i]), 1);
+      mbar_init(smem_u32(&fbar[i]), 1);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(smem_u32(&acc_full[b]), 1);
@@ -460,7 +440,8 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
         bool broke = false;
         for (int kc = 0; kc < nk; ++kc, rp.next(nst)) {
           const int s = rp.s;
-          if (!mbar_wait_or_abort(smem_u32(&full[s]), rp.ph, abort_s)) {
+          if (!mbar_wait_or_abort(smem_u32(&full[s]), rp.ph, abort_s) ||
+              !mbar_wait_or_abort(smem_u32(&fbar[s]), rp.ph, abort_s)) {
             broke = true;
             break;
           }
@@ -491,71 +472,9 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
       }
     }
     __syncwarp();
-  } else if (warp < kAWarp0) {
-    // ---------------- F(t, k) = 2^-((delta_t - a_k) sqrt(c1))^2 ----------------
-    const int f = tid - kFWarp0 * 32;
-    const int m = f & (kGemmRows - 1), g = f >> 7;
-    int chunk = 0, jt = 0;
-    RingPos rp;
-    for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++jt) {
-      const Tile T = decode_tile(t, tile_list, pts, grids);
-      const GridDev* G = T.G;
-      const int nk = G->n_t_pad / kStageK;
-      const int slot = jt & 1;
-      const float* vs = vec_s + slot * vec_floats;
-      if (!warp_wait(smem_u32(&vec_full[slot]), (jt >> 1) & 1, abort_s, lane)) continue;
-      const float sc1 = sqrtf(vs[0]);
-      const bool valid = T.mtile * kGemmRows + m < G->n_m;
-      // Rows past n_m get an offset so large that F = 2^-(x^2) is exactly 0.
-      const float am = valid ? vs[4 + m] * sc1 : 1e18f;
-      const float2 sc2 = make_float2(sc1, sc1), nam2 = make_float2(-am, -am);
-      const float* dsm = vs + 132 + nz_max + g * 8;
-      // Two ring stages per iteration (nk is even): twice the independent
-      // work between waits, one fence for both.
-      for (int kc = 0; kc < nk; kc += 2, chunk += 2) {
-        int sp2[2];
-        uint32_t ph2[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          sp2[h] = rp.s;
-          ph2[h] = rp.ph;
-          rp.next(nst);
-        }
-        if (chunk >= nst && !warp_wait(smem_u32(&empty[sp2[0]]), ph2[0] ^ 1u, abort_s, lane))
-          continue;
-        if (chunk + 1 >= nst && !warp_wait(smem_u32(&empty[sp2[1]]), ph2[1] ^ 1u, abort_s, lane))
-          continue;
-        if (*abort_s) continue;
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          uint8_t* st = smem + sp2[h] * kStageBytes;
-          const float4 d0 = *reinterpret_cast<const float4*>(dsm + (kc + h) * kStageK);
-          const float4 d1 = *reinterpret_cast<const float4*>(dsm + (kc + h) * kStageK + 4);
-          const float2 dd[4] = {make_float2(d0.x, d0.y), make_float2(d0.z, d0.w),
-                                make_float2(d1.x, d1.y), make_float2(d1.z, d1.w)};
-          float2 v[4];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const float2 x = __ffma2_rn(dd[u], sc2, nam2);
-            const float2 e = __fmul2_rn(x, x);
-            v[u] = make_float2(fast_exp2(-e.x), fast_exp2(-e.y));
-          }
-          store_split8(st + g * kLboF + m * 16, st + kFPlane + g * kLboF + m * 16, v);
-        }
-        fence_proxy_async_smem();
-        __syncwarp();
-        if (lane == 0) {
-          mbar_arrive(smem_u32(&full[sp2[0]]));
-          mbar_arrive(smem_u32(&full[sp2[1]]));
-        }
-      }
-      __syncwarp();
-      if (lane == 0) mbar_arrive(smem_u32(&vec_empty[slot]));  // done with this slot
-    }
   } else if (warp < kEpiWarp0) {
     // ---------------- A((i, q), t) = u_t K_i(t, q) 2^(delta_t b_q c2) ----------------
     const int a = tid - kAWarp0 * 32;
-    constexpr int kA = kAWarps * 32;
     int chunk = 0, jt = 0;
     RingPos rp;
     for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++jt) {
@@ -563,31 +482,24 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
       const GridDev* G = T.G;
       const int nk = G->n_t_pad / kStageK, n_z = G->n_z, ntp = G->n_t_pad;
       const int i0 = T.bg * G->nIc, nIh = min(G->nIc, G->nI - i0);
-      const int items = 2 * n_z * ((nIh + 1) >> 1);
       const int slot = jt & 1;
       const float* vs = vec_s + slot * vec_floats;
       if (!warp_wait(smem_u32(&vec_full[slot]), (jt >> 1) & 1, abort_s, lane)) continue;
       const float c2 = vs[1];
-      const float* bsm = vs + 4 + kGemmRows;
       const float* dsm = vs + 132 + nz_max;
+      // This thread's item (q, k half, bin): 2 n_z nIh <= 512 items, one each.
+      const int q = a % n_z, rest = a / n_z;
+      const int g = rest & 1, il = rest >> 1;
+      const bool active = il < nIh;
+      const float bq = active ? vs[4 + kGemmRows + q] * c2 : 0.f;
+      const float2 bq2 = make_float2(bq, bq);
       // u_t K_i(t): the staged copy when P(lam_o | lam_t) has no z dependence,
       // else the per-(i, q) rows in global memory.
       const bool uks = G->uk_zindep != 0 && nIh * ntp <= uk_max;
-      const float* uksm = dsm + ntp_max;
-      const float* __restrict__ UK = G->UK;
+      const float* uksm = dsm + ntp_max + il * ntp;
+      const float* __restrict__ ukg = G->UK + ((size_t)((i0 + il) * n_z + q)) * ntp;
       const uint32_t lboA = (uint32_t)G->ncp_c * 16u;
-      // This thread's items (q, k half, bin pair) of the tile: at most two,
-      // since items <= 2 * 256.
-      int item_q[2], item_g[2], item_il[2], item_ok = 0;
-#pragma unroll
-      for (int r = 0; r < 2; ++r) {
-        const int it = a + r * kA;
-        const int q = it % n_z, rest = it / n_z;
-        item_q[r] = q;
-        item_g[r] = rest & 1;
-        item_il[r] = (rest >> 1) * 2;
-        if (it < items) item_ok |= 1 << r;
-      }
+      const uint32_t row_off = (uint32_t)g * lboA + (uint32_t)(il * n_z + q) * 16u;
       for (int kc = 0; kc < nk; kc += 2, chunk += 2) {
         int sp2[2];
         uint32_t ph2[2];
@@ -602,45 +514,32 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
         if (chunk + 1 >= nst && !warp_wait(smem_u32(&empty[sp2[1]]), ph2[1] ^ 1u, abort_s, lane))
           continue;
         if (*abort_s) continue;
+        if (active) {
 #pragma unroll
-        for (int hr = 0; hr < 4; ++hr) {
-          const int h = hr & 1, r = hr >> 1;
-          if (!(item_ok & (1 << r))) continue;
-          uint8_t* Ahi = smem + sp2[h] * kStageBytes + 2 * kFPlane;
-          uint8_t* Alo = Ahi + kAPlane;
-          const int q = item_q[r], g = item_g[r], il0 = item_il[r];
-          const int t0 = (kc + h) * kStageK + g * 8;
-          const float bq = bsm[q] * c2;
-          const float2 bq2 = make_float2(bq, bq);
-          const float4 d0 = *reinterpret_cast<const float4*>(dsm + t0);
-          const float4 d1 = *reinterpret_cast<const float4*>(dsm + t0 + 4);
-          const float2 dd[4] = {make_float2(d0.x, d0.y), make_float2(d0.z, d0.w),
-                                make_float2(d1.x, d1.y), make_float2(d1.z, d1.w)};
-          float2 gq[4];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const float2 x = __fmul2_rn(dd[u], bq2);
-            gq[u] = make_float2(fast_exp2(x.x), fast_exp2(x.y));
-          }
-          const int il1 = min(il0 + 2, nIh);
-          for (int il = il0; il < il1; ++il) {
+          for (int h = 0; h < 2; ++h) {
+            const int t0 = (kc + h) * kStageK + g * 8;
+            const float4 d0 = *reinterpret_cast<const float4*>(dsm + t0);
+            const float4 d1 = *reinterpret_cast<const float4*>(dsm + t0 + 4);
             float4 u0, u1;
             if (uks) {
-              const float4* uk = reinterpret_cast<const float4*>(uksm + il * ntp + t0);
-              u0 = uk[0];
-              u1 = uk[1];
+              u0 = *reinterpret_cast<const float4*>(uksm + t0);
+              u1 = *reinterpret_cast<const float4*>(uksm + t0 + 4);
             } else {
-              const float4* uk = reinterpret_cast<const float4*>(
-                UK + ((size_t)((i0 + il) * n_z + q)) * ntp + t0);
-              u0 = __ldg(uk);
-              u1 = __ldg(uk + 1);
+              u0 = __ldg(reinterpret_cast<const float4*>(ukg + t0));
+              u1 = __ldg(reinterpret_cast<const float4*>(ukg + t0 + 4));
             }
-            const float2 v[4] = {__fmul2_rn(make_float2(u0.x, u0.y), gq[0]),
-                                 __fmul2_rn(make_float2(u0.z, u0.w), gq[1]),
-                                 __fmul2_rn(make_float2(u1.x, u1.y), gq[2]),
-                                 __fmul2_rn(make_float2(u1.z, u1.w), gq[3])};
-            const int row = il * n_z + q;
-            store_split8(Ahi + g * lboA + row * 16, Alo + g * lboA + row * 16, v);
+            const float2 dd[4] = {make_float2(d0.x, d0.y), make_float2(d0.z, d0.w),
+                                  make_float2(d1.x, d1.y), make_float2(d1.z, d1.w)};
+            const float2 uu[4] = {make_float2(u0.x, u0.y), make_float2(u0.z, u0.w),
+                                  make_float2(u1.x, u1.y), make_float2(u1.z, u1.w)};
+            float2 v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const float2 x = __fmul2_rn(dd[u], bq2);
+              v[u] = __fmul2_rn(uu[u], make_float2(fast_exp2(x.x), fast_exp2(x.y)));
+            }
+            uint8_t* Ahi = smem + sp2[h] * kStageBytes + 2 * kFPlane + row_off;
+            store_split8(Ahi, Ahi + kAPlane, v);
           }
         }
         fence_proxy_async_smem();
@@ -668,14 +567,13 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
         const bool uks = G->uk_zindep != 0 && nIh * ntp <= uk_max;
         const float* sp = s32 + (size_t)T.p * G->s32_stride;
         float* vs = vec_s + slot * vec_floats;
-        const uint32_t bytes = 4u * (4 + kGemmRows + n_z + ntp + (uks ? nIh * ntp : 0));
+        const uint32_t bytes = 4u * (4 + n_z + ntp + (uks ? nIh * ntp : 0));
         const uint32_t vb = smem_u32(&vec_full[slot]);
         fence_proxy_async_smem();  // the producers' reads of this slot come first
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(vb),
                      "r"(bytes)
                      : "memory");
         bulk_g2s(vs, sp + G->f_scal, 16u, vb);
-        bulk_g2s(vs + 4, sp + G->f_a + (size_t)T.mtile * kGemmRows, 4u * kGemmRows, vb);
         bulk_g2s(vs + 4 + kGemmRows, sp + G->f_b, 4u * n_z, vb);
         bulk_g2s(vs + 132 + nz_max, sp + G->f_delta, 4u * ntp, vb);
         if (uks)
@@ -689,6 +587,45 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
       for (int jj = max(0, issued - 1); jj <= issued; ++jj) {
         long long t0 = clock64();
         while (!mbar_try_wait(smem_u32(&vec_full[jj & 1]), (jj >> 1) & 1) &&
+               clock64() - t0 < kWaitBudget) {
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == kFLoadWarp) {
+    // ---------------- F(t, k) blocks, one bulk copy per stage ----------------
+    if (lane == 0) {
+      RingPos rp;
+      int chunk = 0;
+      uint32_t issued = 0, last_ph = 0;  // per stage: copy issued, parity of its last use
+      for (int t = blockIdx.x; t < n_tiles && !*abort_s; t += gridDim.x) {
+        const Tile T = decode_tile(t, tile_list, pts, grids);
+        const int nk = T.G->n_t_pad / kStageK;
+        const uint8_t* src =
+          fbuf + (size_t)T.p * f_stride + (size_t)T.mtile * nk * kFStageBytes;
+        bool broke = false;
+        for (int kc = 0; kc < nk; ++kc, ++chunk, rp.next(nst)) {
+          const int s = rp.s;
+          if (chunk >= nst && !mbar_wait_or_abort(smem_u32(&empty[s]), rp.ph ^ 1u, abort_s)) {
+            broke = true;
+            break;
+          }
+          const uint32_t fb = smem_u32(&fbar[s]);
+          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb),
+                       "r"((uint32_t)kFStageBytes)
+                       : "memory");
+          bulk_g2s(smem + s * kStageBytes, src + (size_t)kc * kFStageBytes, kFStageBytes, fb);
+          issued |= 1u << s;
+          last_ph = (last_ph & ~(1u << s)) | (rp.ph << s);
+        }
+        if (broke) break;
+      }
+      // No copy may still be in flight when the CTA's shared memory is
+      // released: wait for the last one issued into every stage (bounded).
+      for (int s = 0; s < nst; ++s) {
+        if (!((issued >> s) & 1u)) continue;
+        long long t0 = clock64();
+        while (!mbar_try_wait(smem_u32(&fbar[s]), (last_ph >> s) & 1u) &&
                clock64() - t0 < kWaitBudget) {
         }
       }
@@ -812,7 +749,7 @@ contract_smem_at(int stages, const ContractShape& c)
              4u * ((size_t)c.nz_max * kGemmRows + 2u * c.nJ * c.nz_max +
                    2u * vec_slot_floats(c.nz_max, c.ntp_max, c.uk_max));
   b = (b + 15) & ~size_t(15);
-  return b + 8 * (2 * kMaxStages + 9) + 16;
+  return b + 8 * (3 * kMaxStages + 9) + 16;
 }
 
 // Ring depth: as many stages (<= 8) as fit next to the Y block and the
@@ -849,7 +786,8 @@ launch_nj(const ContractLaunch& L, size_t smem)
   const int blocks = (int)std::min<long long>(std::max<long long>(L.max_tiles, 1), L.n_ctas);
   k<<<blocks, kThreads, smem, L.stream>>>(L.grids, L.pts, L.tile_start, L.tile_list, L.n_points,
                                           L.shape.nz_max, L.shape.ntp_max, L.shape.uk_max,
-                                          L.stages, L.s32, L.W, L.Wg, L.w_stride, L.status);
+                                          L.stages, L.fbuf, L.f_stride, L.s32, L.W, L.Wg,
+                                          L.w_stride, L.status);
   count_launch();
   return cuda_status(cudaGetLastError(), "contract_kernel");
 }
