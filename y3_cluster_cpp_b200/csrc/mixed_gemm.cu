@@ -169,11 +169,12 @@ constexpr int kLoadWarp = 25;      // stages the next tile's factor vectors in s
 constexpr int kFLoadWarp = 26;     // copies every stage's F(t, k) block (prep kernel output)
 constexpr int kThreads = 32 * 27;  // 864
 constexpr int kStageK = 16;        // lam_t nodes per pipeline stage (one MMA k-step)
-constexpr int kMaxStages = 8;      // ring depth: what shared memory leaves, at most 8
+constexpr int kMaxStages = 8;      // depth of the A ring (tuned), at most 8
+constexpr int kMaxFStages = 16;    // depth of the F ring: what shared memory leaves, at most 16
 constexpr int kAccCols = 256;      // TMEM columns per accumulator buffer (2 buffers)
 constexpr uint32_t kFPlane = kGemmRows * kStageK * 2;        // one bf16 plane of F: 4 KB
 constexpr uint32_t kAPlane = kAccCols * kStageK * 2;         // one bf16 plane of A: 8 KB
-constexpr uint32_t kStageBytes = 2 * kFPlane + 2 * kAPlane;  // hi + lo of both: 24 KB
+constexpr uint32_t kStageBytes = 2 * kAPlane;               // A ring stage, hi + lo: 16 KB
 constexpr uint32_t kLboF = kGemmRows * 16;                   // K-adjacent core matrices of F
 
 __device__ __forceinline__ void
@@ -365,22 +366,23 @@ __global__ void __launch_bounds__(kThreads, 1)
 contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ pts,
                 const int* __restrict__ tile_start, const int* __restrict__ tile_list,
                 int n_points, int nz_max, int ntp_max, int uk_max, int n_stages,
-                const uint8_t* __restrict__ fbuf, size_t f_stride,
+                int n_fstages, const uint8_t* __restrict__ fbuf, size_t f_stride,
                 const float* __restrict__ s32, double* __restrict__ Wout,
                 double* __restrict__ Wgout, int w_stride, int* status)
 {
   extern __shared__ __align__(1024) uint8_t smem[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int n_tiles = __ldg(tile_start + n_points);
-  const int nst = n_stages;
-  float* Ys = reinterpret_cast<float*>(smem + nst * kStageBytes);  // [n_z][128]
+  const int nst = n_stages, nfs = n_fstages;
+  uint8_t* fring = smem + nst * kStageBytes;                          // [nfs][8 KB]
+  float* Ys = reinterpret_cast<float*>(fring + nfs * kFStageBytes);  // [n_z][128]
   float* CN_s = Ys + (size_t)nz_max * kGemmRows;
   float* CG_s = CN_s + NJ * nz_max;
   // Two slots of per-tile factor vectors: scal[4] | a[128] | b[nz_max] |
   // delta[ntp_max] | u_t K_i(t)[uk_max] (all 16-byte aligned).
   const int vec_floats = vec_slot_floats(nz_max, ntp_max, uk_max);
   float* vec_s = CG_s + NJ * nz_max;
-  uint32_t ctl = nst * kStageBytes +
+  uint32_t ctl = nst * kStageBytes + nfs * kFStageBytes +
                  4u * ((uint32_t)nz_max * kGemmRows + 2u * NJ * nz_max + 2u * vec_floats);
   ctl = (ctl + 15u) & ~15u;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + ctl);
@@ -390,8 +392,9 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
   uint64_t* ybar = acc_empty + 2;
   uint64_t* vec_full = ybar + 1;
   uint64_t* vec_empty = vec_full + 2;
-  uint64_t* fbar = vec_empty + 2;  // F block of stage s has landed
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(fbar + kMaxStages);
+  uint64_t* fbar = vec_empty + 2;         // F ring: block landed
+  uint64_t* fempty = fbar + kMaxFStages;  // F ring: MMAs done with the block
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(fempty + kMaxFStages);
   volatile int* abort_s = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   // Zero the operand ring once: columns a tile does not write stay finite.
@@ -403,7 +406,10 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
     for (int i = 0; i < nst; ++i) {
       mbar_init(smem_u32(&full[i]), kProdWarps);
       mbar_init(smem_u32(&empty[i]), 1);
+    }
+    for (int i = 0; i < nfs; ++i) {
       mbar_init(smem_u32(&fbar[i]), 1);
+      mbar_init(smem_u32(&fempty[i]), 1);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(smem_u32(&acc_full[b]), 1);
@@ -425,7 +431,7 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
   if (warp == kMmaWarp) {
     // ---------------- MMA issuer ----------------
     if (lane == 0) {
-      RingPos rp;
+      RingPos rp, rf;
       int j = 0, last_stage = -1, last_parity = 0;
       for (int t = blockIdx.x; t < n_tiles && !*abort_s; t += gridDim.x) {
         const Tile T = decode_tile(t, tile_list, pts, grids);
@@ -438,22 +444,23 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
         const uint32_t idesc = umma_idesc_bf16(kGemmRows, ncp);
         const uint32_t lboA = (uint32_t)ncp * 16u;
         bool broke = false;
-        for (int kc = 0; kc < nk; ++kc, rp.next(nst)) {
-          const int s = rp.s;
+        for (int kc = 0; kc < nk; ++kc, rp.next(nst), rf.next(nfs)) {
+          const int s = rp.s, f = rf.s;
           if (!mbar_wait_or_abort(smem_u32(&full[s]), rp.ph, abort_s) ||
-              !mbar_wait_or_abort(smem_u32(&fbar[s]), rp.ph, abort_s)) {
+              !mbar_wait_or_abort(smem_u32(&fbar[f]), rf.ph, abort_s)) {
             broke = true;
             break;
           }
           tc_fence_after();
-          const uint32_t fh = smem_u32(smem + s * kStageBytes), fl = fh + kFPlane;
-          const uint32_t ah = fh + 2 * kFPlane, al = ah + kAPlane;
+          const uint32_t fh = smem_u32(fring + f * kFStageBytes), fl = fh + kFPlane;
+          const uint32_t ah = smem_u32(smem + s * kStageBytes), al = ah + kAPlane;
           const uint64_t dfh = umma_desc(fh, kLboF, 128), dfl = umma_desc(fl, kLboF, 128);
           const uint64_t dah = umma_desc(ah, lboA, 128), dal = umma_desc(al, lboA, 128);
           umma_bf16(dacc, dfh, dah, idesc, kc != 0);
           umma_bf16(dacc, dfh, dal, idesc, 1u);
           umma_bf16(dacc, dfl, dah, idesc, 1u);
           umma_commit(smem_u32(&empty[s]));
+          umma_commit(smem_u32(&fempty[f]));
           last_stage = s;
           last_parity = (int)rp.ph;
         }
@@ -538,7 +545,7 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
               const float2 x = __fmul2_rn(dd[u], bq2);
               v[u] = __fmul2_rn(uu[u], make_float2(fast_exp2(x.x), fast_exp2(x.y)));
             }
-            uint8_t* Ahi = smem + sp2[h] * kStageBytes + 2 * kFPlane + row_off;
+            uint8_t* Ahi = smem + sp2[h] * kStageBytes + row_off;
             store_split8(Ahi, Ahi + kAPlane, v);
           }
         }
@@ -603,10 +610,22 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
         const int nk = T.G->n_t_pad / kStageK;
         const uint8_t* src =
           fbuf + (size_t)T.p * f_stride + (size_t)T.mtile * nk * kFStageBytes;
+        // Warm L2 with the next tile's F blocks while this tile streams.
+        if (t + (int)gridDim.x < n_tiles) {
+          const Tile Tn = decode_tile(t + gridDim.x, tile_list, pts, grids);
+          const int nkn = Tn.G->n_t_pad / kStageK;
+          const uint8_t* nsrc =
+            fbuf + (size_t)Tn.p * f_stride + (size_t)Tn.mtile * nkn * kFStageBytes;
+          for (int kc = 0; kc < nkn; ++kc)
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(
+                           nsrc + (size_t)kc * kFStageBytes),
+                         "r"((uint32_t)kFStageBytes)
+                         : "memory");
+        }
         bool broke = false;
-        for (int kc = 0; kc < nk; ++kc, ++chunk, rp.next(nst)) {
+        for (int kc = 0; kc < nk; ++kc, ++chunk, rp.next(nfs)) {
           const int s = rp.s;
-          if (chunk >= nst && !mbar_wait_or_abort(smem_u32(&empty[s]), rp.ph ^ 1u, abort_s)) {
+          if (chunk >= nfs && !mbar_wait_or_abort(smem_u32(&fempty[s]), rp.ph ^ 1u, abort_s)) {
             broke = true;
             break;
           }
@@ -614,7 +633,7 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
           asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb),
                        "r"((uint32_t)kFStageBytes)
                        : "memory");
-          bulk_g2s(smem + s * kStageBytes, src + (size_t)kc * kFStageBytes, kFStageBytes, fb);
+          bulk_g2s(fring + s * kFStageBytes, src + (size_t)kc * kFStageBytes, kFStageBytes, fb);
           issued |= 1u << s;
           last_ph = (last_ph & ~(1u << s)) | (rp.ph << s);
         }
@@ -622,7 +641,7 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
       }
       // No copy may still be in flight when the CTA's shared memory is
       // released: wait for the last one issued into every stage (bounded).
-      for (int s = 0; s < nst; ++s) {
+      for (int s = 0; s < nfs; ++s) {
         if (!((issued >> s) & 1u)) continue;
         long long t0 = clock64();
         while (!mbar_try_wait(smem_u32(&fbar[s]), (last_ph >> s) & 1u) &&
@@ -741,32 +760,49 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
   }
 }
 
-// Shared memory of the contraction with `stages` ring stages.
+// Shared memory of the contraction without its F ring, with `stages` A stages.
 static size_t
-contract_smem_at(int stages, const ContractShape& c)
+contract_smem_base(int stages, const ContractShape& c)
 {
   size_t b = (size_t)stages * kStageBytes +
              4u * ((size_t)c.nz_max * kGemmRows + 2u * c.nJ * c.nz_max +
                    2u * vec_slot_floats(c.nz_max, c.ntp_max, c.uk_max));
   b = (b + 15) & ~size_t(15);
-  return b + 8 * (3 * kMaxStages + 9) + 16;
+  return b + 8 * (2 * kMaxStages + 2 * kMaxFStages + 9) + 16;
 }
 
-// Ring depth: as many stages (<= 8) as fit next to the Y block and the
-// vector slots; 0 if not even 2 do.
+// F ring depth that fits next to `stages` A stages (<= 16).
+int
+contract_fstages(int stages, const ContractShape& c)
+{
+  const size_t base = contract_smem_base(stages, c), cap = 227 * 1024;
+  if (base >= cap) return 0;
+  return (int)std::min<size_t>(kMaxFStages, (cap - base) / kFStageBytes);
+}
+
+static size_t
+contract_smem_at(int stages, const ContractShape& c)
+{
+  return contract_smem_base(stages, c) + (size_t)contract_fstages(stages, c) * kFStageBytes;
+}
+
+// Default A ring depth: the deepest (<= 8) that leaves at least 4 F stages;
+// 0 if not even 2 A stages do.
 int
 contract_stages(const ContractShape& c)
 {
   for (int st = kMaxStages; st >= 2; --st)
-    if (contract_smem_at(st, c) <= 227 * 1024) return st;
+    if (contract_fstages(st, c) >= 4) return st;
   return 0;
 }
 
 size_t
 contract_smem_bytes(const ContractShape& c)
 {
-  const int st = contract_stages(c);
-  return st ? contract_smem_at(st, c) : (size_t)-1;
+  size_t m = 0;
+  for (int st = 2; st <= kMaxStages; ++st)
+    if (contract_fstages(st, c) >= 4) m = std::max(m, contract_smem_at(st, c));
+  return m ? m : (size_t)-1;
 }
 
 template <int NJ, bool SHEAR>
@@ -786,7 +822,8 @@ launch_nj(const ContractLaunch& L, size_t smem)
   const int blocks = (int)std::min<long long>(std::max<long long>(L.max_tiles, 1), L.n_ctas);
   k<<<blocks, kThreads, smem, L.stream>>>(L.grids, L.pts, L.tile_start, L.tile_list, L.n_points,
                                           L.shape.nz_max, L.shape.ntp_max, L.shape.uk_max,
-                                          L.stages, L.fbuf, L.f_stride, L.s32, L.W, L.Wg,
+                                          L.stages, contract_fstages(L.stages, L.shape), L.fbuf,
+                                          L.f_stride, L.s32, L.W, L.Wg,
                                           L.w_stride, L.status);
   count_launch();
   return cuda_status(cudaGetLastError(), "contract_kernel");
@@ -834,7 +871,8 @@ contract_prepare(const ContractShape& c)
 int
 launch_contract(const ContractLaunch& L)
 {
-  if (L.stages < 2 || L.stages > contract_stages(L.shape) || L.n_ctas < 1) {
+  if (L.stages < 2 || L.stages > kMaxStages || contract_fstages(L.stages, L.shape) < 4 ||
+      L.n_ctas < 1) {
     set_error("contract: ring depth %d outside [2, %d] or no CTAs", L.stages,
               contract_stages(L.shape));
     return Y3B_ERR_INVALID;
