@@ -398,7 +398,8 @@ prep_kernel(PrepArgs a)
     const float bb = (float)(q_beta[q] - B0);
     const float* hr0 = h32 + q_y[q] * n_hm;
     const float* hr1 = hr0 + n_hm;
-    float* yrow = Yt + (size_t)q * n_m_pad;
+    // Tile-blocked: [lnM tile of 128][z][128], so a tile's block is contiguous.
+    float* yrow = Yt + (size_t)q * kGemmRows;
     for (int k = lane; k < n_m_pad; k += 32) {
       float y = 0.f;
       if (k < n_m) {
@@ -424,7 +425,7 @@ prep_kernel(PrepArgs a)
         }
         y = n * H * scale;
       }
-      yrow[k] = y;
+      yrow[(size_t)(k >> 7) * n_z * kGemmRows + (k & (kGemmRows - 1))] = y;
     }
   }
   // F(t, k) = 2^-((delta_t - a_k) sqrt(c1))^2 for the contraction, split into

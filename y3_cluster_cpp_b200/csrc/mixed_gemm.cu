@@ -358,9 +358,9 @@ tile_plan_kernel(const GridDev* __restrict__ grids, int n_grids, int grid_mask,
 // empty signalled by tcgen05.commit), each thread reading its point's factor
 // vectors straight from global memory, so no producer waits on another;
 // warps 17-24 read TMEM, apply Y(k,q) and the z-bin weights and write
-// W_ij(k) in FP64.  The tile's block of Y (n_z rows of 128 lnM values) is
-// brought into shared memory by bulk async copies issued while the tile's
-// MMAs run.
+// W_ij(k) in FP64.  The tile's block of Y (n_z rows of 128 lnM values,
+// contiguous in the tile-blocked layout) is brought into shared memory by one
+// bulk async copy issued while the tile's MMAs run.
 template <int NJ, bool SHEAR>
 __global__ void __launch_bounds__(kThreads, 1)
 contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ pts,
@@ -662,7 +662,7 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
     for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
       const Tile T = decode_tile(t, tile_list, pts, grids);
       const GridDev* G = T.G;
-      const int n_z = G->n_z, n_m = G->n_m, n_m_pad = G->n_m_pad, nI = G->nI, nB = G->nB;
+      const int n_z = G->n_z, n_m = G->n_m, nI = G->nI, nB = G->nB;
       const int i0 = T.bg * G->nIc, nIh = min(G->nIc, nI - i0);
       const float* __restrict__ sp = s32 + (size_t)T.p * G->s32_stride;
       group_sync(2, kE);  // the previous tile's Y and weights are no longer read
@@ -676,9 +676,10 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
                        : "memory");
         }
         __syncwarp();
-        const float* ysrc = sp + G->f_Yt + (size_t)T.mtile * kGemmRows;
-        for (int q = lane; q < n_z; q += 32)
-          bulk_g2s(Ys + (size_t)q * kGemmRows, ysrc + (size_t)q * n_m_pad, 4u * kGemmRows, yb);
+        // Y is stored tile-blocked ([lnM tile][z][128 rows]): one copy.
+        if (lane == 0)
+          bulk_g2s(Ys, sp + G->f_Yt + (size_t)T.mtile * n_z * kGemmRows,
+                   (uint32_t)n_z * kGemmRows * 4u, yb);
         y_pending = 1;
       }
       for (int u = etid; u < NJ * n_z; u += kE) {
