@@ -209,6 +209,26 @@ prep_kernel(PrepArgs a)
         "l"(src + L.off[3]), "r"((uint32_t)(tail * sizeof(double))), "r"(smem_addr(&bar))
         : "memory");
   }
+  // FP32 copy of the HMF grid for the mixed form, straight from global memory
+  // while the bulk copy of the small tables is in flight (four loads in
+  // flight per thread).
+  if (a.mixed) {
+    const double* __restrict__ dng = src + L.off[2];
+    const int nn = n_hz * n_hm;
+    for (int i0 = tid; i0 < nn; i0 += 4 * blockDim.x) {
+      double v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = i0 + u * blockDim.x;
+        v[u] = i < nn ? __ldg(dng + i) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = i0 + u * blockDim.x;
+        if (i < nn) h32[i] = (float)v[u];
+      }
+    }
+  }
   {
     long long t0 = clock64();
     uint32_t ok = 0;
@@ -239,8 +259,6 @@ prep_kernel(PrepArgs a)
   const double* sv = tab + head + (L.off[6] - L.off[3]);
   // HMF mass axis ln(m_h (Omega_M - Omega_nu)) (hmf_t.hh:15-25), in place.
   for (int i = tid; i < n_hm; i += blockDim.x) mh[i] = log(mh[i] * (pt.om - pt.onu));
-  if (a.mixed)
-    for (int i = tid; i < n_hz * n_hm; i += blockDim.x) h32[i] = (float)__ldg(dn + i);
   __syncthreads();
   double* s64 = a.s64 + (size_t)p * Gp->s64_stride;
   float* s32 = a.s32 + (size_t)p * Gp->s32_stride;
