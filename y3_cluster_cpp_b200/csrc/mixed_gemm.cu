@@ -183,6 +183,36 @@ mbar_arrive(uint32_t addr)
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(addr) : "memory");
 }
 
+// Non-suspending probe of an mbarrier phase (the MMA thread polls: it has
+// nothing else to do and must react at once).
+__device__ __forceinline__ bool
+mbar_test(uint32_t addr, uint32_t parity)
+{
+  uint32_t ok;
+  asm volatile(
+    "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+    "selp.u32 %0, 1, 0, p;\n\t}\n"
+    : "=r"(ok)
+    : "r"(addr), "r"(parity)
+    : "memory");
+  return ok != 0;
+}
+
+// Bounded polling wait for the MMA thread; gives up when another warp aborts.
+__device__ __forceinline__ bool
+mbar_poll_or_abort(uint32_t addr, uint32_t parity, volatile int* abort_flag)
+{
+  long long t0 = clock64();
+  while (!mbar_test(addr, parity)) {
+    if (*abort_flag) return false;
+    if (clock64() - t0 > kWaitBudget) {
+      *abort_flag = 1;
+      return false;
+    }
+  }
+  return true;
+}
+
 // Bounded wait that also gives up as soon as another warp has aborted.
 __device__ __forceinline__ bool
 mbar_wait_or_abort(uint32_t addr, uint32_t parity, volatile int* abort_flag)
@@ -446,8 +476,8 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
         bool broke = false;
         for (int kc = 0; kc < nk; ++kc, rp.next(nst), rf.next(nfs)) {
           const int s = rp.s, f = rf.s;
-          if (!mbar_wait_or_abort(smem_u32(&full[s]), rp.ph, abort_s) ||
-              !mbar_wait_or_abort(smem_u32(&fbar[f]), rf.ph, abort_s)) {
+          if (!mbar_poll_or_abort(smem_u32(&full[s]), rp.ph, abort_s) ||
+              !mbar_poll_or_abort(smem_u32(&fbar[f]), rf.ph, abort_s)) {
             broke = true;
             break;
           }
