@@ -467,7 +467,7 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
         const Tile T = decode_tile(t, tile_list, pts, grids);
         const int ncp = T.G->ncp_c, nk = T.G->n_t_pad / kStageK;
         const int buf = j & 1;
-        if (j >= 2 && !mbar_wait_or_abort(smem_u32(&acc_empty[buf]), ((j >> 1) - 1) & 1, abort_s))
+        if (j >= 2 && !mbar_poll_or_abort(smem_u32(&acc_empty[buf]), ((j >> 1) - 1) & 1, abort_s))
           break;
         tc_fence_after();
         const uint32_t dacc = tmem + (uint32_t)(buf * kAccCols);
@@ -655,7 +655,7 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
         bool broke = false;
         for (int kc = 0; kc < nk; ++kc, ++chunk, rp.next(nfs)) {
           const int s = rp.s;
-          if (chunk >= nfs && !mbar_wait_or_abort(smem_u32(&fempty[s]), rp.ph ^ 1u, abort_s)) {
+          if (chunk >= nfs && !mbar_poll_or_abort(smem_u32(&fempty[s]), rp.ph ^ 1u, abort_s)) {
             broke = true;
             break;
           }
