@@ -235,12 +235,17 @@ group_sync(int id, int count)
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
-// Warp-uniform bounded wait (lane 0 polls, the warp follows).
+// Warp-uniform bounded wait (lane 0 polls briefly, then suspends; the warp
+// follows).
 __device__ __forceinline__ bool
 warp_wait(uint32_t addr, uint32_t parity, volatile int* abort_flag, int lane)
 {
   int ok = 1;
-  if (lane == 0) ok = mbar_wait_or_abort(addr, parity, abort_flag);
+  if (lane == 0) {
+    bool done = false;
+    for (int i = 0; i < 64 && !done; ++i) done = mbar_test(addr, parity);
+    if (!done) ok = mbar_wait_or_abort(addr, parity, abort_flag);
+  }
   return __shfl_sync(0xffffffffu, ok, 0) != 0;
 }
 
