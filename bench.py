@@ -71,29 +71,74 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed
+    region: NVML queried every 2 ms from a background thread (read-only), or
+    nvidia-smi at 100 ms when NVML is not importable."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
+        self.rows = []
+        self.thread = None
         self.proc = None
         self.path = None
+        self.running = False
 
     def start(self):
+        try:
+            import threading
+
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByUUID(self.gpu) if isinstance(self.gpu, str) \
+                else pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.smax = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            masks = [(n, getattr(pynvml, a, 0)) for n, a in self.REASONS]
+
+            def poll():
+                while self.running:
+                    sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                    r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.rows.append((sm, [n for n, m in masks if m and (r & m)]))
+                    time.sleep(0.002)
+
+            self.running = True
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:  # noqa: BLE001 -- fall back to nvidia-smi
+            self.thread = None
+        fields = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={fields}",
                  "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
 
     def stop(self):
+        if self.thread is not None:
+            self.running = False
+            self.thread.join(timeout=2)
+            rows = self.rows
+            if not rows:
+                return {"sm_mhz": None, "sm_max_mhz": self.smax, "reasons": ["no samples"],
+                        "samples": 0, "source": "nvml"}
+            sm = [r[0] for r in rows]
+            loaded = [x for x in sm if x > 0.5 * self.smax] or sm
+            reasons = sorted({n for _, rs in rows for n in rs})
+            return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": self.smax,
+                    "reasons": reasons, "samples": len(rows), "source": "nvml, 2 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -116,7 +161,7 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": smax, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(rows), "source": "nvidia-smi, 100 ms"}
 
 
 def cpu_baseline(density, n_points):
@@ -399,7 +444,12 @@ def run_ours(a):
     torch.cuda.synchronize(dev)
     if world > 1:
         torch.distributed.barrier()
-    clocks = ClockSampler(local)
+    # NVML enumerates every GPU of the host: find ours by UUID.
+    try:
+        gpu_id = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:  # noqa: BLE001
+        gpu_id = local
+    clocks = ClockSampler(gpu_id)
     clocks.start()
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
