@@ -244,6 +244,8 @@ typedef struct {
 
 typedef enum { Y3B_FP64 = 0, Y3B_MIXED = 1 } y3b_precision;
 
+/* An engine (like a server) is used by one host thread at a time; engines
+ * are independent, one per device or per stream if wanted. */
 typedef struct y3b_engine y3b_engine;
 
 int y3b_engine_create(const y3b_grid* grids, int n_grids,

@@ -1558,30 +1558,47 @@ y3b_engine_eval(y3b_engine* e, int precision, int n, const y3b_point* pts,
   const int nB = e->nB_max, nR = e->shear.n_R;
   const bool want_shear = e->cfg.with_shear && shear;
   int used = 0;
-  for (int c = 0; c < chunks; ++c) {
-    const int off = c * csz, m = std::min(csz, n - off);
-    if (m <= 0) break;
-    Y3B_CUDA(cudaMemcpyAsync(e->pts.get() + off, pts + off, m * sizeof(y3b_point),
-                             cudaMemcpyHostToDevice, xs));
-    Y3B_CUDA(cudaMemcpyAsync(e->tables.get() + off * st, tables + off * st,
-                             m * st * sizeof(double), cudaMemcpyHostToDevice, xs));
-    Y3B_CUDA(cudaEventRecord(e->chunk_ev[c], xs));
-    used = c + 1;
+  auto upload = [&]() -> int {
+    for (int c = 0; c < chunks; ++c) {
+      const int off = c * csz, m = std::min(csz, n - off);
+      if (m <= 0) break;
+      Y3B_CUDA(cudaMemcpyAsync(e->pts.get() + off, pts + off, m * sizeof(y3b_point),
+                               cudaMemcpyHostToDevice, xs));
+      Y3B_CUDA(cudaMemcpyAsync(e->tables.get() + off * st, tables + off * st,
+                               m * st * sizeof(double), cudaMemcpyHostToDevice, xs));
+      Y3B_CUDA(cudaEventRecord(e->chunk_ev[c], xs));
+      used = c + 1;
+    }
+    return Y3B_OK;
+  };
+  if (const int rc = upload()) {
+    cudaStreamSynchronize(xs);
+    return rc;
   }
-  for (int c = 0; c < used; ++c) {
-    const int off = c * csz, m = std::min(csz, n - off);
-    Y3B_CUDA(cudaStreamWaitEvent(s, e->chunk_ev[c], 0));
-    Y3B_TRY(run(e, precision, m, e->pts.get() + off, e->tables.get() + off * st, nullptr,
-                e->counts.get() + (size_t)off * nB,
-                want_shear ? e->shear_out.get() + (size_t)off * nB * nR : nullptr, s, mask,
-                (size_t)off));
-    Y3B_TRY(y3b::engine_status_to_host(e, e->chunk_status + c, s));
-    Y3B_CUDA(cudaMemcpyAsync(counts + (size_t)off * nB, e->counts.get() + (size_t)off * nB,
-                             (size_t)m * nB * sizeof(double), cudaMemcpyDeviceToHost, s));
-    if (want_shear)
-      Y3B_CUDA(cudaMemcpyAsync(shear + (size_t)off * nB * nR,
-                               e->shear_out.get() + (size_t)off * nB * nR,
-                               (size_t)m * nB * nR * sizeof(double), cudaMemcpyDeviceToHost, s));
+  auto evaluate = [&]() -> int {
+    for (int c = 0; c < used; ++c) {
+      const int off = c * csz, m = std::min(csz, n - off);
+      Y3B_CUDA(cudaStreamWaitEvent(s, e->chunk_ev[c], 0));
+      Y3B_TRY(run(e, precision, m, e->pts.get() + off, e->tables.get() + off * st, nullptr,
+                  e->counts.get() + (size_t)off * nB,
+                  want_shear ? e->shear_out.get() + (size_t)off * nB * nR : nullptr, s, mask,
+                  (size_t)off));
+      Y3B_TRY(y3b::engine_status_to_host(e, e->chunk_status + c, s));
+      Y3B_CUDA(cudaMemcpyAsync(counts + (size_t)off * nB, e->counts.get() + (size_t)off * nB,
+                               (size_t)m * nB * sizeof(double), cudaMemcpyDeviceToHost, s));
+      if (want_shear)
+        Y3B_CUDA(cudaMemcpyAsync(shear + (size_t)off * nB * nR,
+                                 e->shear_out.get() + (size_t)off * nB * nR,
+                                 (size_t)m * nB * nR * sizeof(double), cudaMemcpyDeviceToHost,
+                                 s));
+    }
+    return Y3B_OK;
+  };
+  if (const int rc = evaluate()) {
+    // Nothing queued may touch the caller's buffers after we return.
+    cudaStreamSynchronize(xs);
+    cudaStreamSynchronize(s);
+    return rc;
   }
   Y3B_CUDA(cudaStreamSynchronize(s));
   e->last_n = n;
