@@ -381,10 +381,11 @@ prep_kernel(PrepArgs a)
   float* __restrict__ Yt = s32 + Gp->f_Yt;
   const float c2 = (float)(1.4426950408889634 / (sig * sig));
   const float norm0f = (float)norm0;
-  // D_kq = 1 exactly when mu is more than 8.5 sigma inside the lam_t domain;
-  // the FP32 test keeps a 1e-3 margin, everything else takes the FP64 path.
-  const float mu_sat_lo = (float)(ll_lo + 8.5 * sig - L0) + 1e-3f;
-  const float mu_sat_hi = (float)(ll_hi - 8.5 * sig - L0) - 1e-3f;
+  // Y is FP32: where mu is more than 5.6 sigma inside the lam_t domain,
+  // 1 - D < 2^-26 and (float)D is exactly 1, the saturated scale.  The FP32
+  // test keeps a 1e-3 margin; everything else reads the FP64 table of D.
+  const float mu_sat_lo = (float)(ll_lo + 5.6 * sig - L0) + 1e-3f;
+  const float mu_sat_hi = (float)(ll_hi - 5.6 * sig - L0) - 1e-3f;
   // FP32 copies of the per-k vectors, reusing the FP64 arrays' space is not
   // possible (they are read below), so they go after them in h32's tail.
   float* kt_f = reinterpret_cast<float*>(q_y + n_z);  // [n_m]
