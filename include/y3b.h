@@ -300,6 +300,11 @@ int y3b_engine_autotune(y3b_engine* e, int n, const y3b_point* pts_dev,
                         const double* tables_dev, double* counts_dev, double* best_ms);
 /* The current setting: ring depth and bins per tile of each grid (cap >= grids). */
 int y3b_engine_tuning(const y3b_engine* e, int* stages, int* bins_per_tile, int cap);
+/* lam_t stages of the last mixed-form contraction: the stages its tiles
+ * issued (each tile skips the stages where the MOR density of all its
+ * (lnM, z) pairs is below e^-21 of its peak) and the stages of the full
+ * lam_t range.  Reads device memory: call after that evaluation completed. */
+int y3b_engine_stage_count(const y3b_engine* e, long long* executed, long long* dense);
 /* Wait for the engine's work on `stream` and report device-side errors. */
 int y3b_engine_sync(y3b_engine* e, void* stream);
 /* Optional: the mass weights W_b(lnM_k) of the last eval ([n][n_bins][n_m]

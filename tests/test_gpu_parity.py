@@ -197,6 +197,27 @@ def test_engine_counts_match_oracle(gpu, density):
     eng.close()
 
 
+def test_engine_stage_window_skips_only_negligible_stages(gpu):
+    """The contraction issues only the lam_t stages inside mu +- 6.5 sigma of
+    each lnM tile: a narrow MOR scatter issues fewer stages, and both stay
+    within tolerance of the oracle's full-range quadrature."""
+    g = synthetic.grid(4)  # two 128-row lnM tiles, each spanning part of the lam_t range
+    eng = _engine([g])
+    pz, pc = synthetic.plob_baseline()
+    issued = {}
+    for sigma in (0.12, 0.35):
+        p = synthetic.fiducial()
+        p.sigma = sigma
+        ref, _, _ = O.direct_eval(g, pz, pc, p.mor, O.cosmo(p.om, p.h0), p.tables)
+        rmx = eng.eval([p], E.MIXED, grid_of=lambda _: 0)["counts"][0]
+        ex, dn = eng.stage_count()
+        assert 0 < ex <= dn
+        issued[sigma] = ex
+        np.testing.assert_allclose(rmx, ref, rtol=TOLMIX)
+    assert issued[0.12] < issued[0.35] and issued[0.12] < dn
+    eng.close()
+
+
 def test_engine_batched_walkers_mixed_densities(gpu):
     """Uneven grids in one call; each point equals its own evaluation alone
     (bitwise) and the oracle (tolerance)."""

@@ -167,6 +167,7 @@ def _declare(L):
     L.y3b_engine_set_graphs.argtypes = [VP, I]
     L.y3b_engine_autotune.argtypes = [VP, I, VP, VP, VP, PD]
     L.y3b_engine_tuning.argtypes = [VP, PI, PI, I]
+    L.y3b_engine_stage_count.argtypes = [VP, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
     L.y3b_server_create.argtypes = [VP, C.POINTER(ServerConfig), C.POINTER(VP)]
     L.y3b_server_submit.argtypes = [VP, I, VP, VP, VP, VP, C.POINTER(C.c_longlong)]
     L.y3b_server_wait.argtypes = [VP, C.c_longlong, D, PD]
@@ -215,7 +216,7 @@ EXPORTED = [
     "y3b_engine_sync", "y3b_engine_weights", "y3b_selftest_wait_timeout",
     "y3b_engine_profile", "y3b_engine_profile_read", "y3b_sel_function_noalloc",
     "y3b_engine_eval_pooled", "y3b_engine_set_graphs", "y3b_engine_autotune",
-    "y3b_engine_tuning", "y3b_server_create", "y3b_server_submit", "y3b_server_wait",
+    "y3b_engine_tuning", "y3b_engine_stage_count", "y3b_server_create", "y3b_server_submit", "y3b_server_wait",
     "y3b_server_stats_read", "y3b_server_destroy", "y3b_planner_create",
     "y3b_planner_destroy", "y3b_planner_submit", "y3b_planner_admit",
     "y3b_planner_next_batch", "y3b_planner_complete", "y3b_planner_free_points",

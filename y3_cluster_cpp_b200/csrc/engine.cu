@@ -183,7 +183,7 @@ prep_kernel(PrepArgs a)
   int* q_y = k_x + n_m;
   __shared__ __align__(8) uint64_t bar;
   __shared__ int timed_out;
-  __shared__ double red[4];
+  __shared__ double red[6];
 
   const double* src = a.tables + (size_t)(a.slot ? a.slot[p] : p) * L.stride;
   const uint32_t bytes = (uint32_t)((head + tail) * sizeof(double));
@@ -341,6 +341,8 @@ prep_kernel(PrepArgs a)
       red[1] = 0.5 * (bmin + bmax);
       red[2] = amin + bmin;  // range of mu = alpha_k + beta_q
       red[3] = amax + bmax;
+      red[4] = bmin;
+      red[5] = bmax;
       s64[Gp->o_scal] = red[0];
       s64[Gp->o_scal + 1] = red[1];
     }
@@ -455,6 +457,54 @@ prep_kernel(PrepArgs a)
     (reinterpret_cast<uintptr_t>(dtab + 2 * kDTab) + 15) & ~uintptr_t(15));  // [n_t_pad]
   for (int t = tid; t < n_t_pad; t += blockDim.x) dt_f[t] = t < n_t ? (float)(Gp->xl[t] - L0) : 0.f;
   __syncthreads();
+  // lam_t window of the contraction per lnM tile: for every (k, q) of the
+  // tile the MOR density exp(-(l_t - mu_kq)^2 / 2 s^2) is below e^-21 of its
+  // peak outside [min mu - 6.5 s, max mu + 6.5 s], so those stages add
+  // nothing at FP32 accumulation; the stage range is rounded to pairs.
+  {
+    constexpr double kWin = 6.5;
+    const int n_mt = n_m_pad / kGemmRows, nk = n_t_pad / 16;
+    int* win = reinterpret_cast<int*>(s32 + Gp->f_win);
+    for (int mt = warp; mt < n_mt; mt += nw) {
+      double amn = 1e300, amx = -1e300;
+      for (int k = mt * kGemmRows + lane; k < min(n_m, (mt + 1) * kGemmRows); k += 32) {
+        amn = fmin(amn, k_alpha[k]);
+        amx = fmax(amx, k_alpha[k]);
+      }
+      for (int off = 16; off > 0; off >>= 1) {
+        amn = fmin(amn, __shfl_xor_sync(0xffffffffu, amn, off));
+        amx = fmax(amx, __shfl_xor_sync(0xffffffffu, amx, off));
+      }
+      if (lane == 0) {
+        int lo = 0, hi = nk;
+        if (amx >= amn) {
+          const float dlo = (float)(amn + red[4] - kWin * sig - L0);
+          const float dhi = (float)(amx + red[5] + kWin * sig - L0);
+          int a = 0, b = n_t;  // first t with delta_t >= dlo (nodes ascend)
+          while (a < b) {
+            const int m = (a + b) >> 1;
+            if (dt_f[m] < dlo) a = m + 1; else b = m;
+          }
+          const int t_lo = a;
+          a = t_lo;
+          b = n_t;  // first t with delta_t > dhi
+          while (a < b) {
+            const int m = (a + b) >> 1;
+            if (dt_f[m] <= dhi) a = m + 1; else b = m;
+          }
+          const int t_hi = a;
+          lo = (t_lo / 16) & ~1;
+          hi = min(nk, (((t_hi + 15) / 16) + 1) & ~1);
+          if (hi <= lo) {  // no node inside: keep one stage pair, all zero anyway
+            lo = min(lo, nk - 2);
+            hi = lo + 2;
+          }
+        }
+        win[2 * mt] = lo;
+        win[2 * mt + 1] = hi;
+      }
+    }
+  }
   const float sc1 = sqrtf((float)(1.4426950408889634 * 0.5 / (sig * sig)));
   const float2 sc2 = make_float2(sc1, sc1);
   uint8_t* fb = a.fbuf + (size_t)p * a.f_stride;
@@ -713,7 +763,9 @@ struct y3b_engine {
   y3b::DevBuf<y3b::PointDev> pts;
   y3b::DevBuf<double> tables, s64, W, Wg, Phi, counts, shear_out;
   y3b::DevBuf<float> s32;
-  y3b::DevBuf<int> status, order, tile_start, tile_list;
+  y3b::DevBuf<int> status, order, tile_start;
+  y3b::DevBuf<int> stage_ct;  // [2] lam_t stages issued / dense, last contraction
+  y3b::DevBuf<int2> tile_list;
   y3b::DevBuf<uint8_t> fbuf;  // F(t, k) stage blocks of the mixed form
   size_t f_stride = 0;        // bytes per point
   int max_tiles_pp = 0, tile_cap_pp = 0;
@@ -952,6 +1004,8 @@ build_grid(y3b_engine* e, int gi)
   f += (size_t)g.nJ * g.n_z;
   g.f_CG = f;
   f += (size_t)g.nJ * g.n_z;
+  g.f_win = f;
+  f += 2 * (size_t)(g.n_m_pad / kGemmRows);
   g.s32_stride = (f + 3) & ~size_t(3);
   e->grids[gi] = g;
   return Y3B_OK;
@@ -1170,7 +1224,7 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
   size_t bytes = N * sizeof(PointDev) + N * L.stride * 8 + N * e->s64_stride * 8 +
                  N * e->s32_stride * 4 + 2 * N * e->nB_max * (size_t)e->w_stride * 8 +
                  N * e->nB_max * 8 + (2 * N + 1) * sizeof(int) +
-                 N * (size_t)e->tile_cap_pp * sizeof(int);
+                 N * (size_t)e->tile_cap_pp * sizeof(int2);
   for (const auto& g : e->grids)
     e->f_stride = std::max(e->f_stride, (size_t)(g.n_m_pad / kGemmRows) * (g.n_t_pad / 16) *
                                           kFStageBytes);
@@ -1189,6 +1243,7 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
       (rc = e->W.alloc(N * e->nB_max * (size_t)e->w_stride)) ||
       (rc = e->Wg.alloc(N * e->nB_max * (size_t)e->w_stride)) ||
       (rc = e->counts.alloc(N * e->nB_max)) || (rc = e->status.alloc(1)) ||
+      (rc = e->stage_ct.alloc(2)) ||
       (rc = e->order.alloc(N)) || (rc = e->tile_start.alloc(N + 1)) ||
       (rc = e->tile_list.alloc(N * (size_t)e->tile_cap_pp)) ||
       (rc = e->fbuf.alloc(N * e->f_stride)))
@@ -1301,7 +1356,7 @@ enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_t
                      e->order.get(), e->tile_start.get(), e->tile_list.get(),
                      (long long)n * e->max_tiles_pp, e->cshape, e->cstages, e->n_ctas,
                      e->fbuf.get(), e->f_stride,
-                     e->s32.get(), W, Wg, e->w_stride, e->status.get(), s,
+                     e->s32.get(), W, Wg, e->w_stride, e->status.get(), e->stage_ct.get(), s,
                      e->cfg.with_shear && d_shear != nullptr};
     const int rc = launch_contract(L);
     if (rc) {
@@ -1631,6 +1686,19 @@ y3b_engine_weights(y3b_engine* e, int n, double* W)
   Y3B_CUDA(cudaStreamSynchronize(e->stream));
   Y3B_CUDA(cudaMemcpy(W, e->W.get(), (size_t)n * e->nB_max * e->w_stride * sizeof(double),
                       cudaMemcpyDeviceToHost));
+  return Y3B_OK;
+}
+
+extern "C" int
+y3b_engine_stage_count(const y3b_engine* e, long long* executed, long long* dense)
+{
+  clear_error();
+  if (!e || !executed || !dense) return Y3B_ERR_INVALID;
+  int h[2] = {0, 0};
+  if (e->stage_ct.get())
+    Y3B_CUDA(cudaMemcpy(h, e->stage_ct.get(), sizeof(h), cudaMemcpyDeviceToHost));
+  *executed = h[0];
+  *dense = h[1];
   return Y3B_OK;
 }
 

@@ -54,6 +54,7 @@ struct GridDev {
   size_t o_cz, o_czs, o_alpha, o_beta, o_P0, o_V;
   size_t s32_stride;  // floats per point in the FP32 scratch
   size_t f_a, f_b, f_delta, f_scal, f_Yt, f_CN, f_CG;
+  size_t f_win;       // per lnM tile: first and end lam_t stage of the contraction (ints)
 };
 
 struct PointDev {  // mirrors y3b_point
@@ -92,7 +93,8 @@ struct ContractLaunch {
   int n_points;
   int* order;               // [n_points] device scratch: points by grid cost
   int* tile_start;          // [n_points + 1] device scratch: tile offsets
-  int* tile_list;           // [max_tiles] device scratch: (point << 8) | local tile
+  int2* tile_list;          // [max_tiles] device scratch: {(point << 8) | local tile,
+                            //  first stage | end stage << 16}
   long long max_tiles;      // upper bound of the launch's tiles (grid size)
   ContractShape shape;
   int stages;               // ring depth, 2..contract_stages(shape)
@@ -104,6 +106,7 @@ struct ContractLaunch {
   double* Wg;
   int w_stride;             // max n_m over grids
   int* status;
+  int* stage_count;         // [2] device: lam_t stages issued, stages of the full range
   cudaStream_t stream;
   bool shear;               // also accumulate the Sigma_crit-weighted W^g
 };

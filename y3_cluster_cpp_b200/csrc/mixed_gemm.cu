@@ -274,7 +274,8 @@ bulk_g2s(void* dst, const void* src, uint32_t bytes, uint32_t mbar)
     : "memory");
 }
 
-// Tile t of the launch: tile_list[t] = (point << 8) | local tile, local
+// Tile t of the launch: tile_list[t] = {(point << 8) | local tile, the
+// tile's lam_t stage window first | end << 16}, local
 // tiles of a point with the richness-bin groups varying fastest.
 __host__ __device__ inline int
 vec_slot_floats(int nz_max, int ntp_max, int uk_max)
@@ -284,21 +285,24 @@ vec_slot_floats(int nz_max, int ntp_max, int uk_max)
 
 struct Tile {
   int p, mtile, bg;
+  int kc_lo, kc_hi;  // lam_t stages of the tile's window (pairs)
   const GridDev* G;
 };
 
 __device__ __forceinline__ Tile
-decode_tile(int t, const int* __restrict__ tile_list, const PointDev* __restrict__ pts,
+decode_tile(int t, const int2* __restrict__ tile_list, const PointDev* __restrict__ pts,
             const GridDev* __restrict__ grids)
 {
-  const int v = __ldg(tile_list + t);
+  const int2 v = __ldg(tile_list + t);
   Tile T;
-  T.p = v >> 8;
-  const int local = v & 255;
+  T.p = v.x >> 8;
+  const int local = v.x & 255;
   T.G = grids + pts[T.p].grid;
   const int n_bg = T.G->n_bg;
   T.bg = local % n_bg;
   T.mtile = local / n_bg;
+  T.kc_lo = v.y & 0xFFFF;
+  T.kc_hi = v.y >> 16;
   return T;
 }
 
@@ -344,7 +348,8 @@ block_excl_scan(int v, int* sh, int* total)
 __global__ void __launch_bounds__(1024)
 tile_plan_kernel(const GridDev* __restrict__ grids, int n_grids, int grid_mask,
                  const PointDev* __restrict__ pts, int n, int* __restrict__ order,
-                 int* __restrict__ tile_start, int* __restrict__ tile_list)
+                 int* __restrict__ tile_start, int2* __restrict__ tile_list,
+                 const float* __restrict__ s32, int* __restrict__ stage_count)
 {
   __shared__ int sh[33];
   const int C = (n + 1023) / 1024;
@@ -374,14 +379,31 @@ tile_plan_kernel(const GridDev* __restrict__ grids, int n_grids, int grid_mask,
   }
   int tot;
   int off = block_excl_scan(c, sh, &tot);
+  int ex = 0, dn = 0;  // stages issued / of the full lam_t range, this thread's tiles
   for (int i = b; i < e; ++i) {
     tile_start[i] = off;
     const int p = order[i], g = pts[p].grid;
     const int nt = grid_in_mask(grid_mask, g) ? grids[g].tiles_pp : 0;
-    for (int l = 0; l < nt; ++l) tile_list[off + l] = (p << 8) | l;
+    if (nt) {
+      const GridDev& G = grids[g];
+      const int* win = reinterpret_cast<const int*>(s32 + (size_t)p * G.s32_stride + G.f_win);
+      for (int l = 0; l < nt; ++l) {
+        const int mt = l / G.n_bg;
+        tile_list[off + l] = make_int2((p << 8) | l, win[2 * mt] | (win[2 * mt + 1] << 16));
+        ex += win[2 * mt + 1] - win[2 * mt];
+      }
+      dn += nt * (G.n_t_pad / kStageK);
+    }
     off += nt;
   }
   if (threadIdx.x == 0) tile_start[n] = tot;
+  int ex_tot, dn_tot;
+  block_excl_scan(ex, sh, &ex_tot);
+  block_excl_scan(dn, sh, &dn_tot);
+  if (threadIdx.x == 0) {
+    stage_count[0] = ex_tot;
+    stage_count[1] = dn_tot;
+  }
 }
 
 // Persistent contraction: one CTA per SM walks the launch's tiles (point,
@@ -399,7 +421,7 @@ tile_plan_kernel(const GridDev* __restrict__ grids, int n_grids, int grid_mask,
 template <int NJ, bool SHEAR>
 __global__ void __launch_bounds__(kThreads, 1)
 contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ pts,
-                const int* __restrict__ tile_start, const int* __restrict__ tile_list,
+                const int* __restrict__ tile_start, const int2* __restrict__ tile_list,
                 int n_points, int nz_max, int ntp_max, int uk_max, int n_stages,
                 int n_fstages, const uint8_t* __restrict__ fbuf, size_t f_stride,
                 const float* __restrict__ s32, double* __restrict__ Wout,
@@ -470,7 +492,7 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
       int j = 0, last_stage = -1, last_parity = 0;
       for (int t = blockIdx.x; t < n_tiles && !*abort_s; t += gridDim.x) {
         const Tile T = decode_tile(t, tile_list, pts, grids);
-        const int ncp = T.G->ncp_c, nk = T.G->n_t_pad / kStageK;
+        const int ncp = T.G->ncp_c;
         const int buf = j & 1;
         if (j >= 2 && !mbar_poll_or_abort(smem_u32(&acc_empty[buf]), ((j >> 1) - 1) & 1, abort_s))
           break;
@@ -479,7 +501,7 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
         const uint32_t idesc = umma_idesc_bf16(kGemmRows, ncp);
         const uint32_t lboA = (uint32_t)ncp * 16u;
         bool broke = false;
-        for (int kc = 0; kc < nk; ++kc, rp.next(nst), rf.next(nfs)) {
+        for (int kc = T.kc_lo; kc < T.kc_hi; ++kc, rp.next(nst), rf.next(nfs)) {
           const int s = rp.s, f = rf.s;
           if (!mbar_poll_or_abort(smem_u32(&full[s]), rp.ph, abort_s) ||
               !mbar_poll_or_abort(smem_u32(&fbar[f]), rf.ph, abort_s)) {
@@ -491,7 +513,7 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
           const uint32_t ah = smem_u32(smem + s * kStageBytes), al = ah + kAPlane;
           const uint64_t dfh = umma_desc(fh, kLboF, 128), dfl = umma_desc(fl, kLboF, 128);
           const uint64_t dah = umma_desc(ah, lboA, 128), dal = umma_desc(al, lboA, 128);
-          umma_bf16(dacc, dfh, dah, idesc, kc != 0);
+          umma_bf16(dacc, dfh, dah, idesc, kc != T.kc_lo);
           umma_bf16(dacc, dfh, dal, idesc, 1u);
           umma_bf16(dacc, dfl, dah, idesc, 1u);
           umma_commit(smem_u32(&empty[s]));
@@ -522,7 +544,7 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
     for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++jt) {
       const Tile T = decode_tile(t, tile_list, pts, grids);
       const GridDev* G = T.G;
-      const int nk = G->n_t_pad / kStageK, n_z = G->n_z, ntp = G->n_t_pad;
+      const int n_z = G->n_z, ntp = G->n_t_pad;
       const int i0 = T.bg * G->nIc, nIh = min(G->nIc, G->nI - i0);
       const int slot = jt & 1;
       const float* vs = vec_s + slot * vec_floats;
@@ -542,7 +564,7 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
       const float* __restrict__ ukg = G->UK + ((size_t)((i0 + il) * n_z + q)) * ntp;
       const uint32_t lboA = (uint32_t)G->ncp_c * 16u;
       const uint32_t row_off = (uint32_t)g * lboA + (uint32_t)(il * n_z + q) * 16u;
-      for (int kc = 0; kc < nk; kc += 2, chunk += 2) {
+      for (int kc = T.kc_lo; kc < T.kc_hi; kc += 2, chunk += 2) {
         int sp2[2];
         uint32_t ph2[2];
 #pragma unroll
@@ -651,14 +673,14 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
           const int nkn = Tn.G->n_t_pad / kStageK;
           const uint8_t* nsrc =
             fbuf + (size_t)Tn.p * f_stride + (size_t)Tn.mtile * nkn * kFStageBytes;
-          for (int kc = 0; kc < nkn; ++kc)
+          for (int kc = Tn.kc_lo; kc < Tn.kc_hi; ++kc)
             asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(
                            nsrc + (size_t)kc * kFStageBytes),
                          "r"((uint32_t)kFStageBytes)
                          : "memory");
         }
         bool broke = false;
-        for (int kc = 0; kc < nk; ++kc, ++chunk, rp.next(nfs)) {
+        for (int kc = T.kc_lo; kc < T.kc_hi; ++kc, ++chunk, rp.next(nfs)) {
           const int s = rp.s;
           if (chunk >= nfs && !mbar_poll_or_abort(smem_u32(&fempty[s]), rp.ph ^ 1u, abort_s)) {
             broke = true;
@@ -914,7 +936,8 @@ launch_contract(const ContractLaunch& L)
     return Y3B_ERR_INVALID;
   }
   tile_plan_kernel<<<1, 1024, 0, L.stream>>>(L.grids, L.n_grids, L.grid_mask, L.pts, L.n_points,
-                                             L.order, L.tile_start, L.tile_list);
+                                             L.order, L.tile_start, L.tile_list, L.s32,
+                                             L.stage_count);
   count_launch();
   Y3B_CUDA(cudaGetLastError());
   const size_t smem = contract_smem_at(L.stages, L.shape);

@@ -287,6 +287,13 @@ class Engine:
         check(lib().y3b_engine_tuning(self._h, C.byref(st), nic, len(self.grids)))
         return {"stages": st.value, "bins_per_tile": list(nic)}
 
+    def stage_count(self):
+        """(issued, dense) lam_t stages of the last mixed-form contraction;
+        call after that evaluation completed."""
+        ex, dn = C.c_longlong(), C.c_longlong()
+        check(lib().y3b_engine_stage_count(self._h, C.byref(ex), C.byref(dn)))
+        return ex.value, dn.value
+
     def set_graphs(self, on=True):
         """CUDA-graph replay of repeated evaluations (on by default)."""
         check(lib().y3b_engine_set_graphs(self._h, 1 if on else 0))
