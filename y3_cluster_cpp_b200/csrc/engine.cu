@@ -184,6 +184,7 @@ prep_kernel(PrepArgs a)
   __shared__ __align__(8) uint64_t bar;
   __shared__ int timed_out;
   __shared__ double red[6];
+  __shared__ int swin[16];  // lam_t stage window per lnM tile (n_m <= 1024)
 
   const double* src = a.tables + (size_t)(a.slot ? a.slot[p] : p) * L.stride;
   const uint32_t bytes = (uint32_t)((head + tail) * sizeof(double));
@@ -500,17 +501,20 @@ prep_kernel(PrepArgs a)
             hi = lo + 2;
           }
         }
-        win[2 * mt] = lo;
-        win[2 * mt + 1] = hi;
+        win[2 * mt] = swin[2 * mt] = lo;
+        win[2 * mt + 1] = swin[2 * mt + 1] = hi;
       }
     }
   }
+  __syncthreads();
   const float sc1 = sqrtf((float)(1.4426950408889634 * 0.5 / (sig * sig)));
   const float2 sc2 = make_float2(sc1, sc1);
   uint8_t* fb = a.fbuf + (size_t)p * a.f_stride;
   const int nk = n_t_pad / 16, n_g8 = n_t_pad / 8;
   for (int it = tid; it < n_m_pad * n_g8; it += blockDim.x) {
     const int m = it % n_m_pad, t8 = it / n_m_pad;
+    // Only the stages inside each tile's window are ever read (warp-uniform).
+    if ((t8 >> 1) < swin[2 * (m >> 7)] || (t8 >> 1) >= swin[2 * (m >> 7) + 1]) continue;
     const float am = m < n_m ? ka_f[m] * sc1 : 1e18f;
     const float2 nam2 = make_float2(-am, -am);
     const float4 d0 = *reinterpret_cast<const float4*>(dt_f + t8 * 8);
