@@ -405,7 +405,20 @@ prep_kernel(PrepArgs a)
   const double mu0 = red[2];
   const double hmu = red[3] > red[2] ? (red[3] - red[2]) / (kDTab - 1) : 1.0;
   const double inv_hmu = 1.0 / hmu;
-  for (int j = tid; j < kDTab; j += blockDim.x) {
+  // Only nodes next to a mu that fails the FP32 saturation test are read (the
+  // test's margin is 1e-3 plus FP32 rounding, and the nodes used lie within
+  // hmu of mu): the interior nodes hold D = 1, dD = 0 without an erfc.
+  const int j_sat0 =
+    (int)fmin(fmax(ceil((ll_lo + 5.6 * sig + 0.01 - mu0) * inv_hmu) + 2.0, 0.0), (double)kDTab);
+  const int j_sat1 =
+    (int)fmin(fmax(floor((ll_hi - 5.6 * sig - 0.01 - mu0) * inv_hmu) - 2.0, 0.0), (double)kDTab);
+  const int n_lo = min(j_sat0 + 1, kDTab), n_hi = kDTab - max(j_sat1, n_lo);
+  for (int j = n_lo + tid; j < kDTab - n_hi; j += blockDim.x) {
+    dtab[j] = 1.0;
+    dtab[kDTab + j] = 0.0;
+  }
+  for (int r = tid; r < n_lo + n_hi; r += blockDim.x) {
+    const int j = r < n_lo ? r : kDTab - n_hi + (r - n_lo);
     const double mu = mu0 + j * hmu;
     const double aa = (ll_lo - mu) * inv_s, bb = (ll_hi - mu) * inv_s;
     dtab[j] = mor_norm(aa, bb);
