@@ -96,6 +96,8 @@ struct PrepArgs {
   int grid_mask;
   uint8_t* fbuf;    // mixed form: F(t, k) blocks, f_stride bytes per point
   size_t f_stride;
+  int* win_tile;    // mixed form: [n][win_stride] lam_t stage window per local tile
+  int win_stride;
 };
 
 // MOR normalisation D = Phi(b) - Phi(a) in FP64, a = (l_lo - mu)/s,
@@ -478,7 +480,6 @@ prep_kernel(PrepArgs a)
   {
     constexpr double kWin = 6.5;
     const int n_mt = n_m_pad / kGemmRows, nk = n_t_pad / 16;
-    int* win = reinterpret_cast<int*>(s32 + Gp->f_win);
     for (int mt = warp; mt < n_mt; mt += nw) {
       double amn = 1e300, amx = -1e300;
       for (int k = mt * kGemmRows + lane; k < min(n_m, (mt + 1) * kGemmRows); k += 32) {
@@ -514,12 +515,17 @@ prep_kernel(PrepArgs a)
             hi = lo + 2;
           }
         }
-        win[2 * mt] = swin[2 * mt] = lo;
-        win[2 * mt + 1] = swin[2 * mt + 1] = hi;
+        swin[2 * mt] = lo;
+        swin[2 * mt + 1] = hi;
       }
     }
   }
   __syncthreads();
+  // The window of each contraction tile (lnM tile, richness-bin group).
+  for (int l = tid; l < Gp->tiles_pp; l += blockDim.x) {
+    const int mt = l / Gp->n_bg;
+    a.win_tile[(size_t)p * a.win_stride + l] = swin[2 * mt] | (swin[2 * mt + 1] << 16);
+  }
   const float sc1 = sqrtf((float)(1.4426950408889634 * 0.5 / (sig * sig)));
   const float2 sc2 = make_float2(sc1, sc1);
   uint8_t* fb = a.fbuf + (size_t)p * a.f_stride;
@@ -782,7 +788,8 @@ struct y3b_engine {
   y3b::DevBuf<float> s32;
   y3b::DevBuf<int> status, order, tile_start;
   y3b::DevBuf<int> stage_ct;  // [2] lam_t stages issued / dense, last contraction
-  y3b::DevBuf<int2> tile_list;
+  y3b::DevBuf<int> tile_list;
+  y3b::DevBuf<int> win_tile;  // [max_points][tile_cap_pp] stage windows (prep -> contraction)
   y3b::DevBuf<uint8_t> fbuf;  // F(t, k) stage blocks of the mixed form
   size_t f_stride = 0;        // bytes per point
   int max_tiles_pp = 0, tile_cap_pp = 0;
@@ -791,6 +798,10 @@ struct y3b_engine {
   // Chunked host-buffer evaluation: copy stream, one event and one pinned
   // status word per chunk.
   cudaStream_t xstream = nullptr;
+  // The tile planner's stream and the events that fork it from, and join it
+  // back to, an evaluation's stream.
+  cudaStream_t pstream = nullptr;
+  cudaEvent_t plan_fork = nullptr, plan_join = nullptr;
   cudaEvent_t chunk_ev[y3b::kEvalChunks] = {};
   int* chunk_status = nullptr;
   // CUDA graphs of whole evaluations, keyed by their arguments: an
@@ -843,6 +854,9 @@ struct y3b_engine {
       if (ev) cudaEventDestroy(ev);
     if (chunk_status) cudaFreeHost(chunk_status);
     if (xstream) cudaStreamDestroy(xstream);
+    if (pstream) cudaStreamDestroy(pstream);
+    if (plan_fork) cudaEventDestroy(plan_fork);
+    if (plan_join) cudaEventDestroy(plan_join);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -1021,8 +1035,6 @@ build_grid(y3b_engine* e, int gi)
   f += (size_t)g.nJ * g.n_z;
   g.f_CG = f;
   f += (size_t)g.nJ * g.n_z;
-  g.f_win = f;
-  f += 2 * (size_t)(g.n_m_pad / kGemmRows);
   g.s32_stride = (f + 3) & ~size_t(3);
   e->grids[gi] = g;
   return Y3B_OK;
@@ -1183,6 +1195,15 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
   }
   if ((rc = contract_prepare(e->cshape))) return fail(rc);
   rc = cuda_status(cudaStreamCreateWithFlags(&e->xstream, cudaStreamNonBlocking), "cudaStreamCreate");
+  if (!rc)
+    rc = cuda_status(cudaStreamCreateWithFlags(&e->pstream, cudaStreamNonBlocking),
+                     "cudaStreamCreate");
+  if (!rc)
+    rc = cuda_status(cudaEventCreateWithFlags(&e->plan_fork, cudaEventDisableTiming),
+                     "cudaEventCreate");
+  if (!rc)
+    rc = cuda_status(cudaEventCreateWithFlags(&e->plan_join, cudaEventDisableTiming),
+                     "cudaEventCreate");
   for (int c = 0; c < kEvalChunks && !rc; ++c)
     rc = cuda_status(cudaEventCreateWithFlags(&e->chunk_ev[c], cudaEventDisableTiming),
                      "cudaEventCreate");
@@ -1241,7 +1262,7 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
   size_t bytes = N * sizeof(PointDev) + N * L.stride * 8 + N * e->s64_stride * 8 +
                  N * e->s32_stride * 4 + 2 * N * e->nB_max * (size_t)e->w_stride * 8 +
                  N * e->nB_max * 8 + (2 * N + 1) * sizeof(int) +
-                 N * (size_t)e->tile_cap_pp * sizeof(int2);
+                 2 * N * (size_t)e->tile_cap_pp * sizeof(int);
   for (const auto& g : e->grids)
     e->f_stride = std::max(e->f_stride, (size_t)(g.n_m_pad / kGemmRows) * (g.n_t_pad / 16) *
                                           kFStageBytes);
@@ -1263,6 +1284,7 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
       (rc = e->stage_ct.alloc(2)) ||
       (rc = e->order.alloc(N)) || (rc = e->tile_start.alloc(N + 1)) ||
       (rc = e->tile_list.alloc(N * (size_t)e->tile_cap_pp)) ||
+      (rc = e->win_tile.alloc(N * (size_t)e->tile_cap_pp)) ||
       (rc = e->fbuf.alloc(N * e->f_stride)))
     return fail(rc);
   if (cfg->with_shear) {
@@ -1350,12 +1372,37 @@ enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_t
   Y3B_CUDA(cudaMemsetAsync(e->status.get(), 0, sizeof(int), s));
   if (e->prof) ++e->prof_evals;
   PrepArgs pa{e->d_grids.get(), d_pts, d_tables, d_slot, e->lay, prec == Y3B_MIXED,
-              e->s64.get(), e->s32.get(), e->status.get(), grid_mask, e->fbuf.get(), e->f_stride};
+              e->s64.get(), e->s32.get(), e->status.get(), grid_mask, e->fbuf.get(), e->f_stride,
+              e->win_tile.get(), e->tile_cap_pp};
+  ContractLaunch L{e->d_grids.get(), (int)e->grids.size(), grid_mask, d_pts, n,
+                   e->order.get(), e->tile_start.get(), e->tile_list.get(), e->win_tile.get(),
+                   e->tile_cap_pp, (long long)n * e->max_tiles_pp, e->cshape, e->cstages,
+                   e->n_ctas, e->fbuf.get(), e->f_stride, e->s32.get(), W, Wg, e->w_stride,
+                   e->status.get(), e->stage_ct.get(), e->pstream, s,
+                   e->cfg.with_shear && d_shear != nullptr};
+  // Mixed form: the tile planner runs on its own stream beside the prep
+  // kernel (it reads only the points and grids) and joins before the
+  // contraction.  The fork comes after everything already on `s`, so a
+  // previous evaluation's contraction has finished with the tile list.
+  const bool mixed = prec == Y3B_MIXED;
+  if (mixed) {
+    Y3B_TRY(contract_check(L));
+    Y3B_CUDA(cudaEventRecord(e->plan_fork, s));
+    Y3B_CUDA(cudaStreamWaitEvent(e->pstream, e->plan_fork, 0));
+    const int prc = launch_plan(L);
+    Y3B_CUDA(cudaEventRecord(e->plan_join, e->pstream));
+    if (prc) {  // join before returning, so that a capture in progress stays whole
+      cudaStreamWaitEvent(s, e->plan_join, 0);
+      return prc;
+    }
+  }
   {
     StageTimer t(e, s, 0);
     prep_kernel<<<n, 256, e->prep_smem, s>>>(pa);
     count_launch();
-    Y3B_CUDA(cudaGetLastError());
+    const cudaError_t perr = cudaGetLastError();
+    if (mixed) Y3B_CUDA(cudaStreamWaitEvent(s, e->plan_join, 0));
+    Y3B_CUDA(perr);
   }
   StageTimer* tc = new StageTimer(e, s, 1);
   if (prec == Y3B_FP64) {
@@ -1369,12 +1416,6 @@ enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_t
     count_launch();
     Y3B_CUDA(cudaGetLastError());
   } else {
-    ContractLaunch L{e->d_grids.get(), (int)e->grids.size(), grid_mask, d_pts, n,
-                     e->order.get(), e->tile_start.get(), e->tile_list.get(),
-                     (long long)n * e->max_tiles_pp, e->cshape, e->cstages, e->n_ctas,
-                     e->fbuf.get(), e->f_stride,
-                     e->s32.get(), W, Wg, e->w_stride, e->status.get(), e->stage_ct.get(), s,
-                     e->cfg.with_shear && d_shear != nullptr};
     const int rc = launch_contract(L);
     if (rc) {
       delete tc;

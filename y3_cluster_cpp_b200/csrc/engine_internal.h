@@ -54,7 +54,6 @@ struct GridDev {
   size_t o_cz, o_czs, o_alpha, o_beta, o_P0, o_V;
   size_t s32_stride;  // floats per point in the FP32 scratch
   size_t f_a, f_b, f_delta, f_scal, f_Yt, f_CN, f_CG;
-  size_t f_win;       // per lnM tile: first and end lam_t stage of the contraction (ints)
 };
 
 struct PointDev {  // mirrors y3b_point
@@ -93,8 +92,9 @@ struct ContractLaunch {
   int n_points;
   int* order;               // [n_points] device scratch: points by grid cost
   int* tile_start;          // [n_points + 1] device scratch: tile offsets
-  int2* tile_list;          // [max_tiles] device scratch: {(point << 8) | local tile,
-                            //  first stage | end stage << 16}
+  int* tile_list;           // [max_tiles] device scratch: (point << 8) | local tile
+  const int* win_tile;      // [n][win_stride]: lam_t stage window of each local tile,
+  int win_stride;           //   first | end << 16 (written by the prep kernel)
   long long max_tiles;      // upper bound of the launch's tiles (grid size)
   ContractShape shape;
   int stages;               // ring depth, 2..contract_stages(shape)
@@ -107,12 +107,16 @@ struct ContractLaunch {
   int w_stride;             // max n_m over grids
   int* status;
   int* stage_count;         // [2] device: lam_t stages issued, stages of the full range
+  cudaStream_t plan_stream; // the tile planner runs here, beside the prep kernel
   cudaStream_t stream;
   bool shear;               // also accumulate the Sigma_crit-weighted W^g
 };
 
-// One launch of the tile planner and one persistent contraction launch over
-// the points of every grid.
+// The tile planner depends only on the points and their grids, so it runs on
+// L.plan_stream while the prep kernel runs; the persistent contraction over
+// the points of every grid runs on L.stream once both are done.
+int contract_check(const ContractLaunch& L);  // ring depth and CTA count
+int launch_plan(const ContractLaunch& L);
 int launch_contract(const ContractLaunch& L);
 size_t contract_smem_bytes(const ContractShape& c);  // (size_t)-1 if it does not fit
 int contract_stages(const ContractShape& c);

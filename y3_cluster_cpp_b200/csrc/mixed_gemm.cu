@@ -274,9 +274,9 @@ bulk_g2s(void* dst, const void* src, uint32_t bytes, uint32_t mbar)
     : "memory");
 }
 
-// Tile t of the launch: tile_list[t] = {(point << 8) | local tile, the
-// tile's lam_t stage window first | end << 16}, local
-// tiles of a point with the richness-bin groups varying fastest.
+// Tile t of the launch: tile_list[t] = (point << 8) | local tile, local
+// tiles of a point with the richness-bin groups varying fastest; the tile's
+// lam_t stage window (first | end << 16) is win_tile[point][local].
 __host__ __device__ inline int
 vec_slot_floats(int nz_max, int ntp_max, int uk_max)
 {
@@ -290,19 +290,20 @@ struct Tile {
 };
 
 __device__ __forceinline__ Tile
-decode_tile(int t, const int2* __restrict__ tile_list, const PointDev* __restrict__ pts,
-            const GridDev* __restrict__ grids)
+decode_tile(int t, const int* __restrict__ tile_list, const int* __restrict__ win_tile,
+            int win_stride, const PointDev* __restrict__ pts, const GridDev* __restrict__ grids)
 {
-  const int2 v = __ldg(tile_list + t);
+  const int v = __ldg(tile_list + t);
   Tile T;
-  T.p = v.x >> 8;
-  const int local = v.x & 255;
+  T.p = v >> 8;
+  const int local = v & 255;
+  const int w = __ldg(win_tile + (size_t)T.p * win_stride + local);
   T.G = grids + pts[T.p].grid;
   const int n_bg = T.G->n_bg;
   T.bg = local % n_bg;
   T.mtile = local / n_bg;
-  T.kc_lo = v.y & 0xFFFF;
-  T.kc_hi = v.y >> 16;
+  T.kc_lo = w & 0xFFFF;
+  T.kc_hi = w >> 16;
   return T;
 }
 
@@ -342,14 +343,16 @@ block_excl_scan(int v, int* sh, int* total)
 // Orders the points by the cost of their grid's tiles (most expensive grid
 // first, stable inside a grid) and writes the tiles of the launch in that
 // order: tile_start[i] = tiles of order[0..i), tile_start[n] = all tiles,
-// tile_list[t] = (point << 8) | tile inside the point.  One
-// block of 1024 threads, each owning a contiguous chunk of points.  Points
-// whose grid is not in the mask are put last with no tiles.
+// tile_list[t] = (point << 8) | tile inside the point, and the stage count
+// of the full lam_t range (stage_count[1]; stage_count[0], the stages
+// issued, is reset for the contraction to add to).  One block of 1024
+// threads, each owning a contiguous chunk of points.  Points whose grid is
+// not in the mask are put last with no tiles.
 __global__ void __launch_bounds__(1024)
 tile_plan_kernel(const GridDev* __restrict__ grids, int n_grids, int grid_mask,
                  const PointDev* __restrict__ pts, int n, int* __restrict__ order,
-                 int* __restrict__ tile_start, int2* __restrict__ tile_list,
-                 const float* __restrict__ s32, int* __restrict__ stage_count)
+                 int* __restrict__ tile_start, int* __restrict__ tile_list,
+                 int* __restrict__ stage_count)
 {
   __shared__ int sh[33];
   const int C = (n + 1023) / 1024;
@@ -379,29 +382,20 @@ tile_plan_kernel(const GridDev* __restrict__ grids, int n_grids, int grid_mask,
   }
   int tot;
   int off = block_excl_scan(c, sh, &tot);
-  int ex = 0, dn = 0;  // stages issued / of the full lam_t range, this thread's tiles
+  int dn = 0;  // stages of the full lam_t range, this thread's tiles
   for (int i = b; i < e; ++i) {
     tile_start[i] = off;
     const int p = order[i], g = pts[p].grid;
     const int nt = grid_in_mask(grid_mask, g) ? grids[g].tiles_pp : 0;
-    if (nt) {
-      const GridDev& G = grids[g];
-      const int* win = reinterpret_cast<const int*>(s32 + (size_t)p * G.s32_stride + G.f_win);
-      for (int l = 0; l < nt; ++l) {
-        const int mt = l / G.n_bg;
-        tile_list[off + l] = make_int2((p << 8) | l, win[2 * mt] | (win[2 * mt + 1] << 16));
-        ex += win[2 * mt + 1] - win[2 * mt];
-      }
-      dn += nt * (G.n_t_pad / kStageK);
-    }
+    for (int l = 0; l < nt; ++l) tile_list[off + l] = (p << 8) | l;
+    if (nt) dn += nt * (grids[g].n_t_pad / kStageK);
     off += nt;
   }
   if (threadIdx.x == 0) tile_start[n] = tot;
-  int ex_tot, dn_tot;
-  block_excl_scan(ex, sh, &ex_tot);
+  int dn_tot;
   block_excl_scan(dn, sh, &dn_tot);
   if (threadIdx.x == 0) {
-    stage_count[0] = ex_tot;
+    stage_count[0] = 0;
     stage_count[1] = dn_tot;
   }
 }
@@ -421,7 +415,8 @@ tile_plan_kernel(const GridDev* __restrict__ grids, int n_grids, int grid_mask,
 template <int NJ, bool SHEAR>
 __global__ void __launch_bounds__(kThreads, 1)
 contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ pts,
-                const int* __restrict__ tile_start, const int2* __restrict__ tile_list,
+                const int* __restrict__ tile_start, const int* __restrict__ tile_list,
+                const int* __restrict__ win_tile, int win_stride, int* __restrict__ stage_count,
                 int n_points, int nz_max, int ntp_max, int uk_max, int n_stages,
                 int n_fstages, const uint8_t* __restrict__ fbuf, size_t f_stride,
                 const float* __restrict__ s32, double* __restrict__ Wout,
@@ -489,9 +484,9 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
     // ---------------- MMA issuer ----------------
     if (lane == 0) {
       RingPos rp, rf;
-      int j = 0, last_stage = -1, last_parity = 0;
+      int j = 0, last_stage = -1, last_parity = 0, issued_stages = 0;
       for (int t = blockIdx.x; t < n_tiles && !*abort_s; t += gridDim.x) {
-        const Tile T = decode_tile(t, tile_list, pts, grids);
+        const Tile T = decode_tile(t, tile_list, win_tile, win_stride, pts, grids);
         const int ncp = T.G->ncp_c;
         const int buf = j & 1;
         if (j >= 2 && !mbar_poll_or_abort(smem_u32(&acc_empty[buf]), ((j >> 1) - 1) & 1, abort_s))
@@ -523,8 +518,10 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
         }
         if (broke) break;
         umma_commit(smem_u32(&acc_full[buf]));  // tile j's accumulator is complete
+        issued_stages += T.kc_hi - T.kc_lo;
         ++j;
       }
+      atomicAdd(stage_count, issued_stages);
       // Leave only when every issued MMA has completed (bounded).
       if (last_stage >= 0) {
         long long t0 = clock64();
@@ -542,7 +539,7 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
     int chunk = 0, jt = 0;
     RingPos rp;
     for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++jt) {
-      const Tile T = decode_tile(t, tile_list, pts, grids);
+      const Tile T = decode_tile(t, tile_list, win_tile, win_stride, pts, grids);
       const GridDev* G = T.G;
       const int n_z = G->n_z, ntp = G->n_t_pad;
       const int i0 = T.bg * G->nIc, nIh = min(G->nIc, G->nI - i0);
@@ -624,7 +621,7 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
         const int slot = j & 1;
         if (j >= 2 && !mbar_wait_or_abort(smem_u32(&vec_empty[slot]), ((j >> 1) - 1) & 1, abort_s))
           break;
-        const Tile T = decode_tile(t, tile_list, pts, grids);
+        const Tile T = decode_tile(t, tile_list, win_tile, win_stride, pts, grids);
         const GridDev* G = T.G;
         const int n_z = G->n_z, ntp = G->n_t_pad;
         const int i0 = T.bg * G->nIc, nIh = min(G->nIc, G->nI - i0);
@@ -663,13 +660,13 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
       int chunk = 0;
       uint32_t issued = 0, last_ph = 0;  // per stage: copy issued, parity of its last use
       for (int t = blockIdx.x; t < n_tiles && !*abort_s; t += gridDim.x) {
-        const Tile T = decode_tile(t, tile_list, pts, grids);
+        const Tile T = decode_tile(t, tile_list, win_tile, win_stride, pts, grids);
         const int nk = T.G->n_t_pad / kStageK;
         const uint8_t* src =
           fbuf + (size_t)T.p * f_stride + (size_t)T.mtile * nk * kFStageBytes;
         // Warm L2 with the next tile's F blocks while this tile streams.
         if (t + (int)gridDim.x < n_tiles) {
-          const Tile Tn = decode_tile(t + gridDim.x, tile_list, pts, grids);
+          const Tile Tn = decode_tile(t + gridDim.x, tile_list, win_tile, win_stride, pts, grids);
           const int nkn = Tn.G->n_t_pad / kStageK;
           const uint8_t* nsrc =
             fbuf + (size_t)Tn.p * f_stride + (size_t)Tn.mtile * nkn * kFStageBytes;
@@ -717,7 +714,7 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
     const uint32_t lane_base = (uint32_t)(lq * 32) << 16;
     int j = 0, y_pending = 0;
     for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
-      const Tile T = decode_tile(t, tile_list, pts, grids);
+      const Tile T = decode_tile(t, tile_list, win_tile, win_stride, pts, grids);
       const GridDev* G = T.G;
       const int n_z = G->n_z, n_m = G->n_m, nI = G->nI, nB = G->nB;
       const int i0 = T.bg * G->nIc, nIh = min(G->nIc, nI - i0);
@@ -878,7 +875,8 @@ launch_nj(const ContractLaunch& L, size_t smem)
 {
   auto k = contract_kernel<NJ, SHEAR>;
   const int blocks = (int)std::min<long long>(std::max<long long>(L.max_tiles, 1), L.n_ctas);
-  k<<<blocks, kThreads, smem, L.stream>>>(L.grids, L.pts, L.tile_start, L.tile_list, L.n_points,
+  k<<<blocks, kThreads, smem, L.stream>>>(L.grids, L.pts, L.tile_start, L.tile_list, L.win_tile,
+                                          L.win_stride, L.stage_count, L.n_points,
                                           L.shape.nz_max, L.shape.ntp_max, L.shape.uk_max,
                                           L.stages, contract_fstages(L.stages, L.shape), L.fbuf,
                                           L.f_stride, L.s32, L.W, L.Wg,
@@ -927,7 +925,7 @@ contract_prepare(const ContractShape& c)
 }
 
 int
-launch_contract(const ContractLaunch& L)
+contract_check(const ContractLaunch& L)
 {
   if (L.stages < 2 || L.stages > kMaxStages || contract_fstages(L.stages, L.shape) < 4 ||
       L.n_ctas < 1) {
@@ -935,11 +933,23 @@ launch_contract(const ContractLaunch& L)
               contract_stages(L.shape));
     return Y3B_ERR_INVALID;
   }
-  tile_plan_kernel<<<1, 1024, 0, L.stream>>>(L.grids, L.n_grids, L.grid_mask, L.pts, L.n_points,
-                                             L.order, L.tile_start, L.tile_list, L.s32,
-                                             L.stage_count);
+  return Y3B_OK;
+}
+
+int
+launch_plan(const ContractLaunch& L)
+{
+  tile_plan_kernel<<<1, 1024, 0, L.plan_stream>>>(L.grids, L.n_grids, L.grid_mask, L.pts,
+                                                  L.n_points, L.order, L.tile_start, L.tile_list,
+                                                  L.stage_count);
   count_launch();
-  Y3B_CUDA(cudaGetLastError());
+  return cuda_status(cudaGetLastError(), "tile_plan_kernel");
+}
+
+int
+launch_contract(const ContractLaunch& L)
+{
+  Y3B_TRY(contract_check(L));
   const size_t smem = contract_smem_at(L.stages, L.shape);
   return L.shear ? launch_shear<true>(L, smem) : launch_shear<false>(L, smem);
 }
