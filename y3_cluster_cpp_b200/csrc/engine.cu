@@ -146,8 +146,8 @@ prep_smem_bytes(const TableLayout& L, int n_hz, int n_hm, int n_m, int n_z, int 
 {
   size_t b = (L.off[2] + L.stride - L.off[3]) * 8;         // table block without dn/dlnM
   b += (((size_t)n_hz * n_hm * 4) + 15) & ~size_t(15);     // FP32 dn/dlnM
-  b += (size_t)n_m * (8 + 8 + 8 + 4 + 4);                  // alpha, t, kf, xi, pad
-  b += (size_t)n_z * (8 + 8 + 4 + 4);                      // beta, u, yi, pad
+  b += (size_t)n_m * (8 + 8 + 8 + 4);                      // alpha, t, kf, xi
+  b += (size_t)n_z * (8 + 8 + 4);                          // beta, u, yi
   b += (size_t)n_m * 12;                                   // FP32 t, kf, alpha - A0
   b += 8 + 2 * (size_t)kDTab * 8;                          // D(mu) table (mixed form)
   b += 16 + (size_t)n_t_pad * 4;                           // FP32 delta_t (mixed form)
@@ -1300,6 +1300,10 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
   if (rc) return fail(rc);
   Y3B_CUDA(cudaFuncSetAttribute(prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)e->prep_smem));
+  // Four 256-thread CTAs per SM (the register limit) need ~57 KB of shared
+  // memory each at 256 lnM x 128 z nodes: ask for the largest carveout.
+  Y3B_CUDA(cudaFuncSetAttribute(prep_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                (int)cudaSharedmemCarveoutMaxShared));
   Y3B_CUDA(cudaFuncSetAttribute(direct_main_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)e->direct_smem));
   *out = e;
