@@ -477,7 +477,7 @@ prep_kernel(PrepArgs a)
   // tile the MOR density exp(-(l_t - mu_kq)^2 / 2 s^2) is below 3e-7 of its
   // peak outside [min mu - 5.5 s, max mu + 5.5 s] (the Gaussian mass beyond
   // is 2e-8 on each side), so those stages add less than the rounding of the
-  // split-BF16 products; the stage range is rounded to pairs.
+  // split-BF16 products; the stage count is rounded up to pairs.
   {
     constexpr double kWin = 5.5;
     const int n_mt = n_m_pad / kGemmRows, nk = n_t_pad / 16;
@@ -509,12 +509,12 @@ prep_kernel(PrepArgs a)
             if (dt_f[m] <= dhi) a = m + 1; else b = m;
           }
           const int t_hi = a;
-          lo = (t_lo / 16) & ~1;
-          hi = min(nk, (((t_hi + 15) / 16) + 1) & ~1);
-          if (hi <= lo) {  // no node inside: keep one stage pair, all zero anyway
-            lo = min(lo, nk - 2);
-            hi = lo + 2;
-          }
+          // Stages [t_lo / 16, ceil(t_hi / 16)), the count rounded up to
+          // pairs (at least one pair; nk is even) and kept inside [0, nk).
+          const int s_lo = t_lo / 16, s_hi = (t_hi + 15) / 16;
+          const int cnt = max(2, (s_hi - s_lo + 1) & ~1);
+          lo = min(s_lo, nk - cnt);
+          hi = lo + cnt;
         }
         swin[2 * mt] = lo;
         swin[2 * mt + 1] = hi;
