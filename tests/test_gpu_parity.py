@@ -356,14 +356,14 @@ def test_engine_autotune_keeps_results_within_tolerance(gpu):
     eng.close()
 
 
-def test_engine_chunked_host_eval_matches_one_launch(gpu):
+@pytest.mark.parametrize("n", [1100, 2100])  # four and eight chunks
+def test_engine_chunked_host_eval_matches_one_launch(gpu, n):
     """A large host-buffer evaluation is split into chunks whose copies
     overlap the previous chunk's kernels; counts and the mass weights equal
     those of a single device launch over the same batch."""
     import ctypes as C
     import torch
     g = synthetic.grid(1)
-    n = 1100                                  # four chunks
     eng = _engine([g], n_max=n)
     uniq = synthetic.walkers(20, seed=51, densities=(1,))
     pts = [uniq[i % 20] for i in range(n)]

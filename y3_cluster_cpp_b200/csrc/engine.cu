@@ -130,7 +130,7 @@ mor_norm(double a, double b)
 // small in deep tails).
 constexpr int kDTab = 1024;
 
-constexpr int kEvalChunks = 4;  // chunks of a large host-buffer evaluation
+constexpr int kEvalChunks = 8;  // chunks of a large host-buffer evaluation
 
 // Per-point prep, one CTA per point.  The point's packed tables are staged
 // into shared memory with one bulk (TMA) copy completing on an mbarrier;
@@ -1671,7 +1671,9 @@ y3b_engine_eval(y3b_engine* e, int precision, int n, const y3b_point* pts,
   // compute stream, so they share the per-point scratch; their weights and
   // outputs land at their own offsets.
   cudaStream_t s = e->stream, xs = e->xstream;
-  const int chunks = n >= 1024 ? y3b::kEvalChunks : (n >= 256 ? 2 : 1);
+  // About 256 points a chunk: the copies are the long pole, and only the
+  // last chunk's kernels run after them.
+  const int chunks = n >= 2048 ? y3b::kEvalChunks : (n >= 1024 ? 4 : (n >= 256 ? 2 : 1));
   const int csz = (n + chunks - 1) / chunks;
   const size_t st = e->lay.stride;
   const int nB = e->nB_max, nR = e->shear.n_R;
