@@ -484,7 +484,7 @@ def run_ours(a):
     peak_tf, peak_gbs, peak_kind = measured_peaks()
     achieved_tf = flops_alg / (gemm_ms / 1e3) / 1e12
     # The contraction skips lam_t stages where the MOR density of every
-    # (lnM, z) pair of a tile is below 3e-7 of its peak; the tensor pipe
+    # (lnM, z) pair of a tile is below 4e-6 of its peak; the tensor pipe
     # issues this fraction of the dense stages.
     torch.cuda.synchronize(dev)
     st_ex, st_dn = eng.stage_count()

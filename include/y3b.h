@@ -302,7 +302,7 @@ int y3b_engine_autotune(y3b_engine* e, int n, const y3b_point* pts_dev,
 int y3b_engine_tuning(const y3b_engine* e, int* stages, int* bins_per_tile, int cap);
 /* lam_t stages of the last mixed-form contraction: the stages its tiles
  * issued (each tile skips the stages where the MOR density of all its
- * (lnM, z) pairs is below 3e-7 of its peak) and the stages of the full
+ * (lnM, z) pairs is below 4e-6 of its peak) and the stages of the full
  * lam_t range.  Reads device memory: call after that evaluation completed. */
 int y3b_engine_stage_count(const y3b_engine* e, long long* executed, long long* dense);
 /* Wait for the engine's work on `stream` and report device-side errors. */

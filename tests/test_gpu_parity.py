@@ -198,7 +198,7 @@ def test_engine_counts_match_oracle(gpu, density):
 
 
 def test_engine_stage_window_skips_only_negligible_stages(gpu):
-    """The contraction issues only the lam_t stages inside mu +- 5.5 sigma of
+    """The contraction issues only the lam_t stages inside mu +- 5 sigma of
     each lnM tile: a narrow MOR scatter issues fewer stages, and both stay
     within tolerance of the oracle's full-range quadrature."""
     g = synthetic.grid(4)  # two 128-row lnM tiles, each spanning part of the lam_t range

@@ -474,12 +474,12 @@ prep_kernel(PrepArgs a)
   for (int t = tid; t < n_t_pad; t += blockDim.x) dt_f[t] = t < n_t ? (float)(Gp->xl[t] - L0) : 0.f;
   __syncthreads();
   // lam_t window of the contraction per lnM tile: for every (k, q) of the
-  // tile the MOR density exp(-(l_t - mu_kq)^2 / 2 s^2) is below 3e-7 of its
-  // peak outside [min mu - 5.5 s, max mu + 5.5 s] (the Gaussian mass beyond
-  // is 2e-8 on each side), so those stages add less than the rounding of the
+  // tile the MOR density exp(-(l_t - mu_kq)^2 / 2 s^2) is below 4e-6 of its
+  // peak outside [min mu - 5 s, max mu + 5 s] (the Gaussian mass beyond is
+  // 3e-7 on each side), so those stages add less than the rounding of the
   // split-BF16 products; the stage count is rounded up to pairs.
   {
-    constexpr double kWin = 5.5;
+    constexpr double kWin = 5.0;
     const int n_mt = n_m_pad / kGemmRows, nk = n_t_pad / 16;
     for (int mt = warp; mt < n_mt; mt += nw) {
       double amn = 1e300, amx = -1e300;
