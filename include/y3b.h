@@ -177,9 +177,24 @@ int y3b_selgl_build(y3b_selgl* h, const y3b_cosmo* c, const y3b_tables* t,
                     const y3b_selection* sel, int include_sci);
 /* NumCountsSelGL::evaluate over a wall of bin indices -> vals[n]. */
 int y3b_selgl_counts(y3b_selgl* h, int n, const int* bin_index, double* vals);
-/* Shear1hMisSelGL::evaluate over (bin_index[i], r[i]) pairs -> vals[n]. */
+/* Shear1hMisSelGL::evaluate over (bin_index[i], r[i]) pairs -> vals[n].
+ * NFW_DSIGMA_MIS follows the module's construction (n_operator_sel_gl_t.hh:
+ * 248,264): r_s from rho_c = 2.77533742639e11, amplitude
+ * 2 r_s delta_c rho_c Omega_M 1e-12.  Its unit profile comes from the table
+ * set with y3b_selgl_set_mis_table, else from the direct quadrature
+ * (n_theta, n_s, s_max of the y3b_shear_table). */
 int y3b_selgl_shear(y3b_selgl* h, const y3b_shear_table* st, int n,
                     const int* bin_index, const double* r, double* vals);
+/* The miscentred-profile table NFW_DSIGMA_MIS reads
+ * (src/models/nfw_dsigma_mis.hh:62-72, files nfw_off_center/
+ * table_1000_1e-03_5e+03_{gamma_logx, gamma_logxmis,
+ * log_deltasigma_gamma}.txt): axes ln x[n_lx], ln x_mis[n_lxm] (increasing)
+ * and log_tab[n_lxm][n_lx] (x fastest), read by clamped bilinear
+ * interpolation at (ln R/r_s, ln R_mis/r_s).  Host buffers, copied.
+ * n_lx = 0 returns the handle to the direct quadrature. */
+int y3b_selgl_set_mis_table(y3b_selgl* h, int n_lx, const double* logx,
+                            int n_lxm, const double* logxmis,
+                            const double* log_tab);
 /* Copy out W [n_bins][n_lnm], norm, lnm_eff, mu2 and the GL nodes/weights. */
 int y3b_selgl_weights(y3b_selgl* h, double* W, double* norm, double* lnm_eff,
                       double* mu2, double* lnm_x, double* lnm_w);

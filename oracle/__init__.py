@@ -112,6 +112,10 @@ def _declare(L):
     L.y3o_shear1h_mis.argtypes = [I, PD, PD, I, PD, I, PD, D, D, I, PD, D, D,
                                   I, PD, I, PD, PD, I, I, D, PD]
     L.y3o_sigma_crit_inv.argtypes = [I, PD, I, PD, PD, D, D, I, PD, PD, PD]
+    L.y3o_dsigma_mis_tab.argtypes = [D, D, D, D, D, D, I, PD, I, PD, PD]
+    L.y3o_dsigma_mis_tab.restype = D
+    L.y3o_shear1h_mis_tab.argtypes = [I, PD, PD, I, PD, PD, PD, PD, I, D, I, PD, D, D,
+                                      I, PD, D, D, I, PD, I, PD, PD, I, PD, I, PD, PD, PD]
     L.y3o_direct_eval.argtypes = [C.POINTER(DirectGrid), I, PD, PD,
                                   C.POINTER(Lognormal), C.POINTER(Cosmo),
                                   I, PD, I, PD, PD, I, PD, PD,
@@ -231,6 +235,26 @@ def shear1h_mis(lnm_x, lnm_w, W_gamma, R, f_mis, tau_mis, lob_centers, omega_m,
                           f_mis, tau_mis, len(lob), _p(lob), omega_m, conc,
                           len(rs), _p(rs), len(lt), _p(lt), _p(ds),
                           n_theta, n_s, s_max, _p(out))
+    return out
+
+
+def shear1h_mis_tab(lnm_x, lnm_w, W_gamma, norm, lnm_eff, mu2, method, stencil_h, R,
+                    f_mis, tau_mis, lob_centers, omega_m, conc, r_sigma, lnM_tab, dsig_tab,
+                    mis_table):
+    """Shear1hMisSelGL::evaluate with the miscentred profile read from the
+    reference's NFW_DSIGMA_MIS table; mis_table = (logx, logxmis, log_tab)
+    with log_tab [n_lxm, n_lx].  method 0 exact, 1 idea2."""
+    lx, lw, Wg, Rr = _f64(lnm_x), _f64(lnm_w), _f64(W_gamma), _f64(R)
+    nrm, eff, m2 = _f64(norm), _f64(lnm_eff), _f64(mu2)
+    lob, rs, lt, ds = _f64(lob_centers), _f64(r_sigma), _f64(lnM_tab), _f64(dsig_tab)
+    tx, txm, tv = (_f64(a) for a in mis_table)
+    nb = Wg.shape[0]
+    out = np.empty((nb, len(Rr)))
+    lib().y3o_shear1h_mis_tab(len(lx), _p(lx), _p(lw), nb, _p(Wg), _p(nrm), _p(eff), _p(m2),
+                              int(method), float(stencil_h), len(Rr), _p(Rr), f_mis, tau_mis,
+                              len(lob), _p(lob), omega_m, conc, len(rs), _p(rs), len(lt),
+                              _p(lt), _p(ds), len(tx), _p(tx), len(txm), _p(txm), _p(tv),
+                              _p(out))
     return out
 
 

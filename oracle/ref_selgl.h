@@ -1,0 +1,77 @@
+/*
+ * ref_selgl.h -- C interface to the reference's own fixed-GL module classes
+ * (SelGLCore, NumCountsSelGL, Shear1hMisSelGL of
+ * src/models/n_operator_sel_gl_t.hh:75-361), compiled from the reference's
+ * sources against the build shims in oracle/ref_shim/.
+ *
+ * TEST INFRASTRUCTURE ONLY.  The library (oracle/_ref/libselgl_ref.so) is
+ * built by `make -C oracle ref` from the reference checkout and is never
+ * committed.  It pins the oracle (oracle/y3o.c) and the CUDA path to the
+ * reference's own arithmetic, and serves as the timed reference CPU path.
+ * The product library never links or calls it.
+ *
+ * Arrays follow the DataBlock layouts the reference reads:
+ *   mass_function/dndlnmh  [n_hz][n_hm]   (z slow, mass fast)
+ *   sel_function/S_stack   [n_bins][n_sel_z][n_sel_lnm]
+ *   haloModel/dSigma_nfw   [n_hl][n_rs]   (lnM slow, R fast)
+ * Every call returns 0 on success; otherwise it copies the reference's
+ * exception text into err and returns non-zero.
+ */
+#ifndef Y3_REF_SELGL_H
+#define Y3_REF_SELGL_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  int n_lnm, n_z;          /* <= 0: leave unset (reference defaults 96, 64) */
+  double zt_low, zt_high, lnm_low, lnm_high;
+} y3r_cfg;
+
+typedef struct {
+  double omega_m, omega_nu, omega_lambda, omega_k, h0, hmf_s, hmf_q;
+  int n_hm, n_hz;
+  const double *m_h, *hmf_z, *dndlnmh;
+  int nd;
+  const double *dist_z, *dist_da;
+  int n_sci;                       /* 0: no average_sigma_crit_inv section */
+  const double *sci_z, *sci_val;
+  int n_bins, n_sel_z, n_sel_lnm;
+  const double *sel_lnm, *sel_z, *S_stack;
+  int n_rs, n_hl;                  /* 0: no haloModel section */
+  const double *r_sigma, *halo_lnM, *dsigma_nfw;
+  int has_f_mis, has_tau_mis;      /* miscentering/{f_mis,tau_mis} present */
+  double f_mis, tau_mis;
+} y3r_sample;
+
+/* SelGLCore::build_weights -> W [n_bins][n_lnm], norm, lnm_eff, mu2 per bin,
+ * and the GL mass nodes/weights (each may be NULL). */
+int y3r_selgl_weights(const y3r_cfg* cfg, const y3r_sample* s, int include_sci,
+                      double* W, double* norm, double* lnm_eff, double* mu2,
+                      double* lnm_x, double* lnm_w, char* err, int errlen);
+
+/* NumCountsSelGL: set_sample, then evaluate every bin -> vals[n_bins]. */
+int y3r_numcounts(const y3r_cfg* cfg, const y3r_sample* s, double* vals,
+                  char* err, int errlen);
+
+/* Shear1hMisSelGL: set_sample, then evaluate the (bin, R) product, bin slow
+ * and R fast -> vals[n_bins * n_R].  method: 0 exact, 1 idea2, -1 unset;
+ * stencil_h < 0: unset; lob_centers NULL: unset.  data_root is the directory
+ * holding data/nfw_off_center/ (exported as Y3_CLUSTER_CPP_DIR before the
+ * module is constructed, as the reference expects). */
+int y3r_shear1h(const y3r_cfg* cfg, int method, double stencil_h, int n_lob,
+                const double* lob_centers, const char* data_root,
+                const y3r_sample* s, int n_R, const double* R, double* vals,
+                char* err, int errlen);
+
+/* NFW_DSIGMA_MIS(c = 4, rho = RHOC, gamma kernel) with rho_mult = omega_m, at
+ * n points (r, r_mis, lnM) -> out[n]. */
+int y3r_nfw_dsigma_mis(const char* data_root, double omega_m, int n,
+                       const double* r, const double* rmis, const double* lnM,
+                       double* out, char* err, int errlen);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

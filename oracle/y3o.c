@@ -702,10 +702,13 @@ y3o_sigma_mis_unit(double x, double xmis, int n_theta, int n_s, double s_max)
  *   out[b, R] = sum_k w_k W_b[k] phi(b, R, lnM_k),
  *   phi = (1 - f) dSigma_nfw.clamp(R, lnM) + f NFW_DSIGMA_MIS(R, r_mis_b, lnM),
  * r_mis_b = tau R_lambda(lob_centers[b % n_lob]) (269-291,
- * lensing_weights.hh:167-198), NFW_DSIGMA_MIS with concentration conc and
- * rho = RHOC * Omega_M (set_rho_mult, nfw_dsigma_mis.hh:81,95-114).  The
- * miscentred profile comes from y3o_dsigma_mis_unit (the reference reads the
- * same quantity from a table that is not in the snapshot).
+ * lensing_weights.hh:167-198), NFW_DSIGMA_MIS with concentration conc.  The
+ * module constructs that class with rho_c = RHOC and then calls
+ * set_rho_mult(Omega_M) (n_operator_sel_gl_t.hh:248,264), so r_s comes from
+ * rho_c alone while the amplitude 2 r_s delta_c rho_c rho_mult carries Omega_M
+ * (nfw_dsigma_mis.hh:95-114).  The miscentred profile comes from
+ * y3o_dsigma_mis_unit (the reference reads the same quantity from a table
+ * that is not in the snapshot).
  * dsig_tab is the haloModel/dSigma_nfw ndarray, extents (n_ml, n_rs). */
 int
 y3o_shear1h_mis(int n_lnm, const double* lnm_x, const double* lnm_w,
@@ -716,16 +719,15 @@ y3o_shear1h_mis(int n_lnm, const double* lnm_x, const double* lnm_w,
                 const double* lnM_tab, const double* dsig_tab, int n_theta,
                 int n_s, double s_max, double* out)
 {
-  double rho = RHOC * omega_m;
   for (int b = 0; b < n_bins; ++b) {
     double rmis = tau_mis * pow(lob_centers[b % n_lob] / 100.0, 0.2);
     for (int r = 0; r < n_R; ++r) {
       double acc = 0.0;
       for (int k = 0; k < n_lnm; ++k) {
         double lnM = lnm_x[k];
-        double rs = y3o_nfw_rs(lnM, conc, rho);
+        double rs = y3o_nfw_rs(lnM, conc, RHOC);
         double cen = y3o_interp2d_clamp(r_sigma, n_rs, lnM_tab, n_ml, dsig_tab, R[r], lnM);
-        double mis = y3o_nfw_norm(lnM, conc, rho) *
+        double mis = y3o_nfw_norm(lnM, conc, RHOC) * omega_m *
                      y3o_dsigma_mis_unit(R[r] / rs, rmis / rs, n_theta, n_s, s_max);
         double phi = (1.0 - f_mis) * cen + f_mis * mis;
         acc += lnm_w[k] * W_gamma[(size_t)b * n_lnm + k] * phi;
@@ -733,6 +735,66 @@ y3o_shear1h_mis(int n_lnm, const double* lnm_x, const double* lnm_w,
       out[(size_t)b * n_R + r] = acc;
     }
   }
+  return 0;
+}
+
+/* NFW_DSIGMA_MIS::operator() as the reference evaluates it
+ * (nfw_dsigma_mis.hh:95-114): the unit miscentred profile is read from the
+ * table log_tab[j * n_lx + i] on the axes (logx[i], logxmis[j]) (the files
+ * nfw_off_center/table_1000_1e-03_5e+03_{gamma_logx, gamma_logxmis,
+ * log_deltasigma_gamma}.txt, x fastest) by clamped bilinear interpolation
+ * at (ln x, ln x_mis), x = r / r_s with r_s from rho_c, then scaled by
+ * 2 r_s delta_c rho_c rho_mult * 1e-12. */
+double
+y3o_dsigma_mis_tab(double r, double rmis, double lnM, double conc, double rhoc,
+                   double rho_mult, int n_lx, const double* logx, int n_lxm,
+                   const double* logxmis, const double* log_tab)
+{
+  double rs = y3o_nfw_rs(lnM, conc, rhoc);
+  double v = y3o_interp2d_clamp(logx, n_lx, logxmis, n_lxm, log_tab, log(r / rs),
+                                log(rmis / rs));
+  return y3o_nfw_norm(lnM, conc, rhoc) * rho_mult * exp(v);
+}
+
+/* Shear1hMisSelGL::evaluate with the tabulated miscentred profile, both
+ * methods (n_operator_sel_gl_t.hh:293-319):
+ *   exact (method 0): sum_k w_k W_b[k] phi(b, R, lnM_k);
+ *   idea2 (method 1): norm_b [phi(y0) + mu2_b/2 (phi(y0+h) - 2 phi(y0)
+ *                     + phi(y0-h)) / h^2] at y0 = lnm_eff_b. */
+int
+y3o_shear1h_mis_tab(int n_lnm, const double* lnm_x, const double* lnm_w,
+                    int n_bins, const double* W_gamma, const double* norm,
+                    const double* lnm_eff, const double* mu2, int method,
+                    double stencil_h, int n_R, const double* R, double f_mis,
+                    double tau_mis, int n_lob, const double* lob_centers,
+                    double omega_m, double conc, int n_rs, const double* r_sigma,
+                    int n_ml, const double* lnM_tab, const double* dsig_tab,
+                    int n_lx, const double* logx, int n_lxm,
+                    const double* logxmis, const double* log_tab, double* out)
+{
+#define Y3O_PHI(LNM)                                                            \
+  ((1.0 - f_mis) * y3o_interp2d_clamp(r_sigma, n_rs, lnM_tab, n_ml, dsig_tab,  \
+                                      R[r], (LNM)) +                            \
+   f_mis * y3o_dsigma_mis_tab(R[r], rmis, (LNM), conc, RHOC, omega_m, n_lx,     \
+                              logx, n_lxm, logxmis, log_tab))
+  for (int b = 0; b < n_bins; ++b) {
+    double rmis = tau_mis * pow(lob_centers[b % n_lob] / 100.0, 0.2);
+    for (int r = 0; r < n_R; ++r) {
+      double v;
+      if (method == 0) {
+        v = 0.0;
+        for (int k = 0; k < n_lnm; ++k)
+          v += lnm_w[k] * W_gamma[(size_t)b * n_lnm + k] * Y3O_PHI(lnm_x[k]);
+      } else {
+        double h = stencil_h, y0 = lnm_eff[b];
+        double c = Y3O_PHI(y0), p = Y3O_PHI(y0 + h), m = Y3O_PHI(y0 - h);
+        double d2 = (p - 2.0 * c + m) / (h * h);
+        v = norm[b] * (c + 0.5 * mu2[b] * d2);
+      }
+      out[(size_t)b * n_R + r] = v;
+    }
+  }
+#undef Y3O_PHI
   return 0;
 }
 

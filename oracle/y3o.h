@@ -100,6 +100,23 @@ int y3o_shear1h_mis(int n_lnm, const double* lnm_x, const double* lnm_w,
                     double conc, int n_rs, const double* r_sigma, int n_ml,
                     const double* lnM_tab, const double* dsig_tab,
                     int n_theta, int n_s, double s_max, double* out);
+/* The same with the miscentred profile read from the reference's table
+ * (log unit profile on ln x fastest, ln x_mis slow), exact (0) or idea2 (1). */
+double y3o_dsigma_mis_tab(double r, double rmis, double lnM, double conc,
+                          double rhoc, double rho_mult, int n_lx,
+                          const double* logx, int n_lxm, const double* logxmis,
+                          const double* log_tab);
+int y3o_shear1h_mis_tab(int n_lnm, const double* lnm_x, const double* lnm_w,
+                        int n_bins, const double* W_gamma, const double* norm,
+                        const double* lnm_eff, const double* mu2, int method,
+                        double stencil_h, int n_R, const double* R,
+                        double f_mis, double tau_mis, int n_lob,
+                        const double* lob_centers, double omega_m, double conc,
+                        int n_rs, const double* r_sigma, int n_ml,
+                        const double* lnM_tab, const double* dsig_tab,
+                        int n_lx, const double* logx, int n_lxm,
+                        const double* logxmis, const double* log_tab,
+                        double* out);
 
 /* ---- average Sigma_crit^-1 (a13) ----------------------------------------- */
 int y3o_sigma_crit_inv(int n_zl, const double* zl, int n_zs, const double* zs,

@@ -1,10 +1,10 @@
 """Generate the golden fixtures that pin the oracle to the reference.
 
-Run in a container that has the reference checkout at /root/reference
-(read-only); the outputs are committed, so neither the tests nor the GPU runs
-need the reference at run time:
+Run where a checkout of the reference exists (read-only is fine); the outputs
+are committed, so neither the tests nor the GPU runs need the reference at
+run time:
 
-    python tests/golden/make_golden.py [/root/reference]
+    python tests/golden/make_golden.py <reference-checkout>
 
 What it writes (tests/golden/*.npz / *.json):
 
@@ -24,6 +24,23 @@ What it writes (tests/golden/*.npz / *.json):
   cluster_toolkit answers of test/nfw_dsigma_mis.test.cu:32-48 and
   test/nfw_sigma_mis.test.cu:32-46, and the interpolation KATs of
   test/interp_1d.test.cc / test/interp_2d.test.cc.
+* sigma_crit_inv.npz -- <Sigma_crit^-1>(z_l) from the reference's own
+  src/modules/average_sigma_crit_inv/average_sigma_crit_inv.py execute()
+  (imported with CosmoSIS and astropy stubs; its setup() reads a FITS n(z)
+  that is not in the snapshot, so the config tuple is built here with the
+  synthetic source n(z): Gaussian, mean 0.9, sigma 0.3, 200 nodes).
+* selgl_ref.npz -- numcountssel/vals, SelGLCore weights and
+  shear1hmissel/vals (exact and idea2) from the reference's own C++
+  (src/models/n_operator_sel_gl_t.hh:75-361), compiled from its sources by
+  `make -C oracle ref` against the shims of oracle/ref_shim/, on the
+  S_stack fixtures above and the seeded synthetic tables of the configs
+  (Tinker-like HMF 100 x 50, flat LCDM distances, Sigma_crit^-1 64 nodes).
+  The miscentring table the shear module reads
+  (data/nfw_off_center/table_1000_1e-03_5e+03_log_deltasigma_gamma.txt) is
+  missing from the snapshot; the fixture carries a stand-in on every 8th ln x
+  and every 5th ln x_mis node of the shipped axis files, filled by the
+  oracle's direct quadrature of the gamma-kernel profile, and the reference
+  reads it through its own file loader.
 """
 from __future__ import annotations
 
@@ -37,6 +54,9 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
 
 
 def _install_cosmosis_stub():
@@ -212,7 +232,113 @@ def kats(ref):
     return out
 
 
-def main(ref="/root/reference"):
+def sigma_crit_inv_reference(ref):
+    """Runs average_sigma_crit_inv.execute() of the reference on synthetic
+    distances and n(z)."""
+    fits = types.ModuleType("astropy.io.fits")
+    io = types.ModuleType("astropy.io")
+    io.fits = fits
+    astropy = types.ModuleType("astropy")
+    astropy.io = io
+    sys.modules.update({"astropy": astropy, "astropy.io": io, "astropy.io.fits": fits})
+    sys.path.insert(0, os.path.join(ref, "src", "modules", "average_sigma_crit_inv"))
+    import average_sigma_crit_inv as sci_mod
+    from y3_cluster_cpp_b200 import synthetic
+
+    p = synthetic.fiducial()
+    zs, pz = synthetic.source_nz()
+    zl = np.linspace(0.05, 0.85, 64)
+    block = Block()
+    block["cosmological_parameters", "h0"] = p.h0
+    block["photoz", "delta_z"] = 0.0
+    block["distances", "z"] = p.tables["dist_z"]
+    block["distances", "d_a"] = p.tables["dist_da"]
+    sci_mod.execute(block, (zs, pz, zl, False))
+    return dict(zs=zs, pz=pz, zl=zl, h0=p.h0, delta_z=0.0, dist_z=p.tables["dist_z"],
+                dist_da=p.tables["dist_da"],
+                sci=np.asarray(block["average_sigma_crit_inv", "sci_average"]))
+
+
+def _write_mis_table(root, logx, logxmis, log_tab):
+    d = os.path.join(root, "data", "nfw_off_center")
+    os.makedirs(d, exist_ok=True)
+    stem = os.path.join(d, "table_1000_1e-03_5e+03_")
+    np.savetxt(stem + "gamma_logx.txt", logx, fmt="%.17g")
+    np.savetxt(stem + "gamma_logxmis.txt", logxmis, fmt="%.17g")
+    np.savetxt(stem + "log_deltasigma_gamma.txt", np.ravel(log_tab), fmt="%.17g")
+
+
+def selgl_reference(ref):
+    """Runs the reference's compiled SelGLCore / NumCountsSelGL /
+    Shear1hMisSelGL on fixture inputs."""
+    import subprocess
+
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", "REF=" + ref],
+                   check=True)
+    import oracle as O
+    from oracle import ref as R
+    from y3_cluster_cpp_b200 import synthetic
+
+    p = synthetic.fiducial()
+    t = p.tables
+    cosmo = dict(omega_m=p.om, omega_nu=0.0, omega_lambda=1.0 - p.om, omega_k=0.0, h0=p.h0,
+                 hmf_s=0.0, hmf_q=1.0)
+    out = dict(omega_m=p.om, h0=p.h0, **{"t_" + k: np.asarray(v) for k, v in t.items()})
+    cfgs = dict(a=dict(n_lnm=64, n_z=32, zt_low=0.1, zt_high=0.8, lnm_low=29.9336,
+                       lnm_high=35.69),
+                b=dict(zt_low=0.2, zt_high=0.65, lnm_low=30.0, lnm_high=36.5))
+    for name, c in cfgs.items():
+        for k, v in c.items():
+            out[f"cfg_{name}_{k}"] = v
+    sels = {}
+    for mor in ("hod", "lognormal"):
+        g = np.load(os.path.join(HERE, f"sel_function_{mor}.npz"))
+        sels[mor] = (g["lnM"], g["z"], g["S_stack"])
+    for cname in ("a", "b"):
+        for mor in ("hod", "lognormal"):
+            out[f"counts_{cname}_{mor}"] = R.numcounts(cfgs[cname], cosmo, t, sels[mor])
+    sci = (t["sci_z"], t["sci_val"])
+    W, norm, eff, mu2, lx, lw = R.selgl_weights(cfgs["a"], cosmo, t, sels["lognormal"], sci)
+    out.update(wsci_W=W, wsci_norm=norm, wsci_eff=eff, wsci_mu2=mu2, lnm_x=lx, lnm_w=lw)
+    # Miscentring table stand-in on a subset of the shipped axes.
+    axes = os.path.join(ref, "data", "nfw_off_center", "table_1000_1e-03_5e+03_gamma_")
+    lx_full = np.loadtxt(axes + "logx.txt")
+    lxm_full = np.loadtxt(axes + "logxmis.txt")
+    logx = lx_full[np.r_[0:len(lx_full):8, len(lx_full) - 1]]
+    logxmis = lxm_full[np.r_[0:len(lxm_full):5, len(lxm_full) - 1]]
+    # Where x << x_mis the profile is below 1e-11 and the quadrature loses it
+    # to cancellation (values of either sign); those corners, far from any
+    # (R, R_mis, M) the fixtures query, are floored at 1e-30 before the log.
+    tab = np.array([[np.log(max(O.dsigma_mis_unit(np.exp(a), np.exp(b)), 1e-30))
+                     for a in logx] for b in logxmis])
+    out.update(mis_logx=logx, mis_logxmis=logxmis, mis_log_tab=tab)
+    # Centred DeltaSigma table haloModel/{r_sigma, lnM, dSigma_nfw}: the
+    # analytic NFW (c = 4, rho = RHOC Omega_m) on 40 radii x 30 masses.
+    r_sigma = np.logspace(-2, 1.7, 40)
+    halo_lnM = np.linspace(29.9, 36.9, 30)
+    rho = 2.77533742639e11 * p.om
+    ds = np.array([[O.lib().y3o_nfw_norm(m, 4.0, rho) *
+                    O.lib().y3o_nfw_dsigma_unit(r / O.lib().y3o_nfw_rs(m, 4.0, rho))
+                    for r in r_sigma] for m in halo_lnM])
+    halo = dict(r_sigma=r_sigma, lnM=halo_lnM, dSigma_nfw=ds)
+    out.update(halo_r_sigma=r_sigma, halo_lnM=halo_lnM, halo_dSigma_nfw=ds)
+    R15 = np.logspace(np.log10(0.1), np.log10(30.0), 15)
+    out["R"] = R15
+    with tempfile.TemporaryDirectory() as d:
+        _write_mis_table(d, logx, logxmis, tab)
+        out["shear_exact_cfg2"] = R.shear1h(cfgs["a"], cosmo, t, sels["lognormal"], sci, halo,
+                                            R15, d, method=0,
+                                            mis=dict(f_mis=0.2, tau_mis=0.17))
+        out["shear_idea2_default"] = R.shear1h(cfgs["b"], cosmo, t, sels["hod"], sci, halo,
+                                               R15, d, method=1)
+        out["shear_exact_default_b"] = R.shear1h(cfgs["b"], cosmo, t, sels["hod"], sci, halo,
+                                                 R15, d)
+    return out
+
+
+def main(ref=None):
+    if ref is None:
+        raise SystemExit("usage: make_golden.py <reference-checkout>")
     _install_cosmosis_stub()
     with tempfile.TemporaryDirectory():
         lnm, z, S = run_sel_function(ref, lognormal=False)
@@ -229,6 +355,8 @@ def main(ref="/root/reference"):
                  **{"ln_" + k: np.asarray(v) for k, v in LOGNORMAL.items()})
     with open(os.path.join(HERE, "kats.json"), "w") as f:
         json.dump(kats(ref), f, indent=1)
+    np.savez_compressed(os.path.join(HERE, "sigma_crit_inv.npz"), **sigma_crit_inv_reference(ref))
+    np.savez_compressed(os.path.join(HERE, "selgl_ref.npz"), **selgl_reference(ref))
     print("wrote golden fixtures to", HERE)
 
 

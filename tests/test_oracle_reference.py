@@ -1,0 +1,111 @@
+"""Pins the oracle's SelGLCore / Shear1hMisSelGL / Sigma_crit^-1
+restatements to the reference's own code: golden vectors written by the
+reference's C++ module classes (compiled from the reference's sources against
+the shims of oracle/ref_shim/) and by the reference's
+average_sigma_crit_inv.py (tests/golden/make_golden.py), and, where the
+compiled reference library is present, the library itself on more inputs."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from oracle import ref as R
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module")
+def g():
+    return np.load(os.path.join(GOLD, "selgl_ref.npz"))
+
+
+def tables(g):
+    return {k[2:]: g[k] for k in g.files if k.startswith("t_")}
+
+
+def cfg(g, name):
+    c = dict(zt_low=float(g[f"cfg_{name}_zt_low"]), zt_high=float(g[f"cfg_{name}_zt_high"]),
+             lnm_low=float(g[f"cfg_{name}_lnm_low"]), lnm_high=float(g[f"cfg_{name}_lnm_high"]),
+             n_lnm=96, n_z=64)
+    for k in ("n_lnm", "n_z"):
+        if f"cfg_{name}_{k}" in g.files:
+            c[k] = int(g[f"cfg_{name}_{k}"])
+    return c
+
+
+def sel(mor):
+    s = np.load(os.path.join(GOLD, f"sel_function_{mor}.npz"))
+    return s["lnM"], s["z"], s["S_stack"]
+
+
+def oracle_weights(g, name, mor, with_sci):
+    c = cfg(g, name)
+    t = tables(g)
+    sci = (t["sci_z"], t["sci_val"]) if with_sci else None
+    cz = O.cosmo(float(g["omega_m"]), float(g["h0"]))
+    return O.selgl_weights(c["n_lnm"], c["n_z"], c["zt_low"], c["zt_high"], c["lnm_low"],
+                           c["lnm_high"], cz, t, sel(mor), sci)
+
+
+@pytest.mark.parametrize("name", ["a", "b"])
+@pytest.mark.parametrize("mor", ["hod", "lognormal"])
+def test_numcounts_oracle_matches_compiled_reference(g, name, mor):
+    _, norm, _, _ = oracle_weights(g, name, mor, False)
+    ref = g[f"counts_{name}_{mor}"]
+    assert np.all(ref > 0)
+    np.testing.assert_allclose(norm, ref, rtol=1e-12, atol=0)
+
+
+def test_selgl_weights_with_sigma_crit_match_compiled_reference(g):
+    W, norm, eff, mu2 = oracle_weights(g, "a", "lognormal", True)
+    np.testing.assert_allclose(W, g["wsci_W"], rtol=1e-12, atol=1e-12 * np.max(g["wsci_W"]))
+    np.testing.assert_allclose(norm, g["wsci_norm"], rtol=1e-12, atol=0)
+    np.testing.assert_allclose(eff, g["wsci_eff"], rtol=1e-13, atol=0)
+    np.testing.assert_allclose(mu2, g["wsci_mu2"], rtol=1e-10, atol=0)
+
+
+def _shear_oracle(g, name, mor, method, f_mis, tau_mis):
+    c = cfg(g, name)
+    W, norm, eff, mu2 = oracle_weights(g, name, mor, True)
+    lx, lw = O.gl_nodes(c["lnm_low"], c["lnm_high"], c["n_lnm"])
+    mis = (g["mis_logx"], g["mis_logxmis"], g["mis_log_tab"])
+    return O.shear1h_mis_tab(lx, lw, W, norm, eff, mu2, method, 0.15, g["R"], f_mis, tau_mis,
+                             [25.0, 37.5, 52.5, 130.0], float(g["omega_m"]), 4.0,
+                             g["halo_r_sigma"], g["halo_lnM"], g["halo_dSigma_nfw"], mis)
+
+
+@pytest.mark.parametrize("case", [("shear_exact_cfg2", "a", "lognormal", 0, 0.2, 0.17),
+                                  ("shear_idea2_default", "b", "hod", 1, 0.22, 0.17),
+                                  ("shear_exact_default_b", "b", "hod", 0, 0.22, 0.17)])
+def test_shear1h_oracle_matches_compiled_reference(g, case):
+    key, name, mor, method, f, tau = case
+    out = _shear_oracle(g, name, mor, method, f, tau).ravel()
+    ref = g[key]
+    assert np.all(np.isfinite(ref)) and np.max(np.abs(ref)) > 0
+    np.testing.assert_allclose(out, ref, rtol=1e-12, atol=1e-12 * np.max(np.abs(ref)))
+
+
+def test_sigma_crit_inv_matches_reference_python():
+    s = np.load(os.path.join(GOLD, "sigma_crit_inv.npz"))
+    out = O.sigma_crit_inv(s["zl"], s["zs"], s["pz"], float(s["delta_z"]), float(s["h0"]),
+                           s["dist_z"], s["dist_da"])
+    np.testing.assert_allclose(out, s["sci"], rtol=1e-10, atol=1e-10 * np.max(s["sci"]))
+
+
+@pytest.mark.skipif(not R.available(), reason="compiled reference (make -C oracle ref) absent")
+def test_oracle_matches_compiled_reference_on_walkers(g):
+    """The live reference library on walkers of the batched prior (their own
+    cosmologies and tables): counts and weights with Sigma_crit^-1."""
+    from y3_cluster_cpp_b200 import synthetic
+    for p in synthetic.walkers(6, seed=3, densities=(1,)):
+        cosmo = dict(omega_m=p.om, omega_nu=0.0, omega_lambda=1 - p.om, omega_k=0.0,
+                     h0=p.h0, hmf_s=0.0, hmf_q=1.0)
+        t = p.tables
+        for mor in ("hod", "lognormal"):
+            c = cfg(g, "a")
+            ref = R.numcounts(c, cosmo, t, sel(mor))
+            _, norm, _, _ = O.selgl_weights(c["n_lnm"], c["n_z"], c["zt_low"], c["zt_high"],
+                                            c["lnm_low"], c["lnm_high"], O.cosmo(p.om, p.h0),
+                                            t, sel(mor))
+            np.testing.assert_allclose(norm, ref, rtol=1e-12, atol=0)

@@ -141,6 +141,7 @@ def _declare(L):
                                   C.POINTER(Selection), I]
     L.y3b_selgl_counts.argtypes = [VP, I, PI, PD]
     L.y3b_selgl_shear.argtypes = [VP, C.POINTER(ShearTable), I, PI, PD, PD]
+    L.y3b_selgl_set_mis_table.argtypes = [VP, I, PD, I, PD, PD]
     L.y3b_selgl_weights.argtypes = [VP, PD, PD, PD, PD, PD, PD]
     L.y3b_selgl_n_bins.argtypes = [VP]
     L.y3b_selgl_destroy.argtypes = [VP]
@@ -209,7 +210,7 @@ def ptr(a):
 EXPORTED = [
     "y3b_last_error", "y3b_version", "y3b_device_init", "y3b_launch_count",
     "y3b_sel_function", "y3b_selgl_create", "y3b_selgl_build", "y3b_selgl_counts",
-    "y3b_selgl_shear", "y3b_selgl_weights", "y3b_selgl_n_bins", "y3b_selgl_destroy",
+    "y3b_selgl_shear", "y3b_selgl_set_mis_table", "y3b_selgl_weights", "y3b_selgl_n_bins", "y3b_selgl_destroy",
     "y3b_sigma_crit_inv", "y3b_nfw_mis", "y3b_engine_create", "y3b_engine_destroy",
     "y3b_engine_table_stride", "y3b_engine_table_offsets", "y3b_engine_n_bins",
     "y3b_engine_device_bytes", "y3b_engine_eval", "y3b_engine_eval_device",

@@ -10,6 +10,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -124,6 +126,24 @@ get_nd(c_datablock* b, const char* sec, const char* key, int ndim_expected,
   return out;
 }
 
+// Numbers of a whitespace-separated text file, skipping lines that start
+// with '#', as the reference's read_vector does (src/utils/read_vector.hh).
+[[maybe_unused]] bool
+read_numbers(const std::string& path, std::vector<double>& out)
+{
+  std::ifstream f(path);
+  if (!f) return false;
+  out.clear();
+  std::string line;
+  while (std::getline(f, line)) {
+    if (line.rfind('#', 0) == 0) continue;
+    std::istringstream ls(line);
+    double v;
+    while (ls >> v) out.push_back(v);
+  }
+  return true;
+}
+
 struct Module {
   y3b_selgl* core = nullptr;
   std::vector<int> bins;
@@ -224,6 +244,42 @@ setup(c_datablock* options)
 #endif
     int rc = y3b_selgl_create(&cfg, &m->core);
     if (rc != Y3B_OK) throw Failure{std::string("y3b_selgl_create: ") + y3b_last_error()};
+#if Y3B_MODULE_SHEAR
+    // NFW_DSIGMA_MIS reads its gamma-kernel profile table from
+    // $Y3_CLUSTER_CPP_DIR/data/nfw_off_center/ when the module is constructed
+    // (nfw_dsigma_mis.hh:33-55,62-72).  mis_profile = table requires those
+    // files, quadrature computes the profile directly, and the default uses
+    // the table when the files are present.
+    std::string mode = "auto";
+    if (const char* ps = opt_section(options, "mis_profile")) {
+      char* str = nullptr;
+      if (c_datablock_get_string(options, ps, "mis_profile", &str) == DBS_SUCCESS && str) {
+        mode = str;
+        std::free(str);
+      }
+    }
+    if (mode != "auto" && mode != "table" && mode != "quadrature")
+      throw Failure{"mis_profile must be 'table' or 'quadrature', got '" + mode + "'"};
+    if (mode != "quadrature") {
+      const char* root = std::getenv("Y3_CLUSTER_CPP_DIR");
+      std::string stem = std::string(root ? root : "") +
+                         "/data/nfw_off_center/table_1000_1e-03_5e+03_";
+      std::vector<double> lx, lxm, tab;
+      bool ok = root && read_numbers(stem + "gamma_logx.txt", lx) &&
+                read_numbers(stem + "gamma_logxmis.txt", lxm) &&
+                read_numbers(stem + "log_deltasigma_gamma.txt", tab);
+      if (ok) {
+        if (tab.size() != lx.size() * lxm.size())
+          throw Failure{"Interp2D -- wrong number of z values passed (" + stem +
+                        "log_deltasigma_gamma.txt)"};
+        rc = y3b_selgl_set_mis_table(m->core, (int)lx.size(), lx.data(), (int)lxm.size(),
+                                     lxm.data(), tab.data());
+        if (rc != Y3B_OK) throw Failure{y3b_last_error()};
+      } else if (mode == "table") {
+        throw Failure{"Failed to open file: " + stem + "*_gamma*.txt"};
+      }
+    }
+#endif
     return m;
   } catch (const Failure& f) {
     report("setup failed: " + f.msg);

@@ -361,24 +361,44 @@ selgl_build_kernel(int n_lnm, int n_z, const double* lnm_x, const double* lnm_w,
   }
 }
 
+// The miscentred-profile table NFW_DSIGMA_MIS reads: log of the unit profile
+// on ln x (fastest) and ln x_mis axes (nfw_dsigma_mis.hh:62-72,95-114).
+struct MisTable {
+  int n_lx, n_lxm;
+  const double* logx;
+  const double* logxmis;
+  const double* log_tab;  // [n_lxm][n_lx]
+};
+
 // phi(b, R, lnM) = (1 - f) dSigma_nfw.clamp(R, lnM) + f NFW_DSIGMA_MIS(R,
 // r_mis_b, lnM) for a list of (rmis, R, lnM) triples; one warp per triple
-// (n_operator_sel_gl_t.hh:343-349).
+// (n_operator_sel_gl_t.hh:343-349).  The module builds NFW_DSIGMA_MIS with
+// rho_c and sets rho_mult = Omega_M (n_operator_sel_gl_t.hh:248,264), so r_s
+// comes from rho_c and the amplitude 2 r_s delta_c rho_c rho_mult carries
+// Omega_M.  The profile is the reference's table (clamped bilinear at
+// (ln x, ln x_mis)) when one is loaded, otherwise the direct quadrature that
+// generates such a table.
 __global__ void __launch_bounds__(128)
 phi_list_kernel(int n, const double* rmis, const double* R, const double* lnM,
-                double f_mis, double conc, double rho, int n_r, const double* r_sigma,
-                int n_ml, const double* lnM_tab, const double* dsig, MisQuad q,
-                double* out)
+                double f_mis, double conc, double rhoc, double rho_mult, int n_r,
+                const double* r_sigma, int n_ml, const double* lnM_tab, const double* dsig,
+                MisQuad q, MisTable tab, double* out)
 {
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (w >= n) return;
-  const double rs = nfw_rs(lnM[w], conc, rho);
-  double mis = mis_partial<double>(q, R[w] / rs, rmis[w] / rs, true, lane);
-  mis = warp_sum(mis);
+  const double rs = nfw_rs(lnM[w], conc, rhoc);
+  double mis;
+  if (tab.log_tab) {
+    mis = exp(interp2d_clamp(tab.logx, tab.n_lx, tab.logxmis, tab.n_lxm, tab.log_tab,
+                             log(R[w] / rs), log(rmis[w] / rs)));
+  } else {
+    mis = mis_partial<double>(q, R[w] / rs, rmis[w] / rs, true, lane);
+    mis = warp_sum(mis);
+  }
   if (lane == 0) {
     double cen = interp2d_clamp(r_sigma, n_r, lnM_tab, n_ml, dsig, R[w], lnM[w]);
-    out[w] = (1.0 - f_mis) * cen + f_mis * nfw_norm(lnM[w], conc, rho) * mis;
+    out[w] = (1.0 - f_mis) * cen + f_mis * (nfw_norm(lnM[w], conc, rhoc) * rho_mult) * mis;
   }
 }
 
@@ -422,6 +442,8 @@ struct y3b_selgl {
   y3b::DevBuf<double> hax, hz, dn, dz, da, sz, sv, sel_lnm, sel_z, S;
   y3b::DevBuf<int> status;
   y3b::MisQuadCache quad;
+  y3b::DevBuf<double> tab_lx, tab_lxm, tab_v;  // miscentred-profile table (optional)
+  int tab_nlx = 0, tab_nlxm = 0;
   std::vector<double> h_norm, h_eff, h_mu2, h_lnm_x, h_lnm_w;
   int n_bins = 0;
   bool built = false;
@@ -617,6 +639,52 @@ y3b_selgl_weights(y3b_selgl* h, double* W, double* norm, double* lnm_eff, double
   return Y3B_OK;
 }
 
+// NFW_DSIGMA_MIS's profile table (nfw_dsigma_mis.hh:62-72): kept on the
+// device for the handle's shear evaluations; n_lx = 0 drops it.
+extern "C" int
+y3b_selgl_set_mis_table(y3b_selgl* h, int n_lx, const double* logx, int n_lxm,
+                        const double* logxmis, const double* log_tab)
+{
+  using namespace y3b;
+  clear_error();
+  if (!h) {
+    set_error("y3b_selgl_set_mis_table: null handle");
+    return Y3B_ERR_INVALID;
+  }
+  if (n_lx == 0) {
+    h->tab_nlx = h->tab_nlxm = 0;
+    return Y3B_OK;
+  }
+  if (n_lx < 2 || n_lxm < 2 || !logx || !logxmis || !log_tab) {
+    set_error("y3b_selgl_set_mis_table: need at least 2 x 2 nodes and three arrays");
+    return Y3B_ERR_INVALID;
+  }
+  for (int i = 1; i < n_lx; ++i)
+    if (!(logx[i] > logx[i - 1])) {
+      set_error("y3b_selgl_set_mis_table: ln x axis not increasing");
+      return Y3B_ERR_INVALID;
+    }
+  for (int j = 1; j < n_lxm; ++j)
+    if (!(logxmis[j] > logxmis[j - 1])) {
+      set_error("y3b_selgl_set_mis_table: ln x_mis axis not increasing");
+      return Y3B_ERR_INVALID;
+    }
+  const size_t nv = (size_t)n_lx * n_lxm;
+  for (size_t i = 0; i < nv; ++i)
+    if (!std::isfinite(log_tab[i])) {
+      set_error("y3b_selgl_set_mis_table: non-finite table entry");
+      return Y3B_ERR_DOMAIN;
+    }
+  h->tab_nlx = h->tab_nlxm = 0;
+  Y3B_TRY(h->tab_lx.upload(logx, n_lx, h->stream));
+  Y3B_TRY(h->tab_lxm.upload(logxmis, n_lxm, h->stream));
+  Y3B_TRY(h->tab_v.upload(log_tab, nv, h->stream));
+  Y3B_CUDA(cudaStreamSynchronize(h->stream));
+  h->tab_nlx = n_lx;
+  h->tab_nlxm = n_lxm;
+  return Y3B_OK;
+}
+
 // Shear1hMisSelGL::evaluate (n_operator_sel_gl_t.hh:293-319): exact =
 // sum_k w_k W_b[k] phi(b, R, lnM_k); idea2 = norm_b [phi + mu2/2 d2phi] at
 // lnm_eff with a 3-point stencil.
@@ -645,8 +713,9 @@ y3b_selgl_shear(y3b_selgl* h, const y3b_shear_table* st, int n, const int* bin_i
     }
   if (n == 0) return Y3B_OK;
   cudaStream_t s = h->stream;
-  Y3B_TRY(h->quad.ensure(st->n_theta, st->n_s, st->s_max, s));
-  const double rho = kRhoCrit * h->omega_m;
+  if (!h->tab_nlx) Y3B_TRY(h->quad.ensure(st->n_theta, st->n_s, st->s_max, s));
+  MisTable tab{h->tab_nlx, h->tab_nlxm, h->tab_lx.get(), h->tab_lxm.get(),
+               h->tab_nlx ? h->tab_v.get() : nullptr};
   const int nl = h->cfg.n_lnm;
   // Triples (rmis, R, lnM) of phi evaluations.
   std::vector<double> trm, tR, tM;
@@ -683,8 +752,9 @@ y3b_selgl_shear(y3b_selgl* h, const y3b_shear_table* st, int n, const int* bin_i
   Y3B_TRY(d_lt.upload(st->lnM, st->n_lnm, s));
   Y3B_TRY(d_ds.upload(st->dsigma, (size_t)st->n_r * st->n_lnm, s));
   phi_list_kernel<<<(nt * 32 + 127) / 128, 128, 0, s>>>(
-    nt, d_rm.get(), d_R.get(), d_M.get(), st->f_mis, st->conc, rho, st->n_r, d_rs.get(),
-    st->n_lnm, d_lt.get(), d_ds.get(), h->quad.view(), d_phi.get());
+    nt, d_rm.get(), d_R.get(), d_M.get(), st->f_mis, st->conc, kRhoCrit, h->omega_m, st->n_r,
+    d_rs.get(), st->n_lnm, d_lt.get(), d_ds.get(), h->tab_nlx ? MisQuad{} : h->quad.view(), tab,
+    d_phi.get());
   count_launch();
   Y3B_CUDA(cudaGetLastError());
   if (!st->use_idea2) {

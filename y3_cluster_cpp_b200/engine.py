@@ -113,6 +113,18 @@ class SelGL:
                                       ptr(w)))
         return dict(W=W, norm=norm, lnm_eff=eff, mu2=mu2, lnm_x=x, lnm_w=w)
 
+    def set_mis_table(self, logx=None, logxmis=None, log_tab=None):
+        """Miscentred-profile table (NFW_DSIGMA_MIS's file contents): ln x,
+        ln x_mis axes and log_tab [n_lxm, n_lx]; None returns to the direct
+        quadrature."""
+        if logx is None:
+            check(lib().y3b_selgl_set_mis_table(self._h, 0, None, 0, None, None))
+            return self
+        lx, lxm, tv = f64(logx), f64(logxmis), f64(log_tab)
+        check(lib().y3b_selgl_set_mis_table(self._h, len(lx), ptr(lx), len(lxm), ptr(lxm),
+                                            ptr(tv)))
+        return self
+
     def shear(self, bins, r, halo, f_mis=0.22, tau_mis=0.17,
               lob_centers=(25.0, 37.5, 52.5, 130.0), conc=4.0, n_theta=64, n_s=128,
               s_max=20.0, idea2=False, stencil_h=0.15):
