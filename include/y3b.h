@@ -228,7 +228,10 @@ typedef struct {
   int n_lam_bins, n_z_bins;             /* <= 8, <= 8 */
   double lam_edges[9];
   double zob_edges[9];
-  double sz0;                           /* sigma_z(z_t) = sz0 (1 + z_t) */
+  double sz0;                           /* sigma_z(z_t, j) = sz0 (1 + z_t) + sz_bin[j] */
+  double sz_bin[8];                     /* per z_obs bin; sz0 = 0 and sz_bin = the bins'
+                                           sigma_z is sel_function.py's photo-z model
+                                           (_K_j, sel_function.py:260-262) */
 } y3b_grid;
 
 typedef struct {

@@ -53,7 +53,7 @@ class DirectGrid(C.Structure):
                 ("lnm_lo", D), ("lnm_hi", D), ("zt_lo", D), ("zt_hi", D),
                 ("lam_t_lo", D), ("lam_t_hi", D),
                 ("n_lam_bins", I), ("n_z_bins", I),
-                ("lam_edges", PD), ("zob_edges", PD), ("sz0", D)]
+                ("lam_edges", PD), ("zob_edges", PD), ("sz0", D), ("sz_bin", PD)]
 
 
 class Lognormal(C.Structure):
@@ -281,15 +281,16 @@ def direct_eval(grid, plob_z, plob_coef, mor, cz, tables, shear=None):
     """Direct FP64 nested-GL evaluation of one parameter point.
 
     grid: dict (n_m, n_z, n_t, n_o, n_zo, lnm_lo, lnm_hi, zt_lo, zt_hi,
-    lam_t_lo, lam_t_hi, lam_edges, zob_edges, sz0); mor: dict (A, B, C,
+    lam_t_lo, lam_t_hi, lam_edges, zob_edges, sz0, optional sz_bin); mor: dict (A, B, C,
     sigma, Mpiv); shear: optional dict (R, f_mis, tau_mis, lob_centers, c0,
     c_slope, c_pivot, n_theta, n_s, s_max, sci_z, sci_val).
     Returns counts [n_bins], W [n_bins, n_m], shear [n_bins, n_R] or None."""
     le, ze = _f64(grid["lam_edges"]), _f64(grid["zob_edges"])
+    szb = None if grid.get("sz_bin") is None else _f64(grid["sz_bin"])
     g = DirectGrid(grid["n_m"], grid["n_z"], grid["n_t"], grid["n_o"], grid["n_zo"],
                    grid["lnm_lo"], grid["lnm_hi"], grid["zt_lo"], grid["zt_hi"],
                    grid["lam_t_lo"], grid["lam_t_hi"], len(le) - 1, len(ze) - 1,
-                   _p(le), _p(ze), grid["sz0"])
+                   _p(le), _p(ze), grid["sz0"], _p(szb))
     m = Lognormal(mor["A"], mor["B"], mor["C"], mor["sigma"], mor["Mpiv"])
     pz, pc = _f64(plob_z), _f64(plob_coef)
     mh, hz, dn = _f64(tables["hmf_m_h"]), _f64(tables["hmf_z"]), _f64(tables["dndlnmh"])

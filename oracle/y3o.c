@@ -840,7 +840,9 @@ y3o_sigma_crit_inv(int n_zl, const double* zl, int n_zs, const double* zs,
  * bin), contracted in the order lam_o -> lam_t -> (z_t, lnM) of
  * SelGLCore (n_operator_sel_gl_t.hh:91-143):
  *   K_i(t,q)  = sum_o a_o P(lam_o | lam_t, z_q)          (pdf of sel_function.py:153-192)
- *   K_j(q)    = sum_zo b N(z_o; z_q, sz0 (1+z_q))
+ *   K_j(q)    = sum_zo b N(z_o; z_q, sz0 (1+z_q) + sz_bin[j])
+ *               (sz_bin[j] alone is sel_function.py's constant sigma_z of
+ *               the z bin, _K_j at sel_function.py:260-262)
  *   S_i(k,q)  = sum_t u_t K_i(t,q) phi((l_t - mu_kq)/s) / (s D_kq)
  *   W_ij(k)   = sum_q v_q dV(z_q) Omega(z_q) [Sci(z_q)] K_j(q) n(M_k,z_q) S_i(k,q)
  *   N_ij      = sum_k w_k W_ij(k),   N_ij(R) = sum_k w_k W^gamma_ij(k) Phi_i(R,k)
@@ -892,8 +894,8 @@ y3o_direct_eval(const y3o_direct_grid* g, int n_plob, const double* plob_z,
   /* K_j(q) */
   double* Kj = malloc(sizeof(double) * nJ * nz);
   for (int q = 0; q < nz; ++q) {
-    double sz = g->sz0 * (1.0 + xz[q]);
     for (int j = 0; j < nJ; ++j) {
+      double sz = g->sz0 * (1.0 + xz[q]) + (g->sz_bin ? g->sz_bin[j] : 0.0);
       double acc = 0.0;
       for (int o = 0; o < g->n_zo; ++o) {
         double d = (zo_x[j * g->n_zo + o] - xz[q]) / sz;

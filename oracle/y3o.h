@@ -132,7 +132,8 @@ typedef struct {
   int n_lam_bins, n_z_bins;
   const double* lam_edges;               /* n_lam_bins + 1 */
   const double* zob_edges;               /* n_z_bins + 1 */
-  double sz0;                            /* sigma_z = sz0 (1 + z_t) */
+  double sz0;                            /* sigma_z = sz0 (1 + z_t) + sz_bin[j] */
+  const double* sz_bin;                  /* n_z_bins constants, or NULL */
 } y3o_direct_grid;
 
 typedef struct {

@@ -146,27 +146,3 @@ def test_nfw_unit_profile_consistency():
         sbar = 2.0 / x ** 2 * np.dot(ws, xs * sig)
         ds = O.lib().y3o_nfw_dsigma_unit(x) + O.lib().y3o_nfw_sigma_unit(x)
         assert ds == pytest.approx(sbar, rel=2e-6)
-
-
-def test_direct_quadrature_tracks_reference_chain():
-    """O2 (direct nested GL) vs O1 (reference tabulate-then-interpolate chain)
-    on the same inputs: their gap is the tabulation error of the reference
-    chain, reported here (not asserted tighter than the chain's own ~1e-2)."""
-    from y3_cluster_cpp_b200 import synthetic
-    g = synthetic.grid(1)
-    p = synthetic.fiducial()
-    pz, pc = synthetic.plob_baseline()
-    c = O.cosmo(p.om, p.h0)
-    counts, _, _ = O.direct_eval(g, pz, pc, p.mor, c, p.tables)
-    assert np.all(counts > 0)
-    # O1 chain on the same box with the same lognormal MOR
-    cfg = dict(lam_min=np.tile(g["lam_edges"][:-1], 3), lam_max=np.tile(g["lam_edges"][1:], 3),
-               zob_min=np.repeat(g["zob_edges"][:-1], 4), zob_max=np.repeat(g["zob_edges"][1:], 4),
-               sigma_z=np.full(12, 0.01 * 1.45), zt_low=g["zt_lo"], zt_high=g["zt_hi"],
-               lnm_low=g["lnm_lo"], lnm_high=g["lnm_hi"], n_lnm=192, n_z=64, n_q=32)
-    mor = [p.A, p.B, p.C, p.sigma, p.Mpiv, g["lam_t_lo"], g["lam_t_hi"]]
-    sel = O.sel_function(cfg, O.MOR_LOGNORMAL, mor, pz, pc)
-    _, norm, _, _ = O.selgl_weights(96, 64, g["zt_lo"], g["zt_hi"], g["lnm_lo"], g["lnm_hi"],
-                                    c, p.tables, sel)
-    gap = np.abs(norm / counts - 1)
-    assert np.all(gap < 1e-2), gap

@@ -109,3 +109,37 @@ def test_oracle_matches_compiled_reference_on_walkers(g):
                                             c["lnm_low"], c["lnm_high"], O.cosmo(p.om, p.h0),
                                             t, sel(mor))
             np.testing.assert_allclose(norm, ref, rtol=1e-12, atol=0)
+
+
+def test_direct_quadrature_converges_to_reference_chain():
+    """O2 (the direct nested-GL quadrature every engine test compares with)
+    against the reference chain (sel_function.py tabulation of S_stack, then
+    SelGLCore's interpolation and z/lnM contraction; both restatements are
+    pinned above and in test_oracle_golden.py to the reference's own code) on
+    the same integral: the lognormal MOR of the configs, the constant-in-z
+    projection coefficients and sel_function's photo-z model (constant
+    sigma_z = 0.03 per bin).  The chain's only approximation is the bilinear
+    interpolation of its S table, so the gap must shrink as O(h^2) when the
+    table is refined, to a few 1e-5 at 768 x 256 x 64 cells."""
+    from y3_cluster_cpp_b200 import synthetic
+    g = synthetic.grid(4)
+    g["sz0"], g["sz_bin"] = 0.0, np.full(3, 0.03)
+    p = synthetic.fiducial()
+    pz, pc = synthetic.plob_baseline()
+    c = O.cosmo(p.om, p.h0)
+    counts, _, _ = O.direct_eval(g, pz, pc, p.mor, c, p.tables)
+    mor = [p.A, p.B, p.C, p.sigma, p.Mpiv, g["lam_t_lo"], g["lam_t_hi"]]
+    gaps = []
+    for n_lnm, n_z, n_q in ((192, 64, 32), (768, 256, 64)):
+        cfgs = dict(lam_min=np.tile(g["lam_edges"][:-1], 3),
+                    lam_max=np.tile(g["lam_edges"][1:], 3),
+                    zob_min=np.repeat(g["zob_edges"][:-1], 4),
+                    zob_max=np.repeat(g["zob_edges"][1:], 4), sigma_z=np.full(12, 0.03),
+                    zt_low=g["zt_lo"], zt_high=g["zt_hi"], lnm_low=g["lnm_lo"],
+                    lnm_high=g["lnm_hi"], n_lnm=n_lnm, n_z=n_z, n_q=n_q)
+        sel = O.sel_function(cfgs, O.MOR_LOGNORMAL, mor, pz, pc)
+        _, norm, _, _ = O.selgl_weights(g["n_m"], g["n_z"], g["zt_lo"], g["zt_hi"],
+                                        g["lnm_lo"], g["lnm_hi"], c, p.tables, sel)
+        gaps.append(np.max(np.abs(norm / counts - 1)))
+    assert gaps[1] < 3e-5, gaps
+    assert gaps[1] < gaps[0] / 8, gaps

@@ -81,7 +81,7 @@ class Grid(C.Structure):
     _fields_ = [("n_m", I), ("n_z", I), ("n_t", I), ("n_o", I), ("n_zo", I),
                 ("lnm_lo", D), ("lnm_hi", D), ("zt_lo", D), ("zt_hi", D),
                 ("lam_t_lo", D), ("lam_t_hi", D), ("n_lam_bins", I), ("n_z_bins", I),
-                ("lam_edges", D * 9), ("zob_edges", D * 9), ("sz0", D)]
+                ("lam_edges", D * 9), ("zob_edges", D * 9), ("sz0", D), ("sz_bin", D * 8)]
 
 
 class ShearOpts(C.Structure):

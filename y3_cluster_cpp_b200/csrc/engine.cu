@@ -57,14 +57,18 @@ uk_kernel(int nI, int n_z, int n_t, int n_t_pad, const double* wl, const double*
   UK[idx] = t < n_t ? (float)(wl[t] * Ki[(size_t)iq * n_t + t]) : 0.f;
 }
 
+struct SzBins {
+  double v[8];
+};
+
 __global__ void
-kj_kernel(int nJ, int n_z, int n_zo, double sz0, const double* xz, const double* zo_x,
-          const double* zo_w, double* Kj, double* omz)
+kj_kernel(int nJ, int n_z, int n_zo, double sz0, SzBins szb, const double* xz,
+          const double* zo_x, const double* zo_w, double* Kj, double* omz)
 {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= nJ * n_z) return;
   const int q = idx % n_z, j = idx / n_z;
-  const double z = xz[q], sz = sz0 * (1.0 + z);
+  const double z = xz[q], sz = sz0 * (1.0 + z) + szb.v[j];
   double acc = 0.0;
   for (int o = 0; o < n_zo; ++o) {
     double d = (zo_x[j * n_zo + o] - z) / sz;
@@ -922,6 +926,7 @@ build_grid(y3b_engine* e, int gi)
   g.ll_lo = std::log(in.lam_t_lo);
   g.ll_hi = std::log(in.lam_t_hi);
   g.sz0 = in.sz0;
+  for (int j = 0; j < 8; ++j) g.sz_bin[j] = j < in.n_z_bins ? in.sz_bin[j] : 0.0;
   Y3B_TRY(b->xm.alloc(g.n_m));
   Y3B_TRY(b->wm.alloc(g.n_m));
   Y3B_TRY(b->xz.alloc(g.n_z));
@@ -968,7 +973,9 @@ build_grid(y3b_engine* e, int gi)
   count_launch();
   Y3B_CUDA(cudaGetLastError());
   int nkj = g.nJ * g.n_z;
-  kj_kernel<<<(nkj + 127) / 128, 128, 0, s>>>(g.nJ, g.n_z, g.n_zo, g.sz0, b->xz.get(),
+  SzBins szb;
+  for (int j = 0; j < 8; ++j) szb.v[j] = g.sz_bin[j];
+  kj_kernel<<<(nkj + 127) / 128, 128, 0, s>>>(g.nJ, g.n_z, g.n_zo, g.sz0, szb, b->xz.get(),
                                              b->zo_x.get(), b->zo_w.get(), b->Kj.get(),
                                              b->omz.get());
   count_launch();
@@ -1055,10 +1062,15 @@ validate_grid(const y3b_grid& g)
     return Y3B_ERR_UNSUPPORTED;
   }
   if (!(g.lnm_hi > g.lnm_lo) || !(g.zt_hi > g.zt_lo) || !(g.lam_t_lo > 0.0) ||
-      !(g.lam_t_hi > g.lam_t_lo) || !(g.sz0 > 0.0)) {
+      !(g.lam_t_hi > g.lam_t_lo) || !(g.sz0 >= 0.0)) {
     set_error("y3b_engine_create: grid bounds must be ordered and positive");
     return Y3B_ERR_INVALID;
   }
+  for (int j = 0; j < g.n_z_bins && j < 8; ++j)
+    if (!(g.sz_bin[j] >= 0.0) || !(g.sz0 + g.sz_bin[j] > 0.0)) {
+      set_error("y3b_engine_create: sigma_z must be positive in every z_obs bin");
+      return Y3B_ERR_INVALID;
+    }
   for (int i = 0; i < g.n_lam_bins; ++i)
     if (!(g.lam_edges[i + 1] > g.lam_edges[i])) {
       set_error("y3b_engine_create: lam_edges must increase");

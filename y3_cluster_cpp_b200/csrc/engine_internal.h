@@ -38,6 +38,7 @@ struct GridDev {
   int tiles_pp;    // contraction tiles per point: (n_m_pad / kGemmRows) * n_bg
   int cost_rank;   // 0 = the grid with the most expensive tiles (scheduled first)
   double lnm_lo, lnm_hi, zt_lo, zt_hi, ll_lo, ll_hi, sz0;
+  double sz_bin[8];   // sigma_z(z, j) = sz0 (1 + z) + sz_bin[j]
   const double* xm;   // [n_m]  lnM nodes
   const double* wm;
   const double* xz;   // [n_z]  z_t nodes

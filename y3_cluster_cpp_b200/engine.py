@@ -170,6 +170,8 @@ def make_grid(g):
         G.lam_edges[i] = v
     for i, v in enumerate(ze):
         G.zob_edges[i] = v
+    for j, v in enumerate(g.get("sz_bin") if g.get("sz_bin") is not None else []):
+        G.sz_bin[j] = float(v)
     return G
 
 
