@@ -20,6 +20,18 @@
  *            std::out_of_range cross the C boundary).
  *   cleanup  replaces module_macros.hh:93-98; returns 0.
  *
+ * With the option engine = fused in its section, a number-count module
+ * (NumCountsSel.so / NumCountsFastMass.so) computes the whole integral
+ * itself -- the lambda_t / lambda_obs / z_obs stage that sel_function.py
+ * tabulates into S_stack included -- on the engine's fixed nested
+ * Gauss-Legendre nodes (y3b_engine_eval, one parameter point per execute),
+ * in precision = mixed (default) or fp64.  It then reads the sel_function
+ * options (lam_min, lam_max, zob_min, zob_max, sigma_z per bin; from its own
+ * section or the sel_function section), the lognormal MOR from
+ * cluster_mor/{A, B, C, sigma_intr, M_pivot} and P(lambda_obs | lambda_true)
+ * from the plob_ltr_params section (the default projection table when absent), and
+ * with write_s_stack = T also writes sel_function/{lnM, z, S_stack}.
+ *
  * The DataBlock is CosmoSIS's opaque c_datablock.  The modules call only the
  * C accessors declared below, which the host process provides at load time
  * (libcosmosis inside CosmoSIS; libdatablock_shim.so in the tests).
@@ -70,6 +82,9 @@ DATABLOCK_STATUS c_datablock_get_double_array(c_datablock* s, const char* sectio
 DATABLOCK_STATUS c_datablock_put_double_array_1d(c_datablock* s, const char* section,
                                                  const char* name, const double* val,
                                                  int size);
+DATABLOCK_STATUS c_datablock_put_double_array(c_datablock* s, const char* section,
+                                              const char* name, const double* val,
+                                              int ndims, const int* extents);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -69,3 +69,35 @@ def test_compute_without_gpu_fails_loudly():
     with pytest.raises(_capi.Y3BError) as e:
         engine.nfw_mis("dsigma", [0.5], [0.1], [32.0], 4.0, 8e10)
     assert e.value.status == 3
+
+
+def test_fused_module_setup_validates_bins_on_cpu():
+    """engine = fused checks the sel_function bin layout at setup (no device
+    work): a richness-fast product of contiguous bins with one sigma_z per
+    z_obs bin, known precision."""
+    import numpy as np
+    from y3_cluster_cpp_b200.cosmosis import DataBlock, Module
+
+    def opts(**over):
+        o = DataBlock()
+        lab = "NumCountsFastMass"
+        d = dict(engine="fused", bin_index=np.arange(12),
+                 lam_min=[20.0, 30.0, 45.0, 60.0] * 3, lam_max=[30.0, 45.0, 60.0, 200.0] * 3,
+                 zob_min=[0.2] * 4 + [0.35] * 4 + [0.5] * 4,
+                 zob_max=[0.35] * 4 + [0.5] * 4 + [0.65] * 4, sigma_z=[0.03] * 12,
+                 zt_low=0.1, zt_high=0.8, lnm_low=29.9, lnm_high=35.7)
+        d.update(over)
+        for k, v in d.items():
+            o[lab, k] = np.asarray(v, float) if isinstance(v, list) else v
+        return o
+
+    m = Module("NumCountsFastMass")
+    assert m.setup(opts())
+    m.cleanup()
+    assert not Module("NumCountsFastMass").setup(opts(precision="fp16"))
+    assert not Module("NumCountsFastMass").setup(opts(engine="other"))
+    bad = [20.0, 30.0, 45.0, 61.0] * 3                       # gap between bins
+    assert not Module("NumCountsFastMass").setup(opts(lam_min=bad))
+    assert not Module("NumCountsFastMass").setup(opts(sigma_z=[0.03] * 11 + [0.05]))
+    assert not Module("NumCountsFastMass").setup(opts(bin_index=np.arange(13)))
+    assert not Module("Shear1hFastMass").setup(opts())       # counts only

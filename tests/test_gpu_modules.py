@@ -281,3 +281,96 @@ def test_sigma_crit_inv_matches_reference_python(gpu):
     out = E.sigma_crit_inv(s["zl"], s["zs"], s["pz"], float(s["delta_z"]), float(s["h0"]),
                            s["dist_z"], s["dist_da"])
     np.testing.assert_allclose(out, s["sci"], rtol=1e-10, atol=1e-10 * np.max(s["sci"]))
+
+
+# ---- engine = fused: the whole integral behind the module ABI --------------
+
+def _fused_options(label, g, precision, sigma_z, sz0, bins=None, **extra):
+    o = DataBlock()
+    o[label, "engine"] = "fused"
+    o[label, "precision"] = precision
+    o[label, "bin_index"] = np.arange(12) if bins is None else np.asarray(bins)
+    le, ze = g["lam_edges"], g["zob_edges"]
+    o[label, "lam_min"] = np.tile(le[:-1], 3)
+    o[label, "lam_max"] = np.tile(le[1:], 3)
+    o[label, "zob_min"] = np.repeat(ze[:-1], 4)
+    o[label, "zob_max"] = np.repeat(ze[1:], 4)
+    o[label, "sigma_z"] = np.repeat(sigma_z, 4)
+    o[label, "sz0"] = sz0
+    for k, v in dict(zt_low=g["zt_lo"], zt_high=g["zt_hi"], lnm_low=g["lnm_lo"],
+                     lnm_high=g["lnm_hi"]).items():
+        o[label, k] = float(v)
+    o[label, "n_lnm"], o[label, "n_z"], o[label, "n_lt"] = g["n_m"], g["n_z"], g["n_t"]
+    o[label, "n_lo"], o[label, "n_zo"] = g["n_o"], g["n_zo"]
+    for k, v in extra.items():
+        o[label, k] = v
+    return o
+
+
+def _fused_sample(p, pz, pc):
+    b = _sample_block(p)
+    for k, v in dict(A=p.A, B=p.B, C=p.C, sigma_intr=p.sigma, M_pivot=p.Mpiv).items():
+        b["cluster_mor", k] = v
+    b["plob_ltr_params", "z"] = pz
+    from y3_cluster_cpp_b200 import prj_params
+    for k, row in zip(prj_params.COEFF_NAMES, pc):
+        b["plob_ltr_params", k] = row
+    return b
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-8), ("mixed", 1e-4)])
+@pytest.mark.parametrize("photoz", ["baseline", "reference"])
+def test_fused_numcounts_module_matches_oracle(gpu, precision, tol, photoz):
+    """NumCountsFastMass.so with engine = fused, driven through setup /
+    execute / cleanup on a DataBlock, against the FP64 direct quadrature
+    (oracle) on the same nodes: the configs' photo-z sigma = 0.01 (1 + z) and
+    sel_function's constant per-bin sigma_z."""
+    g = synthetic.grid(1)
+    if photoz == "baseline":
+        sz, sz0 = np.zeros(3), 0.01
+    else:
+        sz, sz0 = np.full(3, 0.03), 0.0
+    g["sz0"], g["sz_bin"] = sz0, sz
+    p = synthetic.fiducial()
+    pz, pc = synthetic.plob_baseline()
+    ref, _, _ = O.direct_eval(g, pz, pc, p.mor, O.cosmo(p.om, p.h0), p.tables)
+    bins = [3, 0, 11, 5]
+    m = Module("NumCountsFastMass")
+    assert m.setup(_fused_options("NumCountsFastMass", g, precision, sz, sz0, bins=bins))
+    block = _fused_sample(p, pz, pc)
+    for _ in range(2):                       # second call reuses the engine
+        assert m.execute(block) == 0
+        vals = block["numcounts_fast_mass", "vals"]
+        np.testing.assert_allclose(vals, ref[bins], rtol=tol, atol=0)
+    m.cleanup()
+
+
+def test_fused_module_writes_s_stack_and_defaults(gpu):
+    """write_s_stack = T also publishes sel_function/{lnM, z, S_stack} (the
+    lognormal MOR, as y3b_sel_function); without plob_ltr_params the frozen
+    projection table is used, as sel_function.py does."""
+    g = synthetic.grid(1)
+    p = synthetic.fiducial()
+    from y3_cluster_cpp_b200 import prj_params
+    pz, pc = prj_params.default_table()
+    m = Module("NumCountsFastMass")
+    assert m.setup(_fused_options("NumCountsFastMass", g, "fp64", np.full(3, 0.03), 0.0,
+                                  write_s_stack=1))
+    block = _sample_block(p)
+    for k, v in dict(A=p.A, B=p.B, C=p.C, sigma_intr=p.sigma).items():
+        block["cluster_mor", k] = v
+    assert m.execute(block) == 0
+    S = block["sel_function", "S_stack"]
+    assert S.shape == (12, 20, 40)
+    g2 = dict(g, sz0=0.0, sz_bin=np.full(3, 0.03))
+    ref, _, _ = O.direct_eval(g2, pz, pc, p.mor, O.cosmo(p.om, p.h0), p.tables)
+    np.testing.assert_allclose(block["numcounts_fast_mass", "vals"], ref, rtol=1e-8)
+    cfg = dict(lam_min=np.tile(g["lam_edges"][:-1], 3), lam_max=np.tile(g["lam_edges"][1:], 3),
+               zob_min=np.repeat(g["zob_edges"][:-1], 4),
+               zob_max=np.repeat(g["zob_edges"][1:], 4), sigma_z=np.full(12, 0.03),
+               zt_low=g["zt_lo"], zt_high=g["zt_hi"], lnm_low=g["lnm_lo"],
+               lnm_high=g["lnm_hi"], n_lnm=40, n_z=20, n_q=32)
+    _, _, S2 = E.sel_function(cfg, O.MOR_LOGNORMAL,
+                              [p.A, p.B, p.C, p.sigma, p.Mpiv, 1.0, 1000.0], pz, pc)
+    np.testing.assert_array_equal(S, S2)
+    m.cleanup()

@@ -15,6 +15,7 @@
 #include <string>
 #include <vector>
 
+#include "prj_table.h"
 #include "y3b.h"
 #include "y3b_cosmosis.h"
 
@@ -144,14 +145,34 @@ read_numbers(const std::string& path, std::vector<double>& out)
   return true;
 }
 
+// engine = fused: the whole number-count integral on the engine's nested
+// Gauss-Legendre nodes, one parameter point per execute.
+struct Fused {
+  y3b_grid grid{};
+  int precision = Y3B_MIXED;
+  bool write_s = false;
+  y3b_selfunc_config scfg{};                 // S_stack grid (write_s_stack)
+  std::vector<double> lam_min, lam_max, zob_min, zob_max, sigma_z;
+  y3b_engine* e = nullptr;
+  int n_hm = -1, n_hz = -1, n_dist = -1;
+  std::vector<double> plob_z, plob_coef;
+  std::vector<double> packed;
+  ~Fused() { y3b_engine_destroy(e); }
+};
+
 struct Module {
   y3b_selgl* core = nullptr;
+  Fused* fused = nullptr;
   std::vector<int> bins;
   std::vector<double> r_perp;  // shear only
   std::vector<double> lob_centers;
   bool idea2 = false;
   double stencil_h = 0.15;
-  ~Module() { y3b_selgl_destroy(core); }
+  ~Module()
+  {
+    y3b_selgl_destroy(core);
+    delete fused;
+  }
 };
 
 // Sample tables held while one execute() runs.
@@ -204,6 +225,241 @@ build(Module* m, Sample& s, bool with_sci)
   return y3b_selgl_build(m->core, &s.c, &t, &sel, with_sci ? 1 : 0);
 }
 
+std::string
+opt_string(c_datablock* b, const char* key, const char* dflt)
+{
+  const char* s = opt_section(b, key);
+  char* str = nullptr;
+  if (s && c_datablock_get_string(b, s, key, &str) == DBS_SUCCESS && str) {
+    std::string v(str);
+    std::free(str);
+    return v;
+  }
+  return dflt;
+}
+
+[[maybe_unused]] bool
+opt_bool(c_datablock* b, const char* key, bool dflt)
+{
+  const char* s = opt_section(b, key);
+  if (!s) return dflt;
+  int v;
+  if (c_datablock_get_int(b, s, key, &v) == DBS_SUCCESS) return v != 0;
+  std::string t = opt_string(b, key, "");
+  if (t == "T" || t == "t" || t == "true" || t == "True" || t == "1") return true;
+  if (t == "F" || t == "f" || t == "false" || t == "False" || t == "0") return false;
+  throw Failure{std::string("option ") + key + " must be a boolean"};
+}
+
+// sel_function's per-bin option, from the module's section or the
+// sel_function section of the same ini.
+[[maybe_unused]] std::vector<double>
+bin_option(c_datablock* b, const char* key)
+{
+  const char* s = opt_section(b, key);
+  if (!s && c_datablock_has_value(b, "sel_function", key)) s = "sel_function";
+  return get_vec(b, s, key);
+}
+
+// Distinct intervals in order, from a per-bin edge list with a period.
+[[maybe_unused]] void
+product_edges(const std::vector<double>& lo, const std::vector<double>& hi, int stride,
+              int count, std::vector<double>& edges, const char* what)
+{
+  edges.clear();
+  for (int k = 0; k < count; ++k) {
+    double a = lo[(size_t)k * stride], c = hi[(size_t)k * stride];
+    if (!(c > a)) throw Failure{std::string(what) + " bins must have max > min"};
+    if (k == 0)
+      edges.push_back(a);
+    else if (a != edges.back())
+      throw Failure{std::string("engine = fused needs contiguous ") + what + " bins"};
+    edges.push_back(c);
+  }
+}
+
+#if !Y3B_MODULE_SHEAR
+// setup() of the fused form: the sel_function bins become the engine grid's
+// richness-fast product of contiguous lambda_obs and z_obs bins.
+void
+setup_fused(c_datablock* options, Module* m)
+{
+  Fused* f = m->fused = new Fused();
+  f->lam_min = bin_option(options, "lam_min");
+  f->lam_max = bin_option(options, "lam_max");
+  f->zob_min = bin_option(options, "zob_min");
+  f->zob_max = bin_option(options, "zob_max");
+  f->sigma_z = bin_option(options, "sigma_z");
+  const size_t nb = f->lam_min.size();
+  if (nb == 0 || f->lam_max.size() != nb || f->zob_min.size() != nb ||
+      f->zob_max.size() != nb || f->sigma_z.size() != nb)
+    throw Failure{"sel_function bin arrays must be non-empty and of one length"};
+  int nI = 1;
+  while ((size_t)nI < nb && f->zob_min[nI] == f->zob_min[0] && f->zob_max[nI] == f->zob_max[0])
+    ++nI;
+  if (nb % nI != 0) throw Failure{"engine = fused needs a richness-fast product of bins"};
+  const int nJ = (int)(nb / nI);
+  if (nI > 8 || nJ > 8) throw Failure{"engine = fused supports at most 8 x 8 bins"};
+  for (int j = 0; j < nJ; ++j)
+    for (int i = 0; i < nI; ++i) {
+      size_t b = (size_t)j * nI + i;
+      if (f->lam_min[b] != f->lam_min[i] || f->lam_max[b] != f->lam_max[i] ||
+          f->zob_min[b] != f->zob_min[(size_t)j * nI] ||
+          f->zob_max[b] != f->zob_max[(size_t)j * nI] ||
+          f->sigma_z[b] != f->sigma_z[(size_t)j * nI])
+        throw Failure{"engine = fused needs a richness-fast product of bins with one sigma_z "
+                      "per z_obs bin"};
+    }
+  std::vector<double> le, ze;
+  product_edges(f->lam_min, f->lam_max, 1, nI, le, "lambda_obs");
+  product_edges(f->zob_min, f->zob_max, nI, nJ, ze, "z_obs");
+  y3b_grid& g = f->grid;
+  g.n_m = opt_i(options, "n_lnm", 64);
+  g.n_z = opt_i(options, "n_z", 32);
+  g.n_t = opt_i(options, "n_lt", 64);
+  g.n_o = opt_i(options, "n_lo", 64);
+  g.n_zo = opt_i(options, "n_zo", 16);
+  g.lnm_lo = need_d(options, opt_section(options, "lnm_low"), "lnm_low");
+  g.lnm_hi = need_d(options, opt_section(options, "lnm_high"), "lnm_high");
+  g.zt_lo = need_d(options, opt_section(options, "zt_low"), "zt_low");
+  g.zt_hi = need_d(options, opt_section(options, "zt_high"), "zt_high");
+  g.lam_t_lo = opt_d(options, "lam_t_min", 1.0);
+  g.lam_t_hi = opt_d(options, "lam_t_max", 1000.0);
+  g.n_lam_bins = nI;
+  g.n_z_bins = nJ;
+  for (int i = 0; i <= nI; ++i) g.lam_edges[i] = le[i];
+  for (int j = 0; j <= nJ; ++j) g.zob_edges[j] = ze[j];
+  g.sz0 = opt_d(options, "sz0", 0.0);
+  for (int j = 0; j < nJ; ++j) g.sz_bin[j] = f->sigma_z[(size_t)j * nI];
+  const std::string prec = opt_string(options, "precision", "mixed");
+  if (prec == "mixed")
+    f->precision = Y3B_MIXED;
+  else if (prec == "fp64")
+    f->precision = Y3B_FP64;
+  else
+    throw Failure{"precision must be 'mixed' or 'fp64', got '" + prec + "'"};
+  for (int b : m->bins)
+    if (b < 0 || b >= (int)nb)
+      throw Failure{"NumCountsSelGL: bin_index outside sel_function/S_stack range"};
+  f->write_s = opt_bool(options, "write_s_stack", false);
+  if (f->write_s) {
+    y3b_selfunc_config& s = f->scfg;
+    auto sel_i = [&](const char* k, int d) {
+      int v;
+      return c_datablock_get_int(options, "sel_function", k, &v) == DBS_SUCCESS ? v : d;
+    };
+    s.n_bins = (int)nb;
+    s.zt_low = g.zt_lo;
+    s.zt_high = g.zt_hi;
+    s.lnm_low = g.lnm_lo;
+    s.lnm_high = g.lnm_hi;
+    s.n_lnm = sel_i("n_lnm", 40);  // sel_function.py:437-446 defaults
+    s.n_z = sel_i("n_z_shared", sel_i("n_z", 20));
+    s.n_q = sel_i("N_q", 32);
+  }
+}
+
+// execute() of the fused form for one parameter point.
+void
+execute_fused(c_datablock* block, Module* m, std::vector<double>& vals)
+{
+  Fused* f = m->fused;
+  const char* cp = "cosmological_parameters";
+  y3b_point pt{};
+  pt.cosmo.om = need_d(block, cp, "omega_m");
+  pt.cosmo.ol = need_d(block, cp, "omega_lambda");
+  pt.cosmo.ok = need_d(block, cp, "omega_k");
+  pt.cosmo.h0 = need_d(block, cp, "h0");
+  pt.cosmo.onu = need_d(block, cp, "omega_nu");
+  pt.cosmo.hmf_s = need_d(block, "cluster_abundance", "hmf_s");
+  pt.cosmo.hmf_q = need_d(block, "cluster_abundance", "hmf_q");
+  pt.A = need_d(block, "cluster_mor", "A");
+  pt.B = need_d(block, "cluster_mor", "B");
+  pt.C = need_d(block, "cluster_mor", "C");
+  pt.sigma = need_d(block, "cluster_mor", "sigma_intr");
+  pt.Mpiv = 3e14;
+  get_d(block, "cluster_mor", "M_pivot", &pt.Mpiv);
+  pt.grid = 0;
+  std::vector<double> mh = get_vec(block, "mass_function", "m_h");
+  std::vector<double> hz = get_vec(block, "mass_function", "z");
+  std::vector<int> ext;
+  std::vector<double> dn = get_nd(block, "mass_function", "dndlnmh", 2, ext);
+  if (ext[0] != (int)hz.size() || ext[1] != (int)mh.size())
+    throw Failure{"Interp2D -- ndarray wrong dimensions (mass_function/dndlnmh)"};
+  std::vector<double> dz = get_vec(block, "distances", "z");
+  std::vector<double> da = get_vec(block, "distances", "d_a");
+  if (dz.size() != da.size()) throw Failure{"distances/z and d_a differ in length"};
+  // P(lambda_obs | lambda_true, z): the sample's plob_ltr_params, else the
+  // frozen default table (sel_function.py:477-490).
+  std::vector<double> pz, pc;
+  if (c_datablock_has_value(block, "plob_ltr_params", "z")) {
+    pz = get_vec(block, "plob_ltr_params", "z");
+    for (const char* k : y3b::kPrjNames) {
+      std::vector<double> row = get_vec(block, "plob_ltr_params", k);
+      if (row.size() != pz.size()) throw Failure{"plob_ltr_params arrays differ in length"};
+      pc.insert(pc.end(), row.begin(), row.end());
+    }
+  } else {
+    pz.assign(y3b::kPrjZ, y3b::kPrjZ + y3b::kPrjNodes);
+    for (const auto& row : y3b::kPrjCoef) pc.insert(pc.end(), row, row + y3b::kPrjNodes);
+  }
+  if (!f->e || f->n_hm != (int)mh.size() || f->n_hz != (int)hz.size() ||
+      f->n_dist != (int)dz.size() || pz != f->plob_z || pc != f->plob_coef) {
+    y3b_engine_destroy(f->e);
+    f->e = nullptr;
+    y3b_engine_config ec{};
+    ec.n_hm = (int)mh.size();
+    ec.n_hz = (int)hz.size();
+    ec.n_dist = (int)dz.size();
+    ec.plob = y3b_plob{(int)pz.size(), pz.data(), pc.data()};
+    ec.max_points = 1;
+    int rc = y3b_engine_create(&f->grid, 1, &ec, &f->e);
+    if (rc != Y3B_OK) throw Failure{std::string("y3b_engine_create: ") + y3b_last_error()};
+    f->n_hm = ec.n_hm;
+    f->n_hz = ec.n_hz;
+    f->n_dist = ec.n_dist;
+    f->plob_z = pz;
+    f->plob_coef = pc;
+    f->packed.assign(y3b_engine_table_stride(f->e), 0.0);
+  }
+  size_t off[7];
+  y3b_engine_table_offsets(f->e, off);
+  std::copy(mh.begin(), mh.end(), f->packed.begin() + off[0]);
+  std::copy(hz.begin(), hz.end(), f->packed.begin() + off[1]);
+  std::copy(dn.begin(), dn.end(), f->packed.begin() + off[2]);
+  std::copy(dz.begin(), dz.end(), f->packed.begin() + off[3]);
+  std::copy(da.begin(), da.end(), f->packed.begin() + off[4]);
+  std::vector<double> counts(y3b_engine_n_bins(f->e));
+  int rc = y3b_engine_eval(f->e, f->precision, 1, &pt, f->packed.data(), counts.data(), nullptr);
+  if (rc != Y3B_OK) throw Failure{std::string("y3b_engine_eval: ") + y3b_last_error()};
+  vals.resize(m->bins.size());
+  for (size_t k = 0; k < m->bins.size(); ++k) vals[k] = counts[m->bins[k]];
+  if (f->write_s) {
+    const y3b_selfunc_config& s0 = f->scfg;
+    y3b_selfunc_config s = s0;
+    s.lam_min = f->lam_min.data();
+    s.lam_max = f->lam_max.data();
+    s.zob_min = f->zob_min.data();
+    s.zob_max = f->zob_max.data();
+    s.sigma_z = f->sigma_z.data();
+    y3b_mor mor{Y3B_MOR_LOGNORMAL,
+                {pt.A, pt.B, pt.C, pt.sigma, pt.Mpiv, f->grid.lam_t_lo, f->grid.lam_t_hi, 0.0}};
+    y3b_plob pl{(int)pz.size(), pz.data(), pc.data()};
+    std::vector<double> lnm(s.n_lnm), z(s.n_z), S((size_t)s.n_bins * s.n_z * s.n_lnm);
+    rc = y3b_sel_function(&s, &mor, &pl, lnm.data(), z.data(), S.data());
+    if (rc != Y3B_OK) throw Failure{std::string("y3b_sel_function: ") + y3b_last_error()};
+    const int e3[3] = {s.n_bins, s.n_z, s.n_lnm};
+    if (c_datablock_put_double_array_1d(block, "sel_function", "lnM", lnm.data(), s.n_lnm) !=
+            DBS_SUCCESS ||
+        c_datablock_put_double_array_1d(block, "sel_function", "z", z.data(), s.n_z) !=
+            DBS_SUCCESS ||
+        c_datablock_put_double_array(block, "sel_function", "S_stack", S.data(), 3, e3) !=
+            DBS_SUCCESS)
+      throw Failure{"cannot write sel_function/{lnM, z, S_stack}"};
+  }
+}
+#endif
+
 }  // namespace
 
 extern "C" void*
@@ -220,6 +476,17 @@ setup(c_datablock* options)
     cfg.lnm_high = need_d(options, opt_section(options, "lnm_high"), "lnm_high");
     m = new Module();
     m->bins = get_ivec(options, opt_section(options, "bin_index"), "bin_index");
+    const std::string eng = opt_string(options, "engine", "selgl");
+    if (eng != "selgl" && eng != "fused")
+      throw Failure{"engine must be 'selgl' or 'fused', got '" + eng + "'"};
+    if (eng == "fused") {
+#if Y3B_MODULE_SHEAR
+      throw Failure{"engine = fused is available for the number-count modules"};
+#else
+      setup_fused(options, m);
+      return m;
+#endif
+    }
 #if Y3B_MODULE_SHEAR
     m->r_perp = get_vec(options, opt_section(options, "r_perp"), "r_perp");
     const char* ls = opt_section(options, "lob_centers");
@@ -301,10 +568,18 @@ execute(c_datablock* block, void* module)
   try {
     Sample s;
 #if !Y3B_MODULE_SHEAR
+    std::vector<double> vals;
+    if (m->fused) {
+      execute_fused(block, m, vals);
+      if (c_datablock_put_double_array_1d(block, kOutput, "vals", vals.data(),
+                                          (int)vals.size()) != DBS_SUCCESS)
+        throw Failure{std::string("cannot write ") + kOutput + "/vals"};
+      return DBS_SUCCESS;
+    }
     read_sample(block, s, false);
     int rc = build(m, s, false);
     if (rc != Y3B_OK) throw Failure{y3b_last_error()};
-    std::vector<double> vals(m->bins.size());
+    vals.resize(m->bins.size());
     rc = y3b_selgl_counts(m->core, (int)m->bins.size(), m->bins.data(), vals.data());
     if (rc != Y3B_OK) throw Failure{y3b_last_error()};
 #else
