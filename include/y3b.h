@@ -49,7 +49,11 @@ typedef enum {
   Y3B_ERR_NOMEM = 4,       /* device allocation failed */
   Y3B_ERR_TIMEOUT = 5,     /* a bounded device-side wait ran out */
   Y3B_ERR_BUDGET = 6,      /* request exceeds the configured HBM budget */
-  Y3B_ERR_UNSUPPORTED = 7  /* shape the kernel does not support */
+  Y3B_ERR_UNSUPPORTED = 7, /* shape the kernel does not support */
+  Y3B_ERR_RANGE = 8,       /* mixed form: a point's Gaussian factors would leave the FP32
+                              exponent range (sigma_int too small for the factorisation);
+                              evaluate that point in Y3B_FP64 */
+  Y3B_ERR_CANCELLED = 9    /* the request was cancelled (y3b_server_cancel) */
 } y3b_status;
 
 /* Message of the last failure on the calling thread ("" if none). */
@@ -373,6 +377,9 @@ typedef struct {
   int pool_points, pool_free_points;
   int waiting;         /* submitted, not yet admitted to the pool */
   int unscheduled;     /* admitted, with points not yet in a launch */
+  long long requests_cancelled;
+  size_t device_bytes;      /* HBM the server holds: engine, launch buffers, table pool */
+  size_t pool_bytes_in_use; /* of which table-pool slots now holding a request's tables */
 } y3b_server_stats;
 
 typedef struct y3b_server y3b_server;
@@ -395,6 +402,14 @@ int y3b_server_submit(y3b_server* s, int n, const y3b_point* pts,
 int y3b_server_wait(y3b_server* s, long long ticket, double timeout_s,
                     double* latency_s);
 int y3b_server_stats_read(y3b_server* s, y3b_server_stats* out);
+/* Cancels a request: a request still waiting for admission leaves the queue,
+ * an admitted one gets no further points launched.  Points already on the
+ * device finish; the request completes once they are back, and
+ * y3b_server_wait then returns Y3B_ERR_CANCELLED (results not written).  Its
+ * host buffers must stay valid until that wait has returned.  Returns Y3B_OK,
+ * or Y3B_ERR_INVALID for an unknown ticket; a request that had already
+ * completed keeps its own status. */
+int y3b_server_cancel(y3b_server* s, long long ticket);
 /* Finishes every submitted request, then frees the server (not the engine). */
 void y3b_server_destroy(y3b_server* s);
 
@@ -416,6 +431,10 @@ int y3b_planner_next_batch(y3b_planner* p, long long* ids, int* first,
 /* count points of request id came back; *finished = 1 when it completed. */
 int y3b_planner_complete(y3b_planner* p, long long id, int count,
                          int* finished);
+/* Stops scheduling request id: *finished = 1 when none of its points is out
+ * (it left the planner, slots free), 0 when launched points must still
+ * complete. */
+int y3b_planner_cancel(y3b_planner* p, long long id, int* finished);
 int y3b_planner_free_points(const y3b_planner* p);
 
 #if defined(__GNUC__)

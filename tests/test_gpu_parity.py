@@ -381,3 +381,74 @@ def test_engine_chunked_host_eval_matches_one_launch(gpu, n):
     E.check(E.lib().y3b_engine_weights(eng.handle, n, E.A.ptr(W)))
     np.testing.assert_array_equal(W, r["W"])
     eng.close()
+
+
+@pytest.mark.parametrize("lam_t", [(15.0, 1000.0), (44.7, 1000.0), (1.0, 150.0)])
+def test_engine_window_with_mass_piled_at_a_domain_edge(gpu, lam_t):
+    """lam_t domains that cut into the MOR: with lam_t_lo = 44.7 the first lnM
+    tile's largest mu sits about 4 sigma below ln lam_t_lo (its cells keep
+    only a Gaussian tail, renormalised by a small in-range mass D), with 15
+    the low-mass cells sit far below it, and with lam_t_hi = 150 the
+    high-mass cells sit above ln lam_t_hi.  The contraction's stage window
+    must follow that renormalised density to the domain edge."""
+    g = synthetic.grid(4, lam_t_lo=lam_t[0], lam_t_hi=lam_t[1])
+    eng = _engine([g])
+    p = synthetic.fiducial()
+    pz, pc = synthetic.plob_baseline()
+    ref, _, _ = O.direct_eval(g, pz, pc, p.mor, O.cosmo(p.om, p.h0), p.tables)
+    r64 = eng.eval([p], E.FP64, grid_of=lambda _: 0)["counts"][0]
+    rmx = eng.eval([p], E.MIXED, grid_of=lambda _: 0)["counts"][0]
+    np.testing.assert_allclose(r64, ref, rtol=TOL64)
+    np.testing.assert_allclose(rmx, ref, rtol=TOLMIX)
+    eng.close()
+
+
+@pytest.mark.parametrize("case", [dict(sigma=0.05), dict(sigma=0.1), dict(C=2.0),
+                                  dict(sigma=0.05, C=2.0)])
+def test_mixed_form_exponent_range_guard(gpu, case):
+    """Outside the prior (sigma_int = 0.05, C = 2) the factorised Gaussian's
+    exponents grow as (alpha range)(beta range)/sigma^2.  The mixed form either
+    stays within 1e-4 of the FP64 oracle or reports Y3B_ERR_RANGE for the
+    point; it never returns a NaN or a silently wrong count, and the engine
+    stays usable."""
+    g = synthetic.grid(4)
+    eng = _engine([g])
+    p = synthetic.fiducial()
+    for k, v in case.items():
+        setattr(p, k, v)
+    pz, pc = synthetic.plob_baseline()
+    ref, _, _ = O.direct_eval(g, pz, pc, p.mor, O.cosmo(p.om, p.h0), p.tables)
+    r64 = eng.eval([p], E.FP64, grid_of=lambda _: 0)["counts"][0]
+    np.testing.assert_allclose(r64, ref, rtol=TOL64)
+    try:
+        rmx = eng.eval([p], E.MIXED, grid_of=lambda _: 0)["counts"][0]
+    except E.A.Y3BError as e:
+        assert e.status == E.A.ERR_RANGE
+        assert case.get("sigma", 0.2) <= 0.05        # only the narrowest scatter trips it
+    else:
+        assert np.all(np.isfinite(rmx))
+        np.testing.assert_allclose(rmx, ref, rtol=TOLMIX)
+    ok = eng.eval([synthetic.fiducial()], E.MIXED, grid_of=lambda _: 0)["counts"]
+    assert np.all(np.isfinite(ok)) and np.all(ok > 0)
+    eng.close()
+
+
+@pytest.mark.parametrize("where", ["dndlnmh", "dist_da", "hmf_m_h"])
+@pytest.mark.parametrize("bad", [np.nan, np.inf])
+def test_engine_rejects_non_finite_tables(gpu, where, bad):
+    """A NaN or Inf table entry (host-side injection) gives Y3B_ERR_DOMAIN in
+    both precisions instead of flowing into the counts."""
+    g = synthetic.grid(1)
+    eng = _engine([g], n_max=2)
+    p = synthetic.fiducial()
+    q = synthetic.Point(**{k: getattr(p, k) for k in ("om", "sigma8", "h0", "A", "B", "C",
+                                                       "sigma", "Mpiv", "density")})
+    q.tables = {k: np.array(v, copy=True) for k, v in p.tables.items()}
+    q.tables[where].flat[3] = bad
+    for prec in (E.FP64, E.MIXED):
+        with pytest.raises(E.A.Y3BError) as e:
+            eng.eval([p, q], prec, grid_of=lambda _: 0)
+        assert e.value.status == E.A.ERR_DOMAIN
+    ok = eng.eval([p], E.MIXED, grid_of=lambda _: 0)["counts"]
+    assert np.all(np.isfinite(ok)) and np.all(ok > 0)
+    eng.close()

@@ -119,3 +119,40 @@ def test_submit_checks_tables_and_points(gpu):
         r = srv.wait(srv.submit(pts, tab))                # the server still works
         assert np.all(np.isfinite(r["counts"]))
     eng.close()
+
+
+def test_cancel_and_memory_stats(gpu):
+    """Cancellation through the server (host-side injection): a request
+    cancelled while it waits behind a full pool completes with CANCELLED and
+    writes nothing; the others finish unchanged; the stats report the HBM the
+    server holds and every pool slot comes back.  (Whether the request is
+    still waiting when cancel() arrives depends on timing: eight launches are
+    queued ahead of it, and the scenario is repeated until a cancel lands.)"""
+    eng = _engine(max_points=16)
+    sizes = [16, 16, 12, 4]
+    reqs = _requests(eng, sizes, seed=25)
+    ref = _direct(eng, reqs, E.MIXED)
+    cancelled = 0
+    with serve.Server(eng, pool_points=32, max_batch=4, max_inflight=1) as srv:
+        for _ in range(3):
+            tickets = [srv.submit(p, t) for p, t in reqs]
+            srv.cancel(tickets[2])
+            try:
+                r2 = srv.wait(tickets[2])
+            except A.Y3BError as e:
+                assert e.status == A.ERR_CANCELLED
+                cancelled += 1
+            else:                                # it had finished first: untouched
+                assert _close(r2["counts"], ref[2][0])
+            for i in (0, 1, 3):
+                assert _close(srv.wait(tickets[i])["counts"], ref[i][0])
+            if cancelled:
+                break
+        st = srv.stats()
+        with pytest.raises(A.Y3BError) as e:
+            srv.cancel(tickets[0])              # already collected
+        assert e.value.status == A.ERR_INVALID
+    assert cancelled == 1 and st["requests_cancelled"] == 1
+    assert st["device_bytes"] >= eng.device_bytes() + 32 * eng.stride * 8
+    assert st["pool_bytes_in_use"] == 0 and st["pool_free_points"] == 32
+    eng.close()

@@ -41,6 +41,11 @@ class Planner:
         A.check(self.L.y3b_planner_complete(self.h, rid, count, C.byref(f)))
         return f.value
 
+    def cancel(self, rid):
+        f = C.c_int()
+        A.check(self.L.y3b_planner_cancel(self.h, rid, C.byref(f)))
+        return f.value
+
     def free(self):
         return self.L.y3b_planner_free_points(self.h)
 
@@ -136,4 +141,37 @@ def test_random_stream_conserves_slots():
             break
     assert len(done) == 200
     assert p.free() == pool
+    p.close()
+
+
+def test_cancel_waiting_admitted_and_inflight_requests():
+    """Cancellation (host-side injection, no device): a waiting request leaves
+    the queue; an admitted one gets nothing more scheduled and frees its slots
+    once its launched points are back; others are unaffected."""
+    p = Planner(pool=64, max_batch=16)
+    for rid, n in ((1, 40), (2, 40), (3, 8)):
+        assert p.submit(rid, n) == 0
+    assert p.admit() == [(1, 0)]
+    assert p.cancel(2) == 1                  # waiting: gone at once
+    assert p.admit() == [(3, 40)]            # 3 no longer blocked behind 2
+    chunks, n = p.batch()
+    assert chunks == [(1, 0, 16, 0)]
+    assert p.cancel(1) == 0                  # 16 points still out
+    chunks, n = p.batch()
+    assert chunks == [(3, 0, 8, 40)] and n == 8   # nothing more of 1
+    assert p.free() == 16
+    assert p.complete(1, 16) == 1            # its slots return now
+    assert p.free() == 56
+    assert p.complete(3, 8) == 1 and p.free() == 64
+    with pytest.raises(A.Y3BError):
+        p.cancel(7)
+    p.close()
+
+
+def test_cancel_before_any_launch_frees_slots_immediately():
+    p = Planner(pool=32, max_batch=8)
+    assert p.submit(1, 20) == 0
+    assert p.admit() == [(1, 0)]
+    assert p.cancel(1) == 1 and p.free() == 32
+    assert p.batch() == ([], 0)
     p.close()

@@ -23,7 +23,8 @@ VP = C.c_void_p
 
 Y3B_OK = 0
 STATUS_NAMES = {0: "OK", 1: "INVALID", 2: "DOMAIN", 3: "CUDA", 4: "NOMEM", 5: "TIMEOUT",
-                6: "BUDGET", 7: "UNSUPPORTED"}
+                6: "BUDGET", 7: "UNSUPPORTED", 8: "RANGE", 9: "CANCELLED"}
+ERR_INVALID, ERR_DOMAIN, ERR_RANGE, ERR_CANCELLED = 1, 2, 8, 9
 FP64 = 0
 MIXED = 1
 MOR_HOD = 0
@@ -109,7 +110,9 @@ class ServerConfig(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [("requests_done", C.c_longlong), ("points_done", C.c_longlong),
                 ("launches", C.c_longlong), ("max_launch_points", I), ("pool_points", I),
-                ("pool_free_points", I), ("waiting", I), ("unscheduled", I)]
+                ("pool_free_points", I), ("waiting", I), ("unscheduled", I),
+                ("requests_cancelled", C.c_longlong), ("device_bytes", C.c_size_t),
+                ("pool_bytes_in_use", C.c_size_t)]
 
 
 _lib = None
@@ -173,6 +176,7 @@ def _declare(L):
     L.y3b_server_submit.argtypes = [VP, I, VP, VP, VP, VP, C.POINTER(C.c_longlong)]
     L.y3b_server_wait.argtypes = [VP, C.c_longlong, D, PD]
     L.y3b_server_stats_read.argtypes = [VP, C.POINTER(ServerStats)]
+    L.y3b_server_cancel.argtypes = [VP, C.c_longlong]
     L.y3b_server_destroy.argtypes = [VP]
     L.y3b_server_destroy.restype = None
     PLL = C.POINTER(C.c_longlong)
@@ -183,6 +187,7 @@ def _declare(L):
     L.y3b_planner_admit.argtypes = [VP, PLL, PI, I, PI]
     L.y3b_planner_next_batch.argtypes = [VP, PLL, PI, PI, PI, I, PI, PI]
     L.y3b_planner_complete.argtypes = [VP, C.c_longlong, I, PI]
+    L.y3b_planner_cancel.argtypes = [VP, C.c_longlong, PI]
     L.y3b_planner_free_points.argtypes = [VP]
     L.y3b_engine_profile.argtypes = [VP, I]
     L.y3b_engine_profile_read.argtypes = [VP, PD, PI]
@@ -218,7 +223,8 @@ EXPORTED = [
     "y3b_engine_profile", "y3b_engine_profile_read", "y3b_sel_function_noalloc",
     "y3b_engine_eval_pooled", "y3b_engine_set_graphs", "y3b_engine_autotune",
     "y3b_engine_tuning", "y3b_engine_stage_count", "y3b_server_create", "y3b_server_submit", "y3b_server_wait",
-    "y3b_server_stats_read", "y3b_server_destroy", "y3b_planner_create",
+    "y3b_server_stats_read", "y3b_server_cancel", "y3b_server_destroy", "y3b_planner_create",
     "y3b_planner_destroy", "y3b_planner_submit", "y3b_planner_admit",
-    "y3b_planner_next_batch", "y3b_planner_complete", "y3b_planner_free_points",
+    "y3b_planner_next_batch", "y3b_planner_complete", "y3b_planner_cancel",
+    "y3b_planner_free_points",
 ]

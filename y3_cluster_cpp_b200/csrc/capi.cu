@@ -58,16 +58,30 @@ read_device_status(int* d_status, cudaStream_t s)
   int h = 0;
   Y3B_CUDA(cudaMemcpyAsync(&h, d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
   Y3B_CUDA(cudaStreamSynchronize(s));
-  switch (h) {
+  return device_status_rc(h);
+}
+
+int
+device_status_rc(int code)
+{
+  switch (code) {
     case kDevOk: return Y3B_OK;
     case kDevDomain:
-      set_error("argument out of range in Interp1D (a node lies outside an unclamped table)");
+      set_error("argument out of range in Interp1D (a z node lies outside distances/z or "
+                "another unclamped table)");
       return Y3B_ERR_DOMAIN;
     case kDevTimeout:
       set_error("a bounded device-side wait ran out");
       return Y3B_ERR_TIMEOUT;
+    case kDevNonFinite:
+      set_error("a table entry is not finite (NaN or Inf)");
+      return Y3B_ERR_DOMAIN;
+    case kDevRange:
+      set_error("mixed form: a point's Gaussian factors would leave the FP32 exponent range "
+                "(sigma_int too small for the factorisation); evaluate it in FP64");
+      return Y3B_ERR_RANGE;
     default:
-      set_error("device-side shape check failed (code %d)", h);
+      set_error("device-side shape check failed (code %d)", code);
       return Y3B_ERR_INVALID;
   }
 }

@@ -31,6 +31,8 @@ enum DevErr : int {
   kDevDomain = 1,   // a query outside an unclamped table (d_a, n(z))
   kDevTimeout = 2,  // a bounded wait ran out
   kDevShape = 3,    // launch shape / size mismatch detected on device
+  kDevNonFinite = 4,  // a table entry is NaN or infinite
+  kDevRange = 5,      // mixed form: a factor's exponent is outside the safe FP32 range
 };
 
 __device__ __forceinline__ void

@@ -158,6 +158,10 @@ prep_smem_bytes(const TableLayout& L, int n_hz, int n_hm, int n_m, int n_z, int 
   return b + 64;
 }
 
+// Largest |log2| of a factor of the mixed form's Gaussian (G and H) that the
+// prep kernel admits; FP32 and BF16 hold 2^-126 .. 2^127.
+constexpr double kMaxExp2 = 100.0;
+
 __global__ void __launch_bounds__(256, 4)
 prep_kernel(PrepArgs a)
 {
@@ -189,6 +193,7 @@ prep_kernel(PrepArgs a)
   int* q_y = k_x + n_m;
   __shared__ __align__(8) uint64_t bar;
   __shared__ int timed_out;
+  int bad = 0;  // a non-finite table entry seen by this thread
   __shared__ double red[6];
   __shared__ int swin[16];  // lam_t stage window per lnM tile (n_m <= 1024)
 
@@ -233,6 +238,7 @@ prep_kernel(PrepArgs a)
       for (int u = 0; u < 4; ++u) {
         const int i = i0 + u * blockDim.x;
         if (i < nn) h32[i] = (float)v[u];
+        bad |= !isfinite(v[u]);
       }
     }
   }
@@ -256,6 +262,24 @@ prep_kernel(PrepArgs a)
   if (timed_out) {  // uniform exit; the copy only targets this CTA's shared memory
     if (tid == 0) set_err(a.status, kDevTimeout);
     return;
+  }
+  // Every table entry must be finite: the staged sections (not their
+  // alignment padding) and, for the FP64 form, the HMF grid in global memory
+  // (the mixed form checked it while converting).
+  {
+    const int len[7] = {n_hm, n_hz, 0, L.n_dist, L.n_dist, L.n_sci, L.n_sci};
+    for (int sct = 0; sct < 7; ++sct) {
+      const double* base = sct < 2 ? tab + L.off[sct] : tab + head + (L.off[sct] - L.off[3]);
+      for (int i = tid; i < len[sct]; i += blockDim.x) bad |= !isfinite(base[i]);
+    }
+    if (!a.mixed) {
+      const double* __restrict__ dng = src + L.off[2];
+      for (int i = tid; i < n_hz * n_hm; i += blockDim.x) bad |= !isfinite(__ldg(dng + i));
+    }
+    if (__syncthreads_or(bad)) {
+      if (tid == 0) set_err(a.status, kDevNonFinite);
+      return;
+    }
   }
   double* mh = tab + L.off[0];
   const double* hz = tab + L.off[1];
@@ -477,11 +501,17 @@ prep_kernel(PrepArgs a)
     (reinterpret_cast<uintptr_t>(dtab + 2 * kDTab) + 15) & ~uintptr_t(15));  // [n_t_pad]
   for (int t = tid; t < n_t_pad; t += blockDim.x) dt_f[t] = t < n_t ? (float)(Gp->xl[t] - L0) : 0.f;
   __syncthreads();
-  // lam_t window of the contraction per lnM tile: for every (k, q) of the
-  // tile the MOR density exp(-(l_t - mu_kq)^2 / 2 s^2) is below 4e-6 of its
-  // peak outside [min mu - 5 s, max mu + 5 s] (the Gaussian mass beyond is
-  // 3e-7 on each side), so those stages add less than the rounding of the
-  // split-BF16 products; the stage count is rounded up to pairs.
+  // lam_t window of the contraction per lnM tile.  Each (k, q) cell's
+  // density exp(-(l - mu)^2 / 2 s^2) / D is renormalised to the lam_t domain
+  // [ll_lo, ll_hi], where it peaks at c = clamp(mu, ll_lo, ll_hi); it is below
+  // 4e-6 of that peak outside mu -+ R(mu), R = sqrt((c - mu)^2 + (5 s)^2).
+  // For mu inside the domain that is mu -+ 5 s (Gaussian mass 3e-7 per side);
+  // for mu below ll_lo (above ll_hi) the window reaches from the domain edge
+  // to where the renormalised density has fallen by the same factor, so cells
+  // whose in-range mass D is small keep all of it.  mu -+ R(mu) increase with
+  // mu, so the tile's window runs from the lower end for its smallest mu to
+  // the upper end for its largest; stages outside add less than the rounding
+  // of the split-BF16 products.  The stage count is rounded up to pairs.
   {
     constexpr double kWin = 5.0;
     const int n_mt = n_m_pad / kGemmRows, nk = n_t_pad / 16;
@@ -498,8 +528,12 @@ prep_kernel(PrepArgs a)
       if (lane == 0) {
         int lo = 0, hi = nk;
         if (amx >= amn) {
-          const float dlo = (float)(amn + red[4] - kWin * sig - L0);
-          const float dhi = (float)(amx + red[5] + kWin * sig - L0);
+          const double mu_lo = amn + red[4], mu_hi = amx + red[5];
+          const double e_lo = fmin(fmax(mu_lo, ll_lo), ll_hi) - mu_lo;
+          const double e_hi = fmin(fmax(mu_hi, ll_lo), ll_hi) - mu_hi;
+          const double w2 = (kWin * sig) * (kWin * sig);
+          const float dlo = (float)(mu_lo - sqrt(e_lo * e_lo + w2) - L0);
+          const float dhi = (float)(mu_hi + sqrt(e_hi * e_hi + w2) - L0);
           int a = 0, b = n_t;  // first t with delta_t >= dlo (nodes ascend)
           while (a < b) {
             const int m = (a + b) >> 1;
@@ -526,6 +560,23 @@ prep_kernel(PrepArgs a)
     }
   }
   __syncthreads();
+  // Exponent range of the factorised form: G = 2^(delta b c2) over the
+  // issued stages and H = 2^(-(a b + b^2/2) c2) must stay well inside FP32 /
+  // BF16 (2^-126 .. 2^127).  |a| <= (max alpha - min alpha) / 2 and
+  // |b| <= (max beta - min beta) / 2 after centring, so the bound below holds
+  // for every factor; a point beyond it reports kDevRange (its FP64 form is
+  // unaffected).
+  if (tid == 0) {
+    double dmax = 0.0;
+    for (int mt = 0; mt < n_m_pad / kGemmRows; ++mt) {
+      const int t0 = swin[2 * mt] * 16, t1 = min(swin[2 * mt + 1] * 16, n_t) - 1;
+      if (t1 >= t0) dmax = fmax(dmax, fmax(fabs((double)dt_f[t0]), fabs((double)dt_f[t1])));
+    }
+    const double bmax = 0.5 * (red[5] - red[4]);
+    const double amax = 0.5 * ((red[3] - red[2]) - (red[5] - red[4]));
+    const double e = 1.4426950408889634 / (sig * sig) * bmax * fmax(dmax, amax + 0.5 * bmax);
+    if (!(e <= kMaxExp2)) set_err(a.status, kDevRange);
+  }
   // The window of each contraction tile (lnM tile, richness-bin group).
   for (int l = tid; l < Gp->tiles_pp; l += blockDim.x) {
     const int mt = l / Gp->n_bg;
@@ -1659,10 +1710,7 @@ y3b_engine_sync(y3b_engine* e, void* stream)
   clear_error();
   if (!e) return Y3B_ERR_INVALID;
   cudaStream_t s = stream ? (cudaStream_t)stream : e->stream;
-  int rc = read_device_status(e->status.get(), s);
-  if (rc == Y3B_ERR_DOMAIN) set_error("y3b engine: a z_t node lies outside distances/z");
-  if (rc == Y3B_ERR_TIMEOUT) set_error("y3b engine: a bounded device wait ran out");
-  return rc;
+  return read_device_status(e->status.get(), s);
 }
 
 extern "C" int
@@ -1737,17 +1785,7 @@ y3b_engine_eval(y3b_engine* e, int precision, int n, const y3b_point* pts,
   e->last_n = n;
   for (int c = 0; c < used; ++c) {
     const int h = e->chunk_status[c];
-    if (h == y3b::kDevOk) continue;
-    if (h == y3b::kDevDomain) {
-      set_error("y3b engine: a z_t node lies outside distances/z");
-      return Y3B_ERR_DOMAIN;
-    }
-    if (h == y3b::kDevTimeout) {
-      set_error("y3b engine: a bounded device wait ran out");
-      return Y3B_ERR_TIMEOUT;
-    }
-    set_error("y3b engine: device-side check failed (code %d)", h);
-    return Y3B_ERR_INVALID;
+    if (h != y3b::kDevOk) return y3b::device_status_rc(h);
   }
   return Y3B_OK;
 }

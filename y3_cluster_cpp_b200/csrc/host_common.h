@@ -88,5 +88,8 @@ class DevBuf {
 
 // Device status word for kernel-side checks (domain errors, timeouts).
 int read_device_status(int* d_status, cudaStream_t s);
+// Maps a device-side error code (DevErr) to a y3b_status and leaves its
+// message for y3b_last_error().
+int device_status_rc(int code);
 
 }  // namespace y3b

@@ -13,7 +13,10 @@
 //     not fit (continuous batching: requests admitted while a launch runs join
 //     the next one);
 //   * release: when every point of a request has come back, its run of slots
-//     returns to the pool (neighbouring free runs are merged).
+//     returns to the pool (neighbouring free runs are merged);
+//   * cancellation: a cancelled request leaves the queue, or, once admitted,
+//     gets no further points scheduled; its slots return when the points
+//     already launched have come back.
 #pragma once
 
 #include <algorithm>
@@ -87,7 +90,7 @@ class Planner {
   int submit(long long id, int n)
   {
     if (n < 1 || n > pool_.capacity() || reqs_.count(id)) return 1;
-    reqs_[id] = Req{n, -1, 0, 0};
+    reqs_[id] = Req{n, -1, 0, 0, false};
     waiting_.push_back(id);
     return 0;
   }
@@ -137,7 +140,29 @@ class Planner {
     Req& r = it->second;
     if (r.slot0 < 0 || count < 0 || r.done + count > r.next) return -1;
     r.done += count;
-    if (r.done < r.n) return 0;
+    if (r.done < (r.cancelled ? r.next : r.n)) return 0;
+    pool_.release(r.slot0, r.n);
+    reqs_.erase(it);
+    return 1;
+  }
+
+  // Stops scheduling request `id`.  Returns 1 when nothing of it is out any
+  // more (it has left the planner and its slots are free), 0 when launched
+  // points must still come back through complete(), -1 for an unknown id.
+  int cancel(long long id)
+  {
+    auto it = reqs_.find(id);
+    if (it == reqs_.end()) return -1;
+    Req& r = it->second;
+    if (r.slot0 < 0) {  // still waiting for admission
+      waiting_.erase(std::find(waiting_.begin(), waiting_.end(), id));
+      reqs_.erase(it);
+      return 1;
+    }
+    auto a = std::find(active_.begin(), active_.end(), id);
+    if (a != active_.end()) active_.erase(a);
+    r.cancelled = true;
+    if (r.done < r.next) return 0;
     pool_.release(r.slot0, r.n);
     reqs_.erase(it);
     return 1;
@@ -152,6 +177,7 @@ class Planner {
  private:
   struct Req {
     int n, slot0, next, done;
+    bool cancelled;
   };
   SlotPool pool_;
   int max_batch_;

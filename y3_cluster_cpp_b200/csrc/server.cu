@@ -30,6 +30,8 @@
 #include <unordered_map>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "engine_internal.h"
 #include "host_common.h"
 #include "planner.h"
@@ -56,7 +58,9 @@ struct Request {
   int status = Y3B_OK;
   std::string message;
   bool done = false;
+  bool cancelled = false;
   cudaEvent_t copied = nullptr;  // tables are in the pool once this fires
+  nvtxRangeId_t range = 0;       // NVTX range from submission to completion
 };
 
 struct Launch {
@@ -93,6 +97,7 @@ struct y3b_server {
   bool stop = false;
   std::thread worker;
   y3b_server_stats st{};
+  size_t fixed_bytes = 0;  // engine + launch buffers
   ~y3b_server()
   {
     for (auto& Lp : launches) {
@@ -141,6 +146,22 @@ enqueue_launch(y3b_server* S, Launch& L, const std::vector<cudaEvent_t>& waits)
   return Y3B_OK;
 }
 
+// A request whose points are all back (or that was cancelled with none out):
+// complete it (lock held).
+void
+mark_done(y3b_server* S, Request& r, double t)
+{
+  r.done = true;
+  r.t_done = t;
+  if (r.copied) cudaEventDestroy(r.copied);
+  r.copied = nullptr;
+  nvtxRangeEnd(r.range);
+  if (r.cancelled)
+    ++S->st.requests_cancelled;
+  else
+    ++S->st.requests_done;
+}
+
 // Scatters a finished launch into its requests (lock held).
 void
 finish_launch(y3b_server* S, Launch& L, int status, const char* msg)
@@ -150,7 +171,7 @@ finish_launch(y3b_server* S, Launch& L, int status, const char* msg)
   const double t = now_s();
   for (const PlanChunk& c : L.chunks) {
     Request& r = S->reqs[c.id];
-    if (status == Y3B_OK) {
+    if (status == Y3B_OK && r.status == Y3B_OK) {
       std::memcpy(r.counts + (size_t)c.first * nB, L.h_counts + (size_t)k * nB,
                   (size_t)c.count * nB * sizeof(double));
       if (r.shear && S->cfg.with_shear)
@@ -161,13 +182,7 @@ finish_launch(y3b_server* S, Launch& L, int status, const char* msg)
       r.message = msg ? msg : "";
     }
     k += c.count;
-    if (S->planner->complete(c.id, c.count) == 1) {
-      r.done = true;
-      r.t_done = t;
-      if (r.copied) cudaEventDestroy(r.copied);
-      r.copied = nullptr;
-      ++S->st.requests_done;
-    }
+    if (S->planner->complete(c.id, c.count) == 1) mark_done(S, r, t);
   }
   S->st.points_done += L.n;
   ++S->st.launches;
@@ -175,15 +190,6 @@ finish_launch(y3b_server* S, Launch& L, int status, const char* msg)
   S->cv_done.notify_all();
 }
 
-const char*
-status_message(int st)
-{
-  switch (st) {
-    case Y3B_ERR_DOMAIN: return "a z_t node lies outside distances/z";
-    case Y3B_ERR_TIMEOUT: return "a bounded device wait ran out";
-    default: return "device-side check failed";
-  }
-}
 
 void
 worker_main(y3b_server* S)
@@ -211,8 +217,12 @@ worker_main(y3b_server* S)
       lk.lock();
       r.copied = ev;
       if (ce != cudaSuccess) {
+        // Nothing of the request may be launched from its unfilled slots:
+        // it leaves the planner (nothing of it was scheduled yet) with the
+        // upload error as its status.
         r.status = Y3B_ERR_CUDA;
         r.message = std::string("table upload: ") + cudaGetErrorString(ce);
+        if (S->planner->cancel(a.first) == 1) mark_done(S, r, now_s());
       }
       progressed = true;
     }
@@ -254,13 +264,14 @@ worker_main(y3b_server* S)
       Launch& L = *S->launches[b];
       const cudaError_t q = cudaEventQuery(L.done);
       if (q == cudaSuccess || q != cudaErrorNotReady) {
-        int status = *L.h_status;
+        int status = Y3B_OK;
         std::string msg;
         if (q != cudaSuccess) {
           status = Y3B_ERR_CUDA;
           msg = std::string("launch: ") + cudaGetErrorString(q);
-        } else if (status != Y3B_OK) {
-          msg = status_message(status);
+        } else if (*L.h_status != 0) {  // a device-side error code (0 = ok)
+          status = y3b::device_status_rc(*L.h_status);  // device code -> y3b_status
+          msg = y3b_last_error();
         }
         finish_launch(S, L, status, msg.c_str());
         S->inflight.pop_front();
@@ -373,6 +384,7 @@ y3b_server_create(y3b_engine* e, const y3b_server_config* cfg_in, y3b_server** o
     S->free_launch.push_back(i);
   }
   S->st.pool_points = cfg.pool_points;
+  S->fixed_bytes = fixed;
   S->worker = std::thread(worker_main, S);
   *out = S;
   return Y3B_OK;
@@ -412,6 +424,9 @@ y3b_server_submit(y3b_server* S, int n, const y3b_point* pts, const double* tabl
   r.counts = counts;
   r.shear = S->cfg.with_shear ? shear : nullptr;
   r.t_submit = t0;
+  char label[64];
+  std::snprintf(label, sizeof label, "y3b request %lld (%d points)", id, n);
+  r.range = nvtxRangeStartA(label);
   S->reqs.emplace(id, std::move(r));
   *ticket = id;
   S->cv_work.notify_one();
@@ -462,6 +477,36 @@ y3b_server_stats_read(y3b_server* S, y3b_server_stats* out)
   out->pool_free_points = S->planner->free_slots();
   out->waiting = S->planner->waiting();
   out->unscheduled = S->planner->unscheduled();
+  const size_t slot_bytes = S->info.stride * sizeof(double);
+  out->device_bytes = S->fixed_bytes + (size_t)S->cfg.pool_points * slot_bytes;
+  out->pool_bytes_in_use = (size_t)(S->cfg.pool_points - out->pool_free_points) * slot_bytes;
+  return Y3B_OK;
+}
+
+extern "C" int
+y3b_server_cancel(y3b_server* S, long long ticket)
+{
+  y3b::clear_error();
+  if (!S) return Y3B_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(S->m);
+  auto it = S->reqs.find(ticket);
+  if (it == S->reqs.end()) {
+    y3b::set_error("y3b_server_cancel: unknown ticket %lld (never issued or already collected)",
+                   ticket);
+    return Y3B_ERR_INVALID;
+  }
+  Request& r = it->second;
+  if (r.done || r.cancelled) return Y3B_OK;
+  r.cancelled = true;
+  if (r.status == Y3B_OK) {
+    r.status = Y3B_ERR_CANCELLED;
+    r.message = "request cancelled";
+  }
+  if (S->planner->cancel(ticket) == 1) {
+    mark_done(S, r, now_s());
+    S->cv_done.notify_all();
+  }
+  S->cv_work.notify_one();
   return Y3B_OK;
 }
 
@@ -564,6 +609,20 @@ y3b_planner_complete(y3b_planner* p, long long id, int count, int* finished)
   const int r = p->p.complete(id, count);
   if (r < 0) {
     y3b::set_error("y3b_planner_complete: request %lld has fewer than %d points out", id, count);
+    return Y3B_ERR_INVALID;
+  }
+  *finished = r;
+  return Y3B_OK;
+}
+
+extern "C" int
+y3b_planner_cancel(y3b_planner* p, long long id, int* finished)
+{
+  y3b::clear_error();
+  if (!p || !finished) return Y3B_ERR_INVALID;
+  const int r = p->p.cancel(id);
+  if (r < 0) {
+    y3b::set_error("y3b_planner_cancel: unknown request %lld", id);
     return Y3B_ERR_INVALID;
   }
   *finished = r;

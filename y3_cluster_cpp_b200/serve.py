@@ -86,6 +86,12 @@ class Server:
             out["shear"] = shear
         return out
 
+    def cancel(self, ticket):
+        """Stops launching the request's points; its wait() then raises
+        Y3BError with status CANCELLED once the points already on the device
+        are back (their results are not written)."""
+        check(lib().y3b_server_cancel(self._h, ticket))
+
     def stats(self):
         s = A.ServerStats()
         check(lib().y3b_server_stats_read(self._h, C.byref(s)))
