@@ -20,7 +20,6 @@ import argparse
 import ctypes as C
 import json
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -46,7 +45,10 @@ def parse():
     ap.add_argument("--unique", type=int, default=256, help="distinct walker tables per batch")
     ap.add_argument("--density", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample", type=int, default=2, help="points in the CPU baseline sample")
+    ap.add_argument("--cpu-sample", type=int, default=8,
+                    help="points in the CPU baseline sample (reference chain)")
+    ap.add_argument("--cpu-port-sample", type=int, default=2,
+                    help="points of the FP64 direct-quadrature port timed beside it")
     ap.add_argument("--no-extra-workloads", dest="extra_workloads", action="store_false",
                     help="skip the batched-uneven and DeltaSigma measurements")
     ap.add_argument("--serve-requests", type=int, default=256,
@@ -164,41 +166,117 @@ class ClockSampler:
                 "samples": len(rows), "source": "nvidia-smi, 100 ms"}
 
 
-def cpu_baseline(density, n_points):
-    """The FP64 oracle (a port of the reference algorithm) on the host, one
-    thread, on a bounded sample of the same workload."""
-    import numpy as np  # noqa: F401
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# The reference's production resolution for this path: sel_function.py on the
+# des_y3.ini grid (192 lnM x 64 z x 32 lam_t nodes per cell), then
+# NumCountsSelGL with its defaults (96 lnM x 64 z GL nodes).
+REF_SEL_GRID = dict(n_lnm=192, n_z=64, n_q=32)
+
+
+def _ref_chain_setup():
+    import numpy as np
 
     import oracle
+    from oracle import ref as R
     from y3_cluster_cpp_b200 import synthetic
-    g = synthetic.grid(density)
-    pz, pc = synthetic.plob_baseline()
-    pts = synthetic.walkers(n_points, seed=11, densities=(density,), with_sci=False)
+    g = synthetic.grid(1)
+    le, ze = g["lam_edges"], g["zob_edges"]
+    cfg = dict(lam_min=np.tile(le[:-1], 3), lam_max=np.tile(le[1:], 3),
+               zob_min=np.repeat(ze[:-1], 4), zob_max=np.repeat(ze[1:], 4),
+               sigma_z=np.full(12, 0.0145), zt_low=g["zt_lo"], zt_high=g["zt_hi"],
+               lnm_low=g["lnm_lo"], lnm_high=g["lnm_hi"], **REF_SEL_GRID)
+    selgl = dict(zt_low=g["zt_lo"], zt_high=g["zt_hi"], lnm_low=g["lnm_lo"],
+                 lnm_high=g["lnm_hi"])
     oracle.lib()
-    t0 = time.perf_counter()
-    for p in pts:
-        oracle.direct_eval(g, pz, pc, p.mor, oracle.cosmo(p.om, p.h0), p.tables)
-    dt = time.perf_counter() - t0
-    return {"value": n_points / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"{n_points} points at {density}x nodes, FP64 oracle (C), 1 thread, "
-                      f"{dt:.1f} s"}
+    return cfg, selgl, R.available()
 
 
-def _ref_worker(args):
-    density, seed = args
+def _ref_chain_point(p, cfg, selgl, have_ref):
+    """One parameter point through the reference chain: the S_stack
+    tabulation of sel_function.py (its C restatement, pinned to the
+    reference's Python at 1e-13; Python cannot run on the GPU host) and
+    NumCountsSelGL, the reference's own C++ compiled from its sources (the
+    oracle's bit-identical restatement where that build is absent)."""
     import oracle
+    from oracle import ref as R
     from y3_cluster_cpp_b200 import synthetic
-    g = synthetic.grid(density)
     pz, pc = synthetic.plob_baseline()
-    p = synthetic.walkers(1, seed=seed, densities=(density,), with_sci=False)[0]
-    oracle.direct_eval(g, pz, pc, p.mor, oracle.cosmo(p.om, p.h0), p.tables)
+    mor = [p.A, p.B, p.C, p.sigma, p.Mpiv, 1.0, 1000.0]
+    sel = oracle.sel_function(cfg, oracle.MOR_LOGNORMAL, mor, pz, pc)
+    if have_ref:
+        cosmo = dict(omega_m=p.om, omega_nu=0.0, omega_lambda=1.0 - p.om, omega_k=0.0,
+                     h0=p.h0, hmf_s=0.0, hmf_q=1.0)
+        return R.numcounts(selgl, cosmo, p.tables, sel)
+    return oracle.selgl_weights(96, 64, selgl["zt_low"], selgl["zt_high"], selgl["lnm_low"],
+                                selgl["lnm_high"], oracle.cosmo(p.om, p.h0), p.tables, sel)[1]
+
+
+def _ref_worker(seed):
+    from y3_cluster_cpp_b200 import synthetic
+    cfg, selgl, have_ref = _ref_chain_setup()
+    p = synthetic.walkers(1, seed=seed, densities=(1,), with_sci=False)[0]
+    _ref_chain_point(p, cfg, selgl, have_ref)
     return 1
 
 
+def _ref_kind(have_ref):
+    return "reference" if have_ref else "port"
+
+
+def _ref_sample(have_ref):
+    what = ("NumCountsSelGL: the reference's C++ compiled from its sources"
+            if have_ref else "NumCountsSelGL: the oracle's restatement")
+    return (f"reference chain per point: sel_function S_stack at "
+            f"{REF_SEL_GRID['n_lnm']} lnM x {REF_SEL_GRID['n_z']} z x {REF_SEL_GRID['n_q']} "
+            f"lam_t (C restatement of sel_function.py, pinned to it at 1e-13), then {what} "
+            f"(96 lnM x 64 z); walkers' own tables")
+
+
+def cpu_baseline(n_points, density, n_port):
+    """The reference chain on the host, one thread, on a bounded sample of
+    walkers; beside it the FP64 direct quadrature (the oracle port) at the
+    bench's node density."""
+    from y3_cluster_cpp_b200 import synthetic
+    cfg, selgl, have_ref = _ref_chain_setup()
+    pts = synthetic.walkers(n_points, seed=11, densities=(1,), with_sci=False)
+    _ref_chain_point(pts[0], cfg, selgl, have_ref)
+    t0 = time.perf_counter()
+    for p in pts:
+        _ref_chain_point(p, cfg, selgl, have_ref)
+    dt = time.perf_counter() - t0
+    out = {"value": n_points / dt, "unit": UNIT, "cores": 1, "kind": _ref_kind(have_ref),
+           "sample": f"{n_points} points, {_ref_sample(have_ref)}; 1 thread, {dt:.2f} s",
+           "ms_per_point": 1e3 * dt / n_points, "cpu_model": cpu_model(),
+           "nproc": os.cpu_count()}
+    if n_port > 0:
+        import oracle
+        g = synthetic.grid(density)
+        pz, pc = synthetic.plob_baseline()
+        pp = synthetic.walkers(n_port, seed=11, densities=(density,), with_sci=False)
+        t0 = time.perf_counter()
+        for p in pp:
+            oracle.direct_eval(g, pz, pc, p.mor, oracle.cosmo(p.om, p.h0), p.tables)
+        dt = time.perf_counter() - t0
+        out["port_direct_quadrature"] = {
+            "value": n_port / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{n_port} points, FP64 direct nested GL at {density}x nodes (C), 1 thread"}
+    return out
+
+
 def run_reference(a):
-    """Reference arm: the reference algorithm's CPU form (the oracle port; the
-    reference's own C++ needs CosmoSIS/GSL and is not buildable here) on all
-    host cores, one point per worker per step."""
+    """Reference arm: the reference chain on all host cores (one point per
+    worker process per step; the reference evaluates one point per CosmoSIS
+    execute, single-threaded)."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
@@ -206,22 +284,29 @@ def run_reference(a):
     cores = os.cpu_count() or 1
     import oracle
     oracle.build()
+    _, _, have_ref = _ref_chain_setup()
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
         for w in range(a.warmup):
-            pool.map(_ref_worker, [(a.density, 100 + w * cores + i) for i in range(cores)])
+            pool.map(_ref_worker, [100 + w * cores + i for i in range(cores)])
         t0 = time.perf_counter()
         for s in range(a.steps):
-            pool.map(_ref_worker, [(a.density, 1000 + s * cores + i) for i in range(cores)])
+            pool.map(_ref_worker, [1000 + s * cores + i for i in range(cores)])
         dt = time.perf_counter() - t0
     value = a.steps * cores / dt
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * dt / a.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded walkers, HMF/dV/dz/Sigma_crit tables)",
-            "config": {"workload": WORKLOAD, "points_per_step": cores, "density": a.density},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{cores} points per step (one per core), FP64 oracle"},
+            "data": "synthetic (seeded walkers, HMF/dV/dz tables)",
+            "config": {"workload": WORKLOAD, "points_per_step": cores,
+                       "reference_resolution": "sel_function 192x64x32, SelGL 96x64 (its "
+                                               "tabulation differs from the converged "
+                                               "integral by ~4e-4)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores,
+                             "kind": _ref_kind(have_ref),
+                             "sample": f"{cores} points per step, one per core; "
+                                       + _ref_sample(have_ref),
+                             "cpu_model": cpu_model()},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -303,6 +388,79 @@ def workload_run(name, grids, dens, n_points, shear, steps, dev):
             "tuning": tuning, "l2": "flushed between steps", "cuda_graph": True}
 
 
+def module_latency(n_calls=40):
+    """Per-sample latency of the drop-in module: NumCountsFastMass.so with
+    engine = fused, setup once, then execute() on a CosmoSIS-style DataBlock
+    per parameter point (the whole integral, S_stack stage included), as
+    CosmoSIS calls it; median wall time per execute after warm-up, one point
+    per call, for the configs' 1x and 4x node densities."""
+    import numpy as np
+
+    from y3_cluster_cpp_b200 import prj_params, synthetic
+    from y3_cluster_cpp_b200.cosmosis import DataBlock, Module
+
+    out = {}
+    p = synthetic.fiducial()
+    pz, pc = synthetic.plob_baseline()
+    lab = "NumCountsFastMass"
+    for name, dens in (("1x (64 lnM x 32 z_t x 64 lam_t x 64 lam_o x 16 z_o)", 1),
+                       ("4x (256 x 128 x 256 x 256 x 64)", 4)):
+        g = synthetic.grid(dens)
+        res = {}
+        for prec in ("mixed", "fp64"):
+            o = DataBlock()
+            o[lab, "engine"] = "fused"
+            o[lab, "precision"] = prec
+            o[lab, "bin_index"] = np.arange(12)
+            le, ze = g["lam_edges"], g["zob_edges"]
+            o[lab, "lam_min"], o[lab, "lam_max"] = np.tile(le[:-1], 3), np.tile(le[1:], 3)
+            o[lab, "zob_min"], o[lab, "zob_max"] = np.repeat(ze[:-1], 4), np.repeat(ze[1:], 4)
+            o[lab, "sigma_z"] = np.zeros(12)
+            o[lab, "sz0"] = 0.01
+            for k in ("zt_lo", "zt_hi", "lnm_lo", "lnm_hi"):
+                o[lab, {"zt_lo": "zt_low", "zt_hi": "zt_high", "lnm_lo": "lnm_low",
+                        "lnm_hi": "lnm_high"}[k]] = float(g[k])
+            o[lab, "n_lnm"], o[lab, "n_z"], o[lab, "n_lt"] = g["n_m"], g["n_z"], g["n_t"]
+            o[lab, "n_lo"], o[lab, "n_zo"] = g["n_o"], g["n_zo"]
+            b = DataBlock()
+            b["cosmological_parameters", "omega_M"] = p.om
+            b["cosmological_parameters", "omega_lambda"] = 1 - p.om
+            b["cosmological_parameters", "omega_k"] = 0.0
+            b["cosmological_parameters", "h0"] = p.h0
+            b["cosmological_parameters", "omega_nu"] = 0.0
+            b["cluster_abundance", "hmf_s"] = 0.0
+            b["cluster_abundance", "hmf_q"] = 1.0
+            t = p.tables
+            b["mass_function", "m_h"], b["mass_function", "z"] = t["hmf_m_h"], t["hmf_z"]
+            b["mass_function", "dndlnmh"] = t["dndlnmh"]
+            b["distances", "z"], b["distances", "d_a"] = t["dist_z"], t["dist_da"]
+            for k, v in dict(A=p.A, B=p.B, C=p.C, sigma_intr=p.sigma, M_pivot=p.Mpiv).items():
+                b["cluster_mor", k] = v
+            b["plob_ltr_params", "z"] = pz
+            for k, row in zip(prj_params.COEFF_NAMES, pc):
+                b["plob_ltr_params", k] = row
+            m = Module(lab)
+            if not m.setup(o):
+                raise RuntimeError("fused module setup failed")
+            for _ in range(3):
+                if m.execute(b) != 0:
+                    raise RuntimeError("fused module execute failed")
+            ts = []
+            for _ in range(n_calls):
+                t0 = time.perf_counter()
+                m.execute(b)
+                ts.append(time.perf_counter() - t0)
+            m.cleanup()
+            res[prec + "_ms"] = 1e3 * statistics.median(ts)
+        out[name] = res
+    return {"module": "NumCountsFastMass.so, engine = fused (whole integral per execute)",
+            "calls": n_calls, "per_sample": out,
+            "reference_published_ms": {
+                "NumCountsFastMass/NumCountsSel execute (S_stack given)": 6.0,
+                "number-count module page figure": 22.0,
+                "sel_function S_stack tabulation (upstream module)": 215.0}}
+
+
 def serving_run(a, rank, dev):
     """Serving workload: a Poisson request stream (mean gap 2 ms) of requests
     of 1..1024 points (log-uniform), points from the batched-config prior at
@@ -341,28 +499,36 @@ def serving_run(a, rank, dev):
 
     # plain per-request FP64 GPU form, in arrival order (one request at a time)
     lib = engine.lib()
-    fp64_counts, finish, lat64 = [], 0.0, []
+    fp64_counts, finish, lat64, busy = [], 0.0, [], 0.0
     for (pts, tab), t_arr in zip(reqs, arrivals):
         out = np.empty((len(pts), eng.n_bins))
         t_s = time.perf_counter()
         engine.check(lib.y3b_engine_eval(eng.handle, engine.FP64, len(pts), pts,
                                          _capi.ptr(tab), _capi.ptr(out), None))
         svc = time.perf_counter() - t_s
+        busy += svc
         finish = max(finish, t_arr) + svc
         lat64.append(finish - t_arr)
         fp64_counts.append(out)
     fp64_tp = total / finish
+    fp64_capacity = total / busy     # back to back, no arrival gaps
 
-    # warm the server path once, then the timed stream
+    # warm the server path once, then the timed stream, then the same
+    # requests kept `outstanding` at a time (saturated: no arrival gaps)
+    outstanding = 16
     with serve.Server(eng, pool_points=8192, max_batch=2048, precision=engine.MIXED) as srv:
         srv.wait(srv.submit(*reqs[0]))
         s0 = srv.stats()
         run = serve.run_stream(srv, reqs, arrivals)
         s1 = srv.stats()
+        sat = serve.run_closed_loop(srv, reqs, outstanding)
+        s2 = srv.stats()
     eng.close()
     err = max(float(np.max(np.abs(r["counts"] / c - 1)))
-              for r, c in zip(run["results"], fp64_counts))
+              for rr in (run, sat) for r, c in zip(rr["results"], fp64_counts))
     launches = s1["launches"] - s0["launches"]
+    sat_launches = s2["launches"] - s1["launches"]
+    sat_tp = total / sat["wall_s"]
     return {"requests": n_req, "points": total,
             "arrivals": "Poisson, mean gap 2 ms", "sizes": "round(exp(U[0, ln 1024]))",
             "densities": "1x/2x/4x in thirds per point", "tables": "per point, pinned host",
@@ -372,7 +538,17 @@ def serving_run(a, rank, dev):
             "max_launch_points": s1["max_launch_points"],
             "max_rel_err_vs_fp64": err,
             "fp64_per_request": {"throughput": fp64_tp, "unit": UNIT,
-                                 **serve.percentiles_ms(np.asarray(lat64))}}
+                                 **serve.percentiles_ms(np.asarray(lat64)),
+                                 "capacity": fp64_capacity,
+                                 "form": "FP64 direct nested GL (one exp per lnM, z_t, lam_t "
+                                         "node, no factorisation), one engine call per "
+                                         "request, host tables"},
+            "saturated": {"outstanding_requests": outstanding, "throughput": sat_tp,
+                          "unit": UNIT, **serve.percentiles_ms(sat["latency_s"]),
+                          "launches": sat_launches,
+                          "mean_launch_points": total / max(sat_launches, 1),
+                          "speedup_vs_fp64_per_request": sat_tp / fp64_capacity,
+                          "host_table_bytes_per_point": eng.stride * 8}}
 
 
 def run_ours(a):
@@ -535,6 +711,7 @@ def run_ours(a):
     serving = None
     if a.serve_requests > 0:
         serving = serving_run(a, rank, dev)
+    modlat = module_latency() if a.extra_workloads else None
     extra = None
     if a.extra_workloads:
         from y3_cluster_cpp_b200 import synthetic as _syn
@@ -551,7 +728,7 @@ def run_ours(a):
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        cpu = cpu_baseline(a.density, a.cpu_sample)
+        cpu = cpu_baseline(a.cpu_sample, a.density, a.cpu_port_sample)
 
     if world > 1:
         torch.distributed.barrier()
@@ -589,6 +766,8 @@ def run_ours(a):
         }
         if serving is not None:
             line["serving"] = serving
+        if modlat is not None:
+            line["module_execute"] = modlat
         if extra is not None:
             line["other_workloads"] = extra
         if cpu is not None:
@@ -598,16 +777,19 @@ def run_ours(a):
         torch.distributed.destroy_process_group()
 
 
+# DRAM bytes (read + write) per point of one contraction launch at 4x nodes,
+# from one ncu capture of the small case:
+#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none \
+#       -k regex:contract_kernel -s 2 -c 1 python bench.py --steps 3 --warmup 1 \
+#       --batch 256 --no-cpu-baseline --serve-requests 0 --no-extra-workloads
+# (76.06 MB read + 2.70 MB written over 256 points).  Traffic grows with the
+# points (each reads its own operand blocks), so a launch of B points moves
+# B times this.
+CONTRACT_TRAFFIC_BYTES_PER_POINT_4X = 307652.0
+
+
 def ncu_traffic(density, points):
-    """DRAM bytes (read + write) of one contraction launch, from the committed
-    ncu capture of the 4x kernel, scaled by the points one launch processes
-    (each point reads its own operand vectors, so traffic grows with points)."""
-    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
-                        "contract_kernel_counts_4x.md")
-    if density != 4 or not os.path.exists(path):
-        return None
-    m = re.search(r"traffic_bytes_per_point:\s*([0-9.]+)", open(path).read())
-    return float(m.group(1)) * points if m else None
+    return CONTRACT_TRAFFIC_BYTES_PER_POINT_4X * points if density == 4 else None
 
 
 def main():

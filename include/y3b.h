@@ -136,9 +136,13 @@ int y3b_sel_function(const y3b_selfunc_config* cfg, const y3b_mor* mor,
  * The array is shared by every call on a device and keeps the last call's
  * contents: calls that overlap on the GPU (other streams or threads) race on
  * it and must be serialised by the caller.  The first call on each device
- * looks the array's device address up (cudaGetSymbolAddress); make that
- * first call before any stream capture.  Asynchronous on `stream` (a
- * cudaStream_t, NULL = the legacy default stream). */
+ * (and the first after that device's context was reset) looks the array's
+ * device address up (cudaGetSymbolAddress); make that first call before any
+ * stream capture.  Asynchronous on `stream` (a cudaStream_t, NULL = the
+ * legacy default stream): the per-bin arrays of cfg and the projection table
+ * are copied from the caller's memory on that stream, so when they are in
+ * pinned memory they must stay valid until the stream has finished the
+ * call's work; synchronise before reading the outputs. */
 int y3b_sel_function_noalloc(const y3b_selfunc_config* cfg, const y3b_mor* mor,
                              const y3b_plob* plob, double* lnm_dev, double* z_dev,
                              double* S_dev, void* stream);
@@ -322,10 +326,11 @@ int y3b_engine_autotune(y3b_engine* e, int n, const y3b_point* pts_dev,
                         const double* tables_dev, double* counts_dev, double* best_ms);
 /* The current setting: ring depth and bins per tile of each grid (cap >= grids). */
 int y3b_engine_tuning(const y3b_engine* e, int* stages, int* bins_per_tile, int cap);
-/* lam_t stages of the last mixed-form contraction: the stages its tiles
- * issued (each tile skips the stages where the MOR density of all its
- * (lnM, z) pairs is below 4e-6 of its peak) and the stages of the full
- * lam_t range.  Reads device memory: call after that evaluation completed. */
+/* lam_t stages of the last mixed-form evaluation call (all its chunks): the
+ * stages its tiles issued (each tile skips the stages where the
+ * domain-renormalised MOR density of all its (lnM, z) pairs is below 4e-6 of
+ * its peak) and the stages of the full lam_t range.  Reads device memory:
+ * call after that evaluation completed. */
 int y3b_engine_stage_count(const y3b_engine* e, long long* executed, long long* dense);
 /* Wait for the engine's work on `stream` and report device-side errors. */
 int y3b_engine_sync(y3b_engine* e, void* stream);

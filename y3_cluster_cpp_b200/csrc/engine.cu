@@ -174,6 +174,12 @@ prep_kernel(PrepArgs a)
   }
   const GridDev* __restrict__ Gp = a.grids + pt.grid;
   const int n_m = Gp->n_m, n_z = Gp->n_z, n_m_pad = Gp->n_m_pad, tid = threadIdx.x;
+  // The mixed form runs one CTA per (point, 128-row lnM tile): each computes
+  // its tile's Y rows, stage window and F blocks, and the tile-0 CTA also
+  // writes the point's shared factors.  The FP64 form runs one CTA per point.
+  const int mt0 = blockIdx.y;
+  if (mt0 >= n_m_pad / kGemmRows || (!a.mixed && mt0 > 0)) return;
+  const bool lead = mt0 == 0;
   const TableLayout& L = a.lay;
   const int n_hm = L.n_hm, n_hz = L.n_hz;
   // The small tables (HMF axes, distances, Sigma_crit) are staged in shared
@@ -300,7 +306,7 @@ prep_kernel(PrepArgs a)
     const double x = xm[k];
     const double alpha = pt.B * (x - lnMpiv);
     k_alpha[k] = alpha;
-    s64[Gp->o_alpha + k] = alpha;
+    if (lead) s64[Gp->o_alpha + k] = alpha;
     const double xx = fmin(fmax(x, mh[0]), mh[n_hm - 1]);
     const int xi = bsearch_cell(mh, n_hm, xx);
     k_x[k] = xi;
@@ -314,7 +320,7 @@ prep_kernel(PrepArgs a)
     const double z = xz[q];
     const double beta = pt.A + pt.C * log1p(z);
     q_beta[q] = beta;
-    s64[o_beta + q] = beta;
+    if (lead) s64[o_beta + q] = beta;
     const double zz = fmin(fmax(z, hz[0]), hz[n_hz - 1]);
     const int yi = bsearch_cell(hz, n_hz, zz);
     q_y[q] = yi;
@@ -324,6 +330,7 @@ prep_kernel(PrepArgs a)
       set_err(a.status, kDevDomain);
       dv = 0.0;
     }
+    if (!lead) continue;
     const double cz = Gp->wz[q] * dv * Gp->omz[q];
     const double czs = cz * (L.n_sci > 1 ? interp1d_clamp(sz, sv, L.n_sci, z) : 1.0);
     s64[o_cz + q] = cz;
@@ -374,8 +381,10 @@ prep_kernel(PrepArgs a)
       red[3] = amax + bmax;
       red[4] = bmin;
       red[5] = bmax;
-      s64[Gp->o_scal] = red[0];
-      s64[Gp->o_scal + 1] = red[1];
+      if (lead) {
+        s64[Gp->o_scal] = red[0];
+        s64[Gp->o_scal + 1] = red[1];
+      }
     }
   }
   __syncthreads();
@@ -401,12 +410,14 @@ prep_kernel(PrepArgs a)
   // Mixed form: factor vectors and Y(k, q).
   const double L0 = A0 + B0;
   const int n_t = Gp->n_t, n_t_pad = Gp->n_t_pad;
-  for (int k = tid; k < n_m_pad; k += blockDim.x)
-    s32[Gp->f_a + k] = k < n_m ? (float)(k_alpha[k] - A0) : 0.f;
-  for (int q = tid; q < n_z; q += blockDim.x) s32[Gp->f_b + q] = (float)(q_beta[q] - B0);
-  for (int t = tid; t < n_t_pad; t += blockDim.x)
-    s32[Gp->f_delta + t] = t < n_t ? (float)(Gp->xl[t] - L0) : 0.f;
-  if (tid == 0) {
+  if (lead) {
+    for (int k = tid; k < n_m_pad; k += blockDim.x)
+      s32[Gp->f_a + k] = k < n_m ? (float)(k_alpha[k] - A0) : 0.f;
+    for (int q = tid; q < n_z; q += blockDim.x) s32[Gp->f_b + q] = (float)(q_beta[q] - B0);
+    for (int t = tid; t < n_t_pad; t += blockDim.x)
+      s32[Gp->f_delta + t] = t < n_t ? (float)(Gp->xl[t] - L0) : 0.f;
+  }
+  if (lead && tid == 0) {
     const double log2e = 1.4426950408889634;
     s32[Gp->f_scal] = (float)(log2e * 0.5 / (sig * sig));  // c1: F = exp2(-(d - a)^2 c1)
     s32[Gp->f_scal + 1] = (float)(log2e / (sig * sig));    // c2: G = exp2(d b c2)
@@ -456,41 +467,56 @@ prep_kernel(PrepArgs a)
       hmu * inv_s * (exp(-0.5 * aa * aa) - exp(-0.5 * bb * bb)) / kSqrt2Pi;
   }
   __syncthreads();
-  // One warp per z row; lanes over lnM (no divides, FP32 in the common path).
+  // One warp per z row; lanes over lnM, four lnM rows per lane in flight
+  // (independent chains for the schedulers), FP32 in the common path.  The
+  // few cells whose MOR is cut by the lam_t domain (mu within 5.6 sigma of an
+  // edge) are scaled by the FP64 D(mu) afterwards.
   const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
   for (int q = warp; q < n_z; q += nw) {
     const float u = (float)q_u[q];
     const float bb = (float)(q_beta[q] - B0);
+    const float hx = -bb * c2, hy = -0.5f * bb * bb * c2;  // H = 2^(a hx + hy)
+    const float sat_lo = mu_sat_lo - bb, sat_hi = mu_sat_hi - bb;
     const float* hr0 = h32 + q_y[q] * n_hm;
     const float* hr1 = hr0 + n_hm;
     // Tile-blocked: [lnM tile of 128][z][128], so a tile's block is contiguous.
     float* yrow = Yt + (size_t)q * kGemmRows;
-    for (int k = lane; k < n_m_pad; k += 32) {
-      float y = 0.f;
-      if (k < n_m) {
-        const float t = kt_f[k];
-        const int xi = k_x[k];
-        const float n = ((1.f - t) * (1.f - u) * hr0[xi] + t * (1.f - u) * hr0[xi + 1] +
-                         (1.f - t) * u * hr1[xi] + t * u * hr1[xi + 1]) *
-                        kf_f[k];
-        const float aa = ka_f[k];
-        const float H = fast_exp2(-(aa * bb + 0.5f * bb * bb) * c2);
-        const float mu_rel = aa + bb;  // mu - (A0 + B0)
-        float scale = norm0f;
-        if (!(mu_rel > mu_sat_lo && mu_rel < mu_sat_hi)) {
-          const double mu = k_alpha[k] + q_beta[q];
-          const double uu = (mu - mu0) * inv_hmu;
-          const int j = min(max((int)uu, 0), kDTab - 2);
-          const double t = uu - j, t2 = t * t, t3 = t2 * t;
-          double D = (2.0 * t3 - 3.0 * t2 + 1.0) * dtab[j] + (t3 - 2.0 * t2 + t) * dtab[kDTab + j] +
-                     (3.0 * t2 - 2.0 * t3) * dtab[j + 1] + (t3 - t2) * dtab[kDTab + j + 1];
-          if (D < 1e-3) D = mor_norm_slow((ll_lo - mu) * inv_s, (ll_hi - mu) * inv_s);
-          // Y is FP32, so is the quotient.
-          scale = norm0f * __frcp_rn((float)D);
+    for (int k0 = mt0 * kGemmRows; k0 < (mt0 + 1) * kGemmRows; k0 += 128) {
+      float y[4];
+      unsigned slow = 0u;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int k = k0 + lane + 32 * r;
+        y[r] = 0.f;
+        if (k < n_m) {
+          const float t = kt_f[k];
+          const int xi = k_x[k];
+          const float r0 = fmaf(t, hr0[xi + 1] - hr0[xi], hr0[xi]);
+          const float r1 = fmaf(t, hr1[xi + 1] - hr1[xi], hr1[xi]);
+          const float n = fmaf(u, r1 - r0, r0) * kf_f[k];
+          const float aa = ka_f[k];
+          y[r] = n * fast_exp2(fmaf(aa, hx, hy)) * norm0f;
+          slow |= (aa > sat_lo && aa < sat_hi) ? 0u : (1u << r);
         }
-        y = n * H * scale;
       }
-      yrow[(size_t)(k >> 7) * n_z * kGemmRows + (k & (kGemmRows - 1))] = y;
+      while (slow) {
+        const int r = __ffs(slow) - 1;
+        slow &= slow - 1u;
+        const int k = k0 + lane + 32 * r;
+        const double mu = k_alpha[k] + q_beta[q];
+        const double uu = (mu - mu0) * inv_hmu;
+        const int j = min(max((int)uu, 0), kDTab - 2);
+        const double t = uu - j, t2 = t * t, t3 = t2 * t;
+        double D = (2.0 * t3 - 3.0 * t2 + 1.0) * dtab[j] + (t3 - 2.0 * t2 + t) * dtab[kDTab + j] +
+                   (3.0 * t2 - 2.0 * t3) * dtab[j + 1] + (t3 - t2) * dtab[kDTab + j + 1];
+        if (D < 1e-3) D = mor_norm_slow((ll_lo - mu) * inv_s, (ll_hi - mu) * inv_s);
+        y[r] *= __frcp_rn((float)D);  // Y is FP32, so is the quotient
+      }
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int k = k0 + lane + 32 * r;
+        if (k < n_m_pad) yrow[(size_t)(k >> 7) * n_z * kGemmRows + (k & (kGemmRows - 1))] = y[r];
+      }
     }
   }
   // F(t, k) = 2^-((delta_t - a_k) sqrt(c1))^2 for the contraction, split into
@@ -514,8 +540,8 @@ prep_kernel(PrepArgs a)
   // of the split-BF16 products.  The stage count is rounded up to pairs.
   {
     constexpr double kWin = 5.0;
-    const int n_mt = n_m_pad / kGemmRows, nk = n_t_pad / 16;
-    for (int mt = warp; mt < n_mt; mt += nw) {
+    const int nk = n_t_pad / 16;
+    for (int mt = mt0 + warp; mt == mt0; mt += nw) {  // this CTA's tile, warp 0
       double amn = 1e300, amx = -1e300;
       for (int k = mt * kGemmRows + lane; k < min(n_m, (mt + 1) * kGemmRows); k += 32) {
         amn = fmin(amn, k_alpha[k]);
@@ -568,8 +594,8 @@ prep_kernel(PrepArgs a)
   // unaffected).
   if (tid == 0) {
     double dmax = 0.0;
-    for (int mt = 0; mt < n_m_pad / kGemmRows; ++mt) {
-      const int t0 = swin[2 * mt] * 16, t1 = min(swin[2 * mt + 1] * 16, n_t) - 1;
+    {
+      const int t0 = swin[2 * mt0] * 16, t1 = min(swin[2 * mt0 + 1] * 16, n_t) - 1;
       if (t1 >= t0) dmax = fmax(dmax, fmax(fabs((double)dt_f[t0]), fabs((double)dt_f[t1])));
     }
     const double bmax = 0.5 * (red[5] - red[4]);
@@ -578,16 +604,14 @@ prep_kernel(PrepArgs a)
     if (!(e <= kMaxExp2)) set_err(a.status, kDevRange);
   }
   // The window of each contraction tile (lnM tile, richness-bin group).
-  for (int l = tid; l < Gp->tiles_pp; l += blockDim.x) {
-    const int mt = l / Gp->n_bg;
-    a.win_tile[(size_t)p * a.win_stride + l] = swin[2 * mt] | (swin[2 * mt + 1] << 16);
-  }
+  for (int l = mt0 * Gp->n_bg + tid; l < (mt0 + 1) * Gp->n_bg; l += blockDim.x)
+    a.win_tile[(size_t)p * a.win_stride + l] = swin[2 * mt0] | (swin[2 * mt0 + 1] << 16);
   const float sc1 = sqrtf((float)(1.4426950408889634 * 0.5 / (sig * sig)));
   const float2 sc2 = make_float2(sc1, sc1);
   uint8_t* fb = a.fbuf + (size_t)p * a.f_stride;
   const int nk = n_t_pad / 16, n_g8 = n_t_pad / 8;
-  for (int it = tid; it < n_m_pad * n_g8; it += blockDim.x) {
-    const int m = it % n_m_pad, t8 = it / n_m_pad;
+  for (int it = tid; it < kGemmRows * n_g8; it += blockDim.x) {
+    const int m = mt0 * kGemmRows + it % kGemmRows, t8 = it / kGemmRows;
     // Only the stages inside each tile's window are ever read (warp-uniform).
     if ((t8 >> 1) < swin[2 * (m >> 7)] || (t8 >> 1) >= swin[2 * (m >> 7) + 1]) continue;
     const float am = m < n_m ? ka_f[m] * sc1 : 1e18f;
@@ -849,6 +873,7 @@ struct y3b_engine {
   y3b::DevBuf<uint8_t> fbuf;  // F(t, k) stage blocks of the mixed form
   size_t f_stride = 0;        // bytes per point
   int max_tiles_pp = 0, tile_cap_pp = 0;
+  int max_mtiles = 1;  // largest number of 128-row lnM tiles of a grid
   y3b::ContractShape cshape{};
   int cstages = 0, n_ctas = 0;  // contraction ring depth and persistent CTAs
   // Chunked host-buffer evaluation: copy stream, one event and one pinned
@@ -948,6 +973,8 @@ rank_grids(y3b_engine* e)
   for (int r = 0; r < n_grids; ++r) e->grids[idx[r]].cost_rank = r;
   e->max_tiles_pp = 0;
   for (const auto& g : e->grids) e->max_tiles_pp = std::max(e->max_tiles_pp, g.tiles_pp);
+  e->max_mtiles = 1;
+  for (const auto& g : e->grids) e->max_mtiles = std::max(e->max_mtiles, g.n_m_pad / kGemmRows);
 }
 
 static int
@@ -1438,6 +1465,9 @@ enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_t
   double* Phi = e->Phi.get() ? e->Phi.get() + w_off * e->nI_max * e->shear.n_R * e->w_stride
                              : nullptr;
   Y3B_CUDA(cudaMemsetAsync(e->status.get(), 0, sizeof(int), s));
+  // The stage counters cover one evaluation call: zeroed by its first chunk.
+  if (w_off == 0 && prec == Y3B_MIXED)
+    Y3B_CUDA(cudaMemsetAsync(e->stage_ct.get(), 0, 2 * sizeof(int), s));
   if (e->prof) ++e->prof_evals;
   PrepArgs pa{e->d_grids.get(), d_pts, d_tables, d_slot, e->lay, prec == Y3B_MIXED,
               e->s64.get(), e->s32.get(), e->status.get(), grid_mask, e->fbuf.get(), e->f_stride,
@@ -1466,7 +1496,7 @@ enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_t
   }
   {
     StageTimer t(e, s, 0);
-    prep_kernel<<<n, 256, e->prep_smem, s>>>(pa);
+    prep_kernel<<<dim3(n, mixed ? e->max_mtiles : 1), 256, e->prep_smem, s>>>(pa);
     count_launch();
     const cudaError_t perr = cudaGetLastError();
     if (mixed) Y3B_CUDA(cudaStreamWaitEvent(s, e->plan_join, 0));

@@ -343,9 +343,10 @@ block_excl_scan(int v, int* sh, int* total)
 // Orders the points by the cost of their grid's tiles (most expensive grid
 // first, stable inside a grid) and writes the tiles of the launch in that
 // order: tile_start[i] = tiles of order[0..i), tile_start[n] = all tiles,
-// tile_list[t] = (point << 8) | tile inside the point, and the stage count
-// of the full lam_t range (stage_count[1]; stage_count[0], the stages
-// issued, is reset for the contraction to add to).  One block of 1024
+// tile_list[t] = (point << 8) | tile inside the point, and adds the stage
+// count of the full lam_t range to stage_count[1] (the contraction adds the
+// stages it issues to stage_count[0]; both are zeroed once per evaluation
+// call, so the chunks of one call accumulate).  One block of 1024
 // threads, each owning a contiguous chunk of points.  Points whose grid is
 // not in the mask are put last with no tiles.
 __global__ void __launch_bounds__(1024)
@@ -394,10 +395,7 @@ tile_plan_kernel(const GridDev* __restrict__ grids, int n_grids, int grid_mask,
   if (threadIdx.x == 0) tile_start[n] = tot;
   int dn_tot;
   block_excl_scan(dn, sh, &dn_tot);
-  if (threadIdx.x == 0) {
-    stage_count[0] = 0;
-    stage_count[1] = dn_tot;
-  }
+  if (threadIdx.x == 0) stage_count[1] += dn_tot;
 }
 
 // Persistent contraction: one CTA per SM walks the launch's tiles (point,

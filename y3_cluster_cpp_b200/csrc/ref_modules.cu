@@ -890,6 +890,8 @@ y3b_nfw_mis(int which, int n, const double* r, const double* rmis, const double*
 // bin pairing, the per-bin photo-z edges and widths, the projection table)
 // lives in one file-scope __device__ array of fixed size that every call
 // shares.
+#include <cuda.h>
+
 #include <mutex>
 
 namespace y3b {
@@ -902,10 +904,47 @@ constexpr size_t kNoAllocScratchDoubles =
   (2 * kMaxPairs + kNoAllocMaxBins);    // last term holds the int tables
 static __device__ __align__(256) double g_selfunc_scratch[kNoAllocScratchDoubles];
 
-// Device address of g_selfunc_scratch, looked up once per device (host code
-// may not use the symbol itself: it names a host-side stand-in).
+// Device address of g_selfunc_scratch, looked up once per device context
+// (host code may not use the symbol itself: it names a host-side stand-in).
+// The address belongs to the context the module image was loaded into: a
+// caller that resets the device gets a new context, in which the array lives
+// elsewhere, so the cache is keyed by the context's unique id and the lookup
+// is repeated for a new one.
 static std::mutex g_scratch_mu;
 static void* g_scratch_addr[128];
+static unsigned long long g_scratch_ctx[128];
+
+// Unique id of the calling thread's current context (0 if it cannot be
+// read, in which case the address is looked up on every call).  The driver
+// entry points are fetched through the runtime: the library links no
+// driver-API import.
+static unsigned long long
+current_context_id()
+{
+  using GetCurrentFn = CUresult (*)(CUcontext*);
+  using GetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrentFn get_current = nullptr;
+  static GetIdFn get_id = nullptr;
+  static bool resolved = false;
+  if (!resolved) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetIdFn>(f);
+    resolved = true;
+  }
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx ||
+      get_id(ctx, &id) != CUDA_SUCCESS)
+    return 0;
+  return id;
+}
 
 static int
 scratch_address(double** out)
@@ -917,7 +956,8 @@ scratch_address(double** out)
     return Y3B_ERR_INVALID;
   }
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_addr[dev]) {
+  const unsigned long long ctx = current_context_id();
+  if (!g_scratch_addr[dev] || ctx == 0 || ctx != g_scratch_ctx[dev]) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_selfunc_scratch);
     if (e != cudaSuccess || !p) {
@@ -925,6 +965,8 @@ scratch_address(double** out)
       return Y3B_ERR_CUDA;
     }
     g_scratch_addr[dev] = p;
+    // The lookup made the device's context current if it was not yet.
+    g_scratch_ctx[dev] = ctx ? ctx : current_context_id();
   }
   *out = static_cast<double*>(g_scratch_addr[dev]);
   return Y3B_OK;

@@ -165,6 +165,31 @@ def run_stream(server, requests, arrivals):
             "points": int(sum(len(p) for p, _ in requests))}
 
 
+def run_closed_loop(server, requests, outstanding=16):
+    """Saturating stream: keeps `outstanding` requests submitted at all times,
+    submitting the next as soon as the oldest has completed (requests complete
+    in order: admission and batching are oldest first).  Measures what the
+    server sustains when requests never wait for an arrival.  Returns
+    {"results", "latency_s", "wall_s", "points"}."""
+    n = len(requests)
+    tickets = {}
+    results = [None] * n
+    lat = np.zeros(n)
+    start = time.perf_counter()
+    for i in range(min(outstanding, n)):
+        tickets[i] = server.submit(*requests[i])
+    for i in range(n):
+        r = server.wait(tickets.pop(i))
+        results[i] = r
+        lat[i] = r["latency_s"]
+        j = i + outstanding
+        if j < n:
+            tickets[j] = server.submit(*requests[j])
+    wall = time.perf_counter() - start
+    return {"results": results, "latency_s": lat, "wall_s": wall,
+            "points": int(sum(len(p) for p, _ in requests))}
+
+
 def percentiles_ms(lat_s):
     lat = np.asarray(lat_s) * 1e3
     return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
