@@ -374,3 +374,20 @@ def test_fused_module_writes_s_stack_and_defaults(gpu):
                               [p.A, p.B, p.C, p.sigma, p.Mpiv, 1.0, 1000.0], pz, pc)
     np.testing.assert_array_equal(S, S2)
     m.cleanup()
+
+
+def test_fused_module_narrow_scatter_falls_back_to_fp64(gpu):
+    """sigma_int = 0.05 at the 4x grid leaves the mixed form's exponent range;
+    the fused module evaluates such a point in FP64 and still returns it."""
+    g = synthetic.grid(4)
+    g["sz0"], g["sz_bin"] = 0.01, np.zeros(3)
+    p = synthetic.fiducial()
+    p.sigma = 0.05
+    pz, pc = synthetic.plob_baseline()
+    ref, _, _ = O.direct_eval(g, pz, pc, p.mor, O.cosmo(p.om, p.h0), p.tables)
+    m = Module("NumCountsFastMass")
+    assert m.setup(_fused_options("NumCountsFastMass", g, "mixed", np.zeros(3), 0.01))
+    block = _fused_sample(p, pz, pc)
+    assert m.execute(block) == 0
+    np.testing.assert_allclose(block["numcounts_fast_mass", "vals"], ref, rtol=1e-8)
+    m.cleanup()

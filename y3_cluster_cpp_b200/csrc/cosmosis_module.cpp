@@ -431,6 +431,10 @@ execute_fused(c_datablock* block, Module* m, std::vector<double>& vals)
   std::copy(da.begin(), da.end(), f->packed.begin() + off[4]);
   std::vector<double> counts(y3b_engine_n_bins(f->e));
   int rc = y3b_engine_eval(f->e, f->precision, 1, &pt, f->packed.data(), counts.data(), nullptr);
+  // A MOR scatter too narrow for the mixed form's factorised Gaussian: this
+  // point goes through the FP64 form of the same quadrature instead.
+  if (rc == Y3B_ERR_RANGE)
+    rc = y3b_engine_eval(f->e, Y3B_FP64, 1, &pt, f->packed.data(), counts.data(), nullptr);
   if (rc != Y3B_OK) throw Failure{std::string("y3b_engine_eval: ") + y3b_last_error()};
   vals.resize(m->bins.size());
   for (size_t k = 0; k < m->bins.size(); ++k) vals[k] = counts[m->bins[k]];

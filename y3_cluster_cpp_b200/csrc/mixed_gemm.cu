@@ -546,26 +546,35 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
       if (!warp_wait(smem_u32(&vec_full[slot]), (jt >> 1) & 1, abort_s, lane)) continue;
       const float c2 = vs[1];
       const float* dsm = vs + 132 + nz_max;
-      // This thread's item (q, k half, bin): 2 n_z nIh <= 512 items, one each.
+      // This thread's item: z node q, half g of the stage's 16 lam_t nodes,
+      // the stage(s) h of the pair (hs = 2 groups of threads take one stage
+      // each when 4 n_z <= 512, else each thread takes both), and bpt
+      // richness bins, the fewest that let the 2 hs n_z ceil(nIh / bpt)
+      // items fit the 512 threads.  G(t, q) = 2^(delta_t b_q c2) does not
+      // depend on the bin: it is evaluated once per (q, t) and scaled by
+      // u_t K_i(t) for each of the thread's bins.
+      const int hs = n_z <= 128 ? 2 : 1;
+      int bpt = 1;
+      while (bpt < nIh && 2 * hs * n_z * ((nIh + bpt - 1) / bpt) > kProdWarps * 32) ++bpt;
+      const int nsub = (nIh + bpt - 1) / bpt;
       const int q = a % n_z, rest = a / n_z;
-      const int g = rest & 1, il = rest >> 1;
-      const bool active = il < nIh;
+      const int g = rest & 1, h0 = hs == 2 ? (rest >> 1) & 1 : 0;
+      const int sub = hs == 2 ? rest >> 2 : rest >> 1;
+      const int il0 = sub * bpt, nb = max(0, min(bpt, nIh - il0));
+      const bool active = sub < nsub && nb > 0;
       const float bq = active ? vs[4 + kGemmRows + q] * c2 : 0.f;
       const float2 bq2 = make_float2(bq, bq);
       // u_t K_i(t): the staged copy when P(lam_o | lam_t) has no z dependence,
       // else the per-(i, q) rows in global memory.
       const bool uks = G->uk_zindep != 0 && nIh * ntp <= uk_max;
-      const float* uksm = dsm + ntp_max + il * ntp;
-      const float* __restrict__ ukg = G->UK + ((size_t)((i0 + il) * n_z + q)) * ntp;
       const uint32_t lboA = (uint32_t)G->ncp_c * 16u;
-      const uint32_t row_off = (uint32_t)g * lboA + (uint32_t)(il * n_z + q) * 16u;
       for (int kc = T.kc_lo; kc < T.kc_hi; kc += 2, chunk += 2) {
         int sp2[2];
         uint32_t ph2[2];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          sp2[h] = rp.s;
-          ph2[h] = rp.ph;
+        for (int hh = 0; hh < 2; ++hh) {
+          sp2[hh] = rp.s;
+          ph2[hh] = rp.ph;
           rp.next(nst);
         }
         if (chunk >= nst && !warp_wait(smem_u32(&empty[sp2[0]]), ph2[0] ^ 1u, abort_s, lane))
@@ -573,31 +582,37 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
         if (chunk + 1 >= nst && !warp_wait(smem_u32(&empty[sp2[1]]), ph2[1] ^ 1u, abort_s, lane))
           continue;
         if (*abort_s) continue;
-        if (active) {
+        for (int h = h0; active && h < (hs == 2 ? h0 + 1 : 2); ++h) {
+          const int t0 = (kc + h) * kStageK + g * 8;
+          const float4 d0 = *reinterpret_cast<const float4*>(dsm + t0);
+          const float4 d1 = *reinterpret_cast<const float4*>(dsm + t0 + 4);
+          const float2 dd[4] = {make_float2(d0.x, d0.y), make_float2(d0.z, d0.w),
+                                make_float2(d1.x, d1.y), make_float2(d1.z, d1.w)};
+          float2 gq[4];
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int t0 = (kc + h) * kStageK + g * 8;
-            const float4 d0 = *reinterpret_cast<const float4*>(dsm + t0);
-            const float4 d1 = *reinterpret_cast<const float4*>(dsm + t0 + 4);
+          for (int u = 0; u < 4; ++u) {
+            const float2 x = __fmul2_rn(dd[u], bq2);
+            gq[u] = make_float2(fast_exp2(x.x), fast_exp2(x.y));
+          }
+          uint8_t* Ah = smem + sp2[h] * kStageBytes + (uint32_t)g * lboA;
+          for (int b = 0; b < nb; ++b) {
+            const int il = il0 + b;
             float4 u0, u1;
             if (uks) {
+              const float* uksm = dsm + ntp_max + il * ntp;
               u0 = *reinterpret_cast<const float4*>(uksm + t0);
               u1 = *reinterpret_cast<const float4*>(uksm + t0 + 4);
             } else {
+              const float* __restrict__ ukg = G->UK + ((size_t)((i0 + il) * n_z + q)) * ntp;
               u0 = __ldg(reinterpret_cast<const float4*>(ukg + t0));
               u1 = __ldg(reinterpret_cast<const float4*>(ukg + t0 + 4));
             }
-            const float2 dd[4] = {make_float2(d0.x, d0.y), make_float2(d0.z, d0.w),
-                                  make_float2(d1.x, d1.y), make_float2(d1.z, d1.w)};
             const float2 uu[4] = {make_float2(u0.x, u0.y), make_float2(u0.z, u0.w),
                                   make_float2(u1.x, u1.y), make_float2(u1.z, u1.w)};
             float2 v[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              const float2 x = __fmul2_rn(dd[u], bq2);
-              v[u] = __fmul2_rn(uu[u], make_float2(fast_exp2(x.x), fast_exp2(x.y)));
-            }
-            uint8_t* Ahi = smem + sp2[h] * kStageBytes + row_off;
+            for (int u = 0; u < 4; ++u) v[u] = __fmul2_rn(uu[u], gq[u]);
+            uint8_t* Ahi = Ah + (uint32_t)(il * n_z + q) * 16u;
             store_split8(Ahi, Ahi + kAPlane, v);
           }
         }
