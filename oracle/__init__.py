@@ -116,6 +116,8 @@ def _declare(L):
     L.y3o_dsigma_mis_tab.restype = D
     L.y3o_shear1h_mis_tab.argtypes = [I, PD, PD, I, PD, PD, PD, PD, I, D, I, PD, D, D,
                                       I, PD, D, D, I, PD, I, PD, PD, I, PD, I, PD, PD, PD]
+    L.y3o_loglike.argtypes = [I, I, PD, PD, PD, I, PD, PD, I, PD, PD, I]
+    L.y3o_loglike.restype = D
     L.y3o_direct_eval.argtypes = [C.POINTER(DirectGrid), I, PD, PD,
                                   C.POINTER(Lognormal), C.POINTER(Cosmo),
                                   I, PD, I, PD, PD, I, PD, PD,
@@ -319,3 +321,18 @@ def direct_eval(grid, plob_z, plob_coef, mor, cz, tables, shear=None):
     if rc:
         raise ValueError("z outside distances table")
     return counts, W, sh_out
+
+
+# ---- Gaussian likelihood ------------------------------------------------------
+
+def loglike(nc, s1h, prj, log_space, data_nc, ic_nc, data_sh, ic_sh):
+    """likelihood_cp.execute's logL from the module outputs; data and invcov
+    as setup() stores them (logged / delta-method in log space).  s1h and
+    prj are [n_bins, n_R] (prj may be None)."""
+    nc, s1h = _f64(nc), _f64(s1h)
+    nb = nc.size
+    nr = s1h.size // nb
+    dn, icn, ds, ics = _f64(data_nc), _f64(ic_nc), _f64(data_sh), _f64(ic_sh)
+    pj = None if prj is None else _f64(prj)
+    return lib().y3o_loglike(nb, nr, _p(nc), _p(s1h), _p(pj), int(bool(log_space)), _p(dn),
+                             _p(icn), int(icn.ndim == 2), _p(ds), _p(ics), int(ics.ndim == 2))

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cctype>
 #include <map>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <utility>

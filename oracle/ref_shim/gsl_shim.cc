@@ -140,3 +140,45 @@ gsl_interp2d_free(gsl_interp2d* interp)
 }
 
 } // extern "C"
+
+// Adaptive quadrature is declared for the reference's adaptive modules only;
+// nothing on the fixed-grid path calls it.  These report failure.
+#include "gsl/gsl_integration.h"
+
+#include <new>
+
+extern "C" {
+
+gsl_integration_workspace*
+gsl_integration_workspace_alloc(size_t n)
+{
+  auto* w = new (std::nothrow) gsl_integration_workspace;
+  if (w) w->limit = n;
+  return w;
+}
+
+void
+gsl_integration_workspace_free(gsl_integration_workspace* w)
+{
+  delete w;
+}
+
+int
+gsl_integration_qag(const gsl_function*, double, double, double, double, size_t, int,
+                    gsl_integration_workspace*, double* result, double* abserr)
+{
+  *result = 0.0;
+  *abserr = 0.0;
+  return 5;  // GSL_EFAILED
+}
+
+int
+gsl_integration_qagp(const gsl_function*, double*, size_t, double, double, size_t,
+                     gsl_integration_workspace*, double* result, double* abserr)
+{
+  *result = 0.0;
+  *abserr = 0.0;
+  return 5;  // GSL_EFAILED
+}
+
+}  // extern "C"

@@ -979,3 +979,52 @@ y3o_direct_eval(const y3o_direct_grid* g, int n_plob, const double* plob_z,
   free(W); free(Wg); free(S);
   return rc;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Gaussian log-likelihood of y3_buzzard/likelihood_cp.py:132-200:
+ *   shear theory[b, r] = (NC_b > 0 ? S1h[b, r] / NC_b : 0) + prj[b, r]
+ *   (NC repeated over the n_R radii of each bin, bin slow and R fast),
+ *   delta = data - theory, or ln data - ln max(theory, 1e-300) in log space
+ *   (data already logged and invcov already the delta-method one, as setup()
+ *   stores them: likelihood_cp.py:79-92,113-118),
+ *   logL = -0.5 (delta_NC^T C^-1 delta_NC + delta_Sh^T C^-1 delta_Sh),
+ *   a diagonal invcov (dense = 0) as sum delta^2 ic, a dense one as a
+ *   matrix product (likelihood_cp.py:66-72).  prj may be NULL (zero). */
+static double
+y3o_chi2(int n, const double* delta, const double* ic, int dense)
+{
+  double acc = 0.0;
+  if (!dense) {
+    for (int i = 0; i < n; ++i) acc += delta[i] * delta[i] * ic[i];
+    return acc;
+  }
+  for (int i = 0; i < n; ++i) {
+    double row = 0.0;
+    for (int j = 0; j < n; ++j) row += ic[(size_t)i * n + j] * delta[j];
+    acc += delta[i] * row;
+  }
+  return acc;
+}
+
+double
+y3o_loglike(int n_bins, int n_R, const double* nc, const double* s1h,
+            const double* prj, int log_space, const double* data_nc,
+            const double* ic_nc, int nc_dense, const double* data_sh,
+            const double* ic_sh, int sh_dense)
+{
+  int nsh = n_bins * n_R;
+  double* d = calloc((size_t)(n_bins > nsh ? n_bins : nsh) + 1, sizeof(double));
+  for (int b = 0; b < n_bins; ++b)
+    d[b] = log_space ? data_nc[b] - log(nc[b] > 1e-300 ? nc[b] : 1e-300)
+                     : data_nc[b] - nc[b];
+  double chi2 = y3o_chi2(n_bins, d, ic_nc, nc_dense);
+  for (int b = 0; b < n_bins; ++b)
+    for (int r = 0; r < n_R; ++r) {
+      int u = b * n_R + r;
+      double th = (nc[b] <= 0.0 ? 0.0 : s1h[u] / nc[b]) + (prj ? prj[u] : 0.0);
+      d[u] = log_space ? data_sh[u] - log(th > 1e-300 ? th : 1e-300) : data_sh[u] - th;
+    }
+  chi2 += y3o_chi2(nsh, d, ic_sh, sh_dense);
+  free(d);
+  return -0.5 * chi2;
+}

@@ -124,6 +124,12 @@ int y3o_sigma_crit_inv(int n_zl, const double* zl, int n_zs, const double* zs,
                        const double* dist_z, const double* dist_da,
                        double* out);
 
+/* ---- Gaussian likelihood (y3_buzzard/likelihood_cp.py:132-200) ------------ */
+double y3o_loglike(int n_bins, int n_R, const double* nc, const double* s1h,
+                   const double* prj, int log_space, const double* data_nc,
+                   const double* ic_nc, int nc_dense, const double* data_sh,
+                   const double* ic_sh, int sh_dense);
+
 /* ---- direct nested Gauss-Legendre quadrature (the configs' form) ---------- */
 typedef struct {
   int n_m, n_z, n_t, n_o, n_zo;          /* nodes: lnM, z_t, ln lam_t, lam_o/bin, z_o/bin */

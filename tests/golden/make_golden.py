@@ -29,6 +29,10 @@ What it writes (tests/golden/*.npz / *.json):
   (imported with CosmoSIS and astropy stubs; its setup() reads a FITS n(z)
   that is not in the snapshot, so the config tuple is built here with the
   synthetic source n(z): Gaussian, mean 0.9, sigma 0.3, 200 nodes).
+* likelihood_ref.npz -- likelihoods/likelihoods_like from the reference's
+  y3_buzzard/likelihood_cp.py setup/execute on a seeded mock data vector
+  (12 counts, 12 x 10 shear; diagonal and dense inverse covariances; linear
+  and log space) for four seeded theory blocks.
 * selgl_ref.npz -- numcountssel/vals, SelGLCore weights and
   shear1hmissel/vals (exact and idea2) from the reference's own C++
   (src/models/n_operator_sel_gl_t.hh:75-361), compiled from its sources by
@@ -336,6 +340,63 @@ def selgl_reference(ref):
     return out
 
 
+def likelihood_reference(ref):
+    """Runs the reference's y3_buzzard/likelihood_cp.py setup/execute on a
+    synthetic mock data vector (12 counts, 12 x 10 shear) with diagonal and
+    dense inverse covariances, in linear and log space, for a set of seeded
+    theory blocks (counts, 1-halo shear, projection shear)."""
+    sys.path.insert(0, os.path.join(ref, "y3_buzzard"))
+    import likelihood_cp as L
+
+    rng = np.random.default_rng(7)
+    nb, nr = 12, 10
+    data_nc = rng.uniform(50.0, 500.0, nb)
+    data_sh = rng.uniform(0.005, 0.05, nb * nr)
+    A = rng.normal(size=(nb, nb))
+    dense_nc = np.linalg.inv(A @ A.T + nb * np.diag(data_nc))
+    B = rng.normal(size=(nb * nr, nb * nr))
+    dense_sh = np.linalg.inv(1e-6 * (B @ B.T) + np.diag((0.1 * data_sh) ** 2))
+    diag_nc = 1.0 / (0.1 * data_nc) ** 2
+    diag_sh = 1.0 / (0.1 * data_sh) ** 2
+    thr_nc = data_nc[None, :] * rng.uniform(0.8, 1.2, (4, nb))
+    thr_nc[3, 5] = -1.0                      # a non-positive count: shear theory 0 there
+    thr_s1h = (data_sh.reshape(nb, nr) * data_nc[:, None])[None] * rng.uniform(0.7, 1.1, (4, nb, nr))
+    thr_prj = 0.1 * data_sh.reshape(nb, nr)[None] * rng.uniform(-1.0, 1.0, (4, nb, nr))
+    out = dict(data_nc=data_nc, data_sh=data_sh, dense_nc=dense_nc, dense_sh=dense_sh,
+               diag_nc=diag_nc, diag_sh=diag_sh, thr_nc=thr_nc, thr_s1h=thr_s1h,
+               thr_prj=thr_prj)
+    with tempfile.TemporaryDirectory() as d:
+        for form in ("diag", "dense"):
+            fname = os.path.join(d, f"mock_{form}.npz")
+            ic_nc = diag_nc if form == "diag" else dense_nc
+            ic_sh = diag_sh if form == "diag" else dense_sh
+            np.savez(fname, data_NC=data_nc, invcov_NC=ic_nc, data_Shear=data_sh,
+                     invcov_Shear=ic_sh)
+            for log_space in (False, True):
+                cfg = L.setup(_OptionsIndex(filename=fname, log_space=log_space,
+                                            verbose=False))
+                vals = []
+                for t in range(4):
+                    block = Block()
+                    block["numcountssel", "vals"] = thr_nc[t]
+                    block["shear1hmissel", "vals"] = thr_s1h[t].ravel()
+                    block["shear_prj", "vals"] = thr_prj[t].ravel()
+                    L.execute(block, cfg)
+                    vals.append(block["likelihoods", "likelihoods_like"])
+                out[f"logL_{form}_{'log' if log_space else 'lin'}"] = np.array(vals)
+    return out
+
+
+class _OptionsIndex(dict):
+    """options[section, key] and options.get_bool(section, key, default)."""
+
+    def __getitem__(self, key):
+        return dict.__getitem__(self, key[1])
+
+    def get_bool(self, section, key, default=False):
+        return bool(self.get(key, default))
+
+
 def main(ref=None):
     if ref is None:
         raise SystemExit("usage: make_golden.py <reference-checkout>")
@@ -357,6 +418,7 @@ def main(ref=None):
         json.dump(kats(ref), f, indent=1)
     np.savez_compressed(os.path.join(HERE, "sigma_crit_inv.npz"), **sigma_crit_inv_reference(ref))
     np.savez_compressed(os.path.join(HERE, "selgl_ref.npz"), **selgl_reference(ref))
+    np.savez_compressed(os.path.join(HERE, "likelihood_ref.npz"), **likelihood_reference(ref))
     print("wrote golden fixtures to", HERE)
 
 

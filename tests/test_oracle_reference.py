@@ -143,3 +143,24 @@ def test_direct_quadrature_converges_to_reference_chain():
         gaps.append(np.max(np.abs(norm / counts - 1)))
     assert gaps[1] < 3e-5, gaps
     assert gaps[1] < gaps[0] / 8, gaps
+
+
+@pytest.mark.parametrize("form", ["diag", "dense"])
+@pytest.mark.parametrize("space", ["lin", "log"])
+def test_loglike_matches_reference_likelihood(form, space):
+    """y3o_loglike against likelihoods/likelihoods_like of the reference's
+    y3_buzzard/likelihood_cp.py (setup + execute) on the golden mock data
+    vector: counts + (1-halo shear / counts + projection shear)."""
+    g = np.load(os.path.join(GOLD, "likelihood_ref.npz"))
+    log_space = space == "log"
+    dn, ds = g["data_nc"], g["data_sh"]
+    icn, ics = g[f"{form}_nc"], g[f"{form}_sh"]
+    if log_space:   # what setup() stores (likelihood_cp.py:79-92, 113-118)
+        icn = icn * (np.outer(dn, dn) if icn.ndim == 2 else dn * dn)
+        ics = ics * (np.outer(ds, ds) if ics.ndim == 2 else ds * ds)
+        dn, ds = np.log(dn), np.log(ds)
+    ref = g[f"logL_{form}_{space}"]
+    for t in range(len(ref)):
+        v = O.loglike(g["thr_nc"][t], g["thr_s1h"][t], g["thr_prj"][t], log_space,
+                      dn, icn, ds, ics)
+        assert v == pytest.approx(ref[t], rel=1e-12, abs=1e-9)
