@@ -338,6 +338,40 @@ int y3b_engine_sync(y3b_engine* e, void* stream);
  * of each point's grid, padded to the largest n_m), host buffer. */
 int y3b_engine_weights(y3b_engine* e, int n, double* W);
 
+/* Gaussian likelihood of the counts + tangential shear data vector, as
+ * y3_buzzard/likelihood_cp.py:94-200 computes it from numcountssel/vals,
+ * shear1hmissel/vals and shear_prj/vals:
+ *   shear theory[b][r] = (N_b > 0 ? S1h[b][r] / N_b : 0) + prj[b][r],
+ *   logL = -0.5 (d_NC^T C^-1 d_NC + d_Sh^T C^-1 d_Sh), d = data - theory, or
+ *   ln data - ln max(theory, 1e-300) in log space (the inverse covariance then
+ *   becomes invcov * data data^T, as the reference's setup() does).
+ * Inverse covariances are diagonal ([n]) or dense ([n][n], *_dense = 1); the
+ * shear vector is bin slow, R fast; n_R = 0 uses the counts alone. */
+typedef struct {
+  int log_space;
+  int n_bins, n_R;
+  const double* data_nc;  const double* invcov_nc; int nc_dense;
+  const double* data_sh;  const double* invcov_sh; int sh_dense;
+  const double* shear_prj;              /* [n_bins][n_R] projection shear, or NULL */
+} y3b_likelihood;
+/* Fuses the likelihood into every later evaluation: the block that sums a
+ * point's counts and shear also writes its logL (n_bins must match every
+ * grid; a shear data vector needs the engine's shear and radii).  Copies the
+ * vectors; NULL switches it off.  Drops captured CUDA graphs. */
+int y3b_engine_set_likelihood(y3b_engine* e, const y3b_likelihood* L);
+/* logL [n] of the last evaluation's points, copied on `stream` (NULL: the
+ * engine's stream) and synchronised. */
+int y3b_engine_loglike(y3b_engine* e, int n, double* logL, void* stream);
+/* Host-buffer evaluation that returns only each point's logL [n]. */
+int y3b_engine_eval_loglike(y3b_engine* e, int precision, int n,
+                            const y3b_point* pts, const double* tables,
+                            double* logL);
+/* The same likelihood of one data vector (counts [n_bins], N_i-weighted
+ * one-halo shear [n_bins][n_R]) on the device: the CosmoSIS likelihood
+ * module's evaluation. */
+int y3b_gaussian_loglike(const y3b_likelihood* L, const double* counts,
+                         const double* shear_1h, double* logL);
+
 /* Stage timing with CUDA events recorded on the launching stream around each
  * stage of every evaluation: 0 = per-point prep, 1 = lambda_t contraction
  * (tcgen05 GEMM or FP64 direct sum + z reduction), 2 = miscentred profile,

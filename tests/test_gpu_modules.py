@@ -391,3 +391,35 @@ def test_fused_module_narrow_scatter_falls_back_to_fp64(gpu):
     assert m.execute(block) == 0
     np.testing.assert_allclose(block["numcounts_fast_mass", "vals"], ref, rtol=1e-8)
     m.cleanup()
+
+
+# ---- Gaussian likelihood (y3_buzzard/likelihood_cp.py) ------------------------
+
+class _Opt(dict):
+    def __getitem__(self, key):
+        return dict.__getitem__(self, key[1])
+
+    def get_bool(self, section, key, default=False):
+        return bool(self.get(key, default))
+
+
+@pytest.mark.parametrize("form", ["diag", "dense"])
+@pytest.mark.parametrize("space", ["lin", "log"])
+def test_likelihood_module_matches_reference(gpu, tmp_path, form, space):
+    """The likelihood module (setup/execute on a block, evaluated on the GPU)
+    against likelihoods/likelihoods_like of the reference's likelihood_cp.py
+    on the golden mock data vector and theory blocks."""
+    from y3_cluster_cpp_b200 import likelihood_cp as LK
+    g = np.load(os.path.join(GOLD, "likelihood_ref.npz"))
+    fname = str(tmp_path / "mock.npz")
+    np.savez(fname, data_NC=g["data_nc"], invcov_NC=g[f"{form}_nc"], data_Shear=g["data_sh"],
+             invcov_Shear=g[f"{form}_sh"])
+    cfg = LK.setup(_Opt(filename=fname, log_space=space == "log"))
+    ref = g[f"logL_{form}_{space}"]
+    for t in range(len(ref)):
+        block = {("numcountssel", "vals"): g["thr_nc"][t],
+                 ("shear1hmissel", "vals"): g["thr_s1h"][t].ravel(),
+                 ("shear_prj", "vals"): g["thr_prj"][t].ravel()}
+        assert LK.execute(block, cfg) == 0
+        assert block["likelihoods", "likelihoods_like"] == pytest.approx(ref[t], rel=1e-10,
+                                                                          abs=1e-8)

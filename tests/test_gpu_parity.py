@@ -493,3 +493,49 @@ def test_batched_config_sample_counts_and_delta_sigma_match_oracle(gpu):
             np.testing.assert_allclose(r["counts"][i], c_ref, rtol=tol)
             np.testing.assert_allclose(r["shear"][i], s_ref, rtol=tol)
     eng.close()
+
+
+@pytest.mark.parametrize("dense", [False, True])
+@pytest.mark.parametrize("log_space", [False, True])
+def test_engine_fused_likelihood(gpu, dense, log_space):
+    """The likelihood fused into the engine's final sums: each point's logL
+    equals the oracle's likelihood (restated from likelihood_cp.py, pinned to
+    it) of that point's own counts and shear, in both precisions, for the
+    device-buffer path and the host-buffer loglike-only call."""
+    g = synthetic.grid(1, n_m=32)
+    sh = synthetic.shear_opts(n_theta=16, n_s=32, n_R=5)
+    eng = _engine([g], n_max=6, shear=sh)
+    pts = synthetic.walkers(6, seed=9, densities=(1,))
+    rng = np.random.default_rng(3)
+    fid = eng.eval([synthetic.fiducial()], E.FP64, grid_of=lambda _: 0)
+    d_nc = fid["counts"][0] * rng.uniform(0.9, 1.1, 12)
+    d_sh = (fid["shear"][0] / fid["counts"][0][:, None]).ravel() * rng.uniform(0.9, 1.1, 60)
+    prj = 0.05 * d_sh * rng.uniform(-1, 1, 60)
+    if dense:
+        A = rng.normal(size=(12, 12))
+        ic_nc = np.linalg.inv(A @ A.T + np.diag(d_nc))
+        Bm = rng.normal(size=(60, 60))
+        ic_sh = np.linalg.inv(1e-3 * np.diag(d_sh ** 2) @ (np.eye(60) + 0.01 * Bm @ Bm.T))
+    else:
+        ic_nc, ic_sh = 1.0 / d_nc, 1.0 / (0.1 * d_sh) ** 2
+    spec = E.LikelihoodSpec(d_nc, ic_nc, d_sh, ic_sh, shear_prj=prj, log_space=log_space)
+    eng.set_likelihood(spec)
+    dn, ds, icn, ics = d_nc, d_sh, ic_nc, ic_sh
+    if log_space:
+        icn = icn * (np.outer(dn, dn) if dense else dn * dn)
+        ics = ics * (np.outer(ds, ds) if dense else ds * ds)
+        dn, ds = np.log(dn), np.log(ds)
+    for prec in (E.FP64, E.MIXED):
+        r = eng.eval(pts, prec, grid_of=lambda _: 0)
+        ll = eng.loglike(len(pts))
+        for i in range(len(pts)):
+            ref = O.loglike(r["counts"][i], r["shear"][i], prj, log_space, dn, icn, ds, ics)
+            assert ll[i] == pytest.approx(ref, rel=1e-11, abs=1e-9)
+        parr = eng.points_array(pts, grid_of=lambda _: 0)
+        tab = np.ascontiguousarray(eng.pack(pts))
+        out = np.empty(len(pts))
+        E.check(E.lib().y3b_engine_eval_loglike(eng.handle, prec, len(pts), parr,
+                                                E.A.ptr(tab), E.A.ptr(out)))
+        np.testing.assert_array_equal(out, ll)
+    eng.set_likelihood(None)
+    eng.close()

@@ -107,6 +107,13 @@ class ServerConfig(C.Structure):
                 ("precision", I), ("with_shear", I), ("max_inflight", I)]
 
 
+class Likelihood(C.Structure):
+    _fields_ = [("log_space", I), ("n_bins", I), ("n_R", I),
+                ("data_nc", PD), ("invcov_nc", PD), ("nc_dense", I),
+                ("data_sh", PD), ("invcov_sh", PD), ("sh_dense", I),
+                ("shear_prj", PD)]
+
+
 class ServerStats(C.Structure):
     _fields_ = [("requests_done", C.c_longlong), ("points_done", C.c_longlong),
                 ("launches", C.c_longlong), ("max_launch_points", I), ("pool_points", I),
@@ -189,6 +196,10 @@ def _declare(L):
     L.y3b_planner_complete.argtypes = [VP, C.c_longlong, I, PI]
     L.y3b_planner_cancel.argtypes = [VP, C.c_longlong, PI]
     L.y3b_planner_free_points.argtypes = [VP]
+    L.y3b_engine_set_likelihood.argtypes = [VP, C.POINTER(Likelihood)]
+    L.y3b_engine_loglike.argtypes = [VP, I, PD, VP]
+    L.y3b_engine_eval_loglike.argtypes = [VP, I, I, C.POINTER(Point), PD, PD]
+    L.y3b_gaussian_loglike.argtypes = [C.POINTER(Likelihood), PD, PD, PD]
     L.y3b_engine_profile.argtypes = [VP, I]
     L.y3b_engine_profile_read.argtypes = [VP, PD, PI]
 
@@ -226,5 +237,6 @@ EXPORTED = [
     "y3b_server_stats_read", "y3b_server_cancel", "y3b_server_destroy", "y3b_planner_create",
     "y3b_planner_destroy", "y3b_planner_submit", "y3b_planner_admit",
     "y3b_planner_next_batch", "y3b_planner_complete", "y3b_planner_cancel",
-    "y3b_planner_free_points",
+    "y3b_planner_free_points", "y3b_engine_set_likelihood", "y3b_engine_loglike",
+    "y3b_engine_eval_loglike", "y3b_gaussian_loglike",
 ]

@@ -25,6 +25,7 @@
 #include "common.cuh"
 #include "engine_internal.h"
 #include "host_common.h"
+#include "likelihood.cuh"
 #include "mis_quad.cuh"
 
 namespace y3b {
@@ -814,8 +815,11 @@ shear_tab_kernel(const GridDev* grids, const PointDev* pts, int n_points, int w_
 __global__ void __launch_bounds__(256)
 finalize_kernel(const GridDev* grids, const PointDev* pts, const double* W, const double* Wg,
                 const double* Phi, int w_stride, int nB_max, int nI_max, int n_R,
-                double* counts, double* shear, int grid_mask)
+                double* counts, double* shear, int grid_mask, LikeDev like, double* logL)
 {
+  __shared__ double s_nc[kMaxLamBins * kMaxZBins];
+  __shared__ double s_sh[kMaxLamBins * kMaxZBins * kMaxR];
+  __shared__ double s_red[256];
   const int p = blockIdx.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const PointDev pt = pts[p];
   if (!grid_in_mask(grid_mask, pt.grid)) return;
@@ -826,7 +830,10 @@ finalize_kernel(const GridDev* grids, const PointDev* pts, const double* W, cons
     double acc = 0.0;
     for (int k = lane; k < G.n_m; k += 32) acc += G.wm[k] * Wb[k];
     acc = warp_sum(acc);
-    if (lane == 0) counts[(size_t)p * nB_max + b] = acc;
+    if (lane == 0) {
+      counts[(size_t)p * nB_max + b] = acc;
+      s_nc[b] = acc;
+    }
   }
   if (shear && Phi) {
     for (int u = warp; u < G.nB * n_R; u += nw) {
@@ -836,8 +843,18 @@ finalize_kernel(const GridDev* grids, const PointDev* pts, const double* W, cons
       double acc = 0.0;
       for (int k = lane; k < G.n_m; k += 32) acc += G.wm[k] * Wb[k] * ph[k];
       acc = warp_sum(acc);
-      if (lane == 0) shear[((size_t)p * nB_max + b) * n_R + iR] = acc;
+      if (lane == 0) {
+        shear[((size_t)p * nB_max + b) * n_R + iR] = acc;
+        s_sh[u] = acc;
+      }
     }
+  }
+  // The point's Gaussian likelihood, in the block that produced its counts
+  // and shear (likelihood_cp.py:132-200): no second pass over them.
+  if (like.on && logL) {
+    __syncthreads();
+    const double v = gaussian_loglike_block(like, G.nB, like.n_R, s_nc, s_sh, s_red);
+    if (threadIdx.x == 0) logL[p] = v;
   }
 }
 
@@ -871,6 +888,8 @@ struct y3b_engine {
   y3b::DevBuf<int> tile_list;
   y3b::DevBuf<int> win_tile;  // [max_points][tile_cap_pp] stage windows (prep -> contraction)
   y3b::DevBuf<uint8_t> fbuf;  // F(t, k) stage blocks of the mixed form
+  y3b::LikeDev like{};        // Gaussian likelihood fused into the final sums (on = 0: none)
+  y3b::DevBuf<double> like_buf, logL;
   size_t f_stride = 0;        // bytes per point
   int max_tiles_pp = 0, tile_cap_pp = 0;
   int max_mtiles = 1;  // largest number of 128-row lnM tiles of a grid
@@ -1539,10 +1558,13 @@ enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_t
   }
   {
     StageTimer t(e, s, 3);
+    // The likelihood needs the shear when its data vector has one.
+    const bool like = e->like.on && (e->like.n_R == 0 || shear);
     finalize_kernel<<<n, 256, 0, s>>>(e->d_grids.get(), d_pts, W, Wg,
                                       shear ? Phi : nullptr, e->w_stride, e->nB_max,
                                       e->nI_max, e->shear.n_R, d_counts,
-                                      shear ? d_shear : nullptr, grid_mask);
+                                      shear ? d_shear : nullptr, grid_mask, e->like,
+                                      like ? e->logL.get() + w_off : nullptr);
     count_launch();
     Y3B_CUDA(cudaGetLastError());
   }
@@ -1997,5 +2019,167 @@ y3b_engine_tuning(const y3b_engine* e, int* stages, int* bins_per_tile, int cap)
   }
   *stages = e->cstages;
   for (size_t g = 0; g < e->grids.size(); ++g) bins_per_tile[g] = e->grids[g].nIc;
+  return Y3B_OK;
+}
+
+// ===========================================================================
+// Gaussian likelihood (y3_buzzard/likelihood_cp.py:94-200).
+namespace y3b {
+
+// Host side of likelihood_cp.setup(): checks the sizes and, in log space,
+// stores ln(data) and the delta-method inverse covariance invcov * d d^T
+// (likelihood_cp.py:79-92, 113-118).  The device copy is one buffer.
+static int
+like_upload(const y3b_likelihood* L, DevBuf<double>& buf, LikeDev* out, cudaStream_t s)
+{
+  const int nB = L->n_bins, nR = L->n_R, nsh = nB * nR;
+  if (nB < 1 || nB > kMaxLamBins * kMaxZBins || nR < 0 || nR > kMaxR || !L->data_nc ||
+      !L->invcov_nc || (nsh && (!L->data_sh || !L->invcov_sh))) {
+    set_error("likelihood: need 1 <= n_bins <= %d, 0 <= n_R <= %d and the data and inverse "
+              "covariance of each observable", kMaxLamBins * kMaxZBins, kMaxR);
+    return Y3B_ERR_INVALID;
+  }
+  const size_t icn = L->nc_dense ? (size_t)nB * nB : nB;
+  const size_t ics = L->sh_dense ? (size_t)nsh * nsh : nsh;
+  std::vector<double> h;
+  h.reserve(nB + icn + nsh + ics + (L->shear_prj ? nsh : 0));
+  auto put = [&](const double* d, const double* ic, int n, int dense) -> int {
+    for (int i = 0; i < n; ++i) {
+      if (!std::isfinite(d[i]) || (L->log_space && !(d[i] > 0.0))) {
+        set_error("likelihood: %s data entry %d (log space requires data > 0)",
+                  std::isfinite(d[i]) ? "non-positive" : "non-finite", i);
+        return Y3B_ERR_INVALID;
+      }
+      h.push_back(L->log_space ? std::log(d[i]) : d[i]);
+    }
+    const size_t m = dense ? (size_t)n * n : n;
+    for (size_t u = 0; u < m; ++u) {
+      const size_t i = dense ? u / n : u, j = dense ? u % n : u;
+      h.push_back(L->log_space ? ic[u] * d[i] * d[j] : ic[u]);
+    }
+    return Y3B_OK;
+  };
+  Y3B_TRY(put(L->data_nc, L->invcov_nc, nB, L->nc_dense != 0));
+  if (nsh) Y3B_TRY(put(L->data_sh, L->invcov_sh, nsh, L->sh_dense != 0));
+  if (nsh && L->shear_prj) h.insert(h.end(), L->shear_prj, L->shear_prj + nsh);
+  Y3B_TRY(buf.upload(h.data(), h.size(), s));
+  Y3B_CUDA(cudaStreamSynchronize(s));
+  const double* d = buf.get();
+  LikeDev& o = *out;
+  o.on = 1;
+  o.log_space = L->log_space != 0;
+  o.n_R = nR;
+  o.nc_dense = L->nc_dense != 0;
+  o.sh_dense = L->sh_dense != 0;
+  o.data_nc = d;
+  o.ic_nc = d + nB;
+  o.data_sh = nsh ? o.ic_nc + icn : nullptr;
+  o.ic_sh = nsh ? o.data_sh + nsh : nullptr;
+  o.prj = nsh && L->shear_prj ? o.ic_sh + ics : nullptr;
+  return Y3B_OK;
+}
+
+// One data vector (the CosmoSIS likelihood module's case).
+__global__ void __launch_bounds__(256)
+loglike_kernel(LikeDev L, int nB, const double* nc, const double* sh, double* out)
+{
+  __shared__ double s_nc[kMaxLamBins * kMaxZBins];
+  __shared__ double s_sh[kMaxLamBins * kMaxZBins * kMaxR];
+  __shared__ double s_red[256];
+  for (int b = threadIdx.x; b < nB; b += blockDim.x) s_nc[b] = nc[b];
+  for (int u = threadIdx.x; u < nB * L.n_R; u += blockDim.x) s_sh[u] = sh[u];
+  __syncthreads();
+  const double v = gaussian_loglike_block(L, nB, L.n_R, s_nc, s_sh, s_red);
+  if (threadIdx.x == 0) *out = v;
+}
+
+}  // namespace y3b
+
+extern "C" int
+y3b_engine_set_likelihood(y3b_engine* e, const y3b_likelihood* L)
+{
+  using namespace y3b;
+  clear_error();
+  if (!e) return Y3B_ERR_INVALID;
+  // Captured graphs hold the previous settings: drop them (they are
+  // re-captured on repeat).
+  const int mode = e->graph_mode;
+  Y3B_TRY(y3b_engine_set_graphs(e, 0));
+  e->graph_mode = mode;
+  e->like = LikeDev{};
+  if (!L) return Y3B_OK;
+  for (const auto& g : e->grids)
+    if (g.nB != L->n_bins) {
+      set_error("y3b_engine_set_likelihood: n_bins %d differs from a grid's %d bins", L->n_bins,
+                g.nB);
+      return Y3B_ERR_INVALID;
+    }
+  if (L->n_R && (!e->cfg.with_shear || L->n_R != e->shear.n_R)) {
+    set_error("y3b_engine_set_likelihood: a shear data vector needs an engine with shear and "
+              "the same %d radii", e->shear.n_R);
+    return Y3B_ERR_INVALID;
+  }
+  LikeDev ld{};
+  Y3B_TRY(like_upload(L, e->like_buf, &ld, e->stream));
+  Y3B_TRY(e->logL.alloc(e->cfg.max_points));
+  e->like = ld;
+  return Y3B_OK;
+}
+
+extern "C" int
+y3b_engine_loglike(y3b_engine* e, int n, double* logL, void* stream)
+{
+  using namespace y3b;
+  clear_error();
+  if (!e || !logL || n < 1 || n > e->cfg.max_points || !e->like.on) {
+    set_error("y3b_engine_loglike: no likelihood set, or n outside 1..max_points");
+    return Y3B_ERR_INVALID;
+  }
+  cudaStream_t s = stream ? (cudaStream_t)stream : e->stream;
+  Y3B_CUDA(cudaMemcpyAsync(logL, e->logL.get(), n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  Y3B_CUDA(cudaStreamSynchronize(s));
+  return Y3B_OK;
+}
+
+extern "C" int
+y3b_engine_eval_loglike(y3b_engine* e, int precision, int n, const y3b_point* pts,
+                        const double* tables, double* logL)
+{
+  using namespace y3b;
+  clear_error();
+  if (!e || !logL || !e->like.on) {
+    set_error("y3b_engine_eval_loglike: no likelihood set (y3b_engine_set_likelihood)");
+    return Y3B_ERR_INVALID;
+  }
+  std::vector<double> counts((size_t)std::max(n, 0) * e->nB_max);
+  std::vector<double> shear(e->like.n_R ? (size_t)std::max(n, 0) * e->nB_max * e->shear.n_R : 0);
+  Y3B_TRY(y3b_engine_eval(e, precision, n, pts, tables, counts.data(),
+                          e->like.n_R ? shear.data() : nullptr));
+  return y3b_engine_loglike(e, n, logL, nullptr);
+}
+
+extern "C" int
+y3b_gaussian_loglike(const y3b_likelihood* L, const double* counts, const double* shear_1h,
+                     double* logL)
+{
+  using namespace y3b;
+  clear_error();
+  if (!L || !counts || !logL || (L->n_R && !shear_1h)) {
+    set_error("y3b_gaussian_loglike: null argument");
+    return Y3B_ERR_INVALID;
+  }
+  Y3B_TRY(require_device());
+  DevBuf<double> buf, in, out;
+  LikeDev ld{};
+  Y3B_TRY(like_upload(L, buf, &ld, 0));
+  const int nB = L->n_bins, nsh = nB * L->n_R;
+  std::vector<double> h(counts, counts + nB);
+  if (nsh) h.insert(h.end(), shear_1h, shear_1h + nsh);
+  Y3B_TRY(in.upload(h.data(), h.size(), 0));
+  Y3B_TRY(out.alloc(1));
+  loglike_kernel<<<1, 256>>>(ld, nB, in.get(), nsh ? in.get() + nB : nullptr, out.get());
+  count_launch();
+  Y3B_CUDA(cudaGetLastError());
+  Y3B_CUDA(cudaMemcpy(logL, out.get(), sizeof(double), cudaMemcpyDeviceToHost));
   return Y3B_OK;
 }

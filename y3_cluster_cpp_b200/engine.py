@@ -139,6 +139,42 @@ class SelGL:
         return out
 
 
+class LikelihoodSpec:
+    """Host arrays of a y3b_likelihood kept alive with the struct: data and
+    inverse covariance (1-D: diagonal, 2-D: dense) of the counts and, when
+    data_sh is given, of the shear (bin slow, R fast); shear_prj optional."""
+
+    def __init__(self, data_nc, invcov_nc, data_sh=None, invcov_sh=None, shear_prj=None,
+                 log_space=False):
+        self.keep = [f64(data_nc), f64(invcov_nc)]
+        nb = self.keep[0].size
+        L = A.Likelihood()
+        L.log_space = int(bool(log_space))
+        L.n_bins = nb
+        L.data_nc, L.invcov_nc = ptr(self.keep[0]), ptr(self.keep[1])
+        L.nc_dense = int(self.keep[1].ndim == 2)
+        if data_sh is not None:
+            ds, ics = f64(data_sh).ravel(), f64(invcov_sh)
+            self.keep += [ds, ics]
+            L.n_R = ds.size // nb
+            L.data_sh, L.invcov_sh = ptr(ds), ptr(ics)
+            L.sh_dense = int(ics.ndim == 2)
+            if shear_prj is not None:
+                pj = f64(shear_prj).ravel()
+                self.keep.append(pj)
+                L.shear_prj = ptr(pj)
+        self.struct = L
+
+
+def gaussian_loglike(spec, counts, shear_1h=None):
+    """The likelihood of one data vector on the device (y3b_gaussian_loglike)."""
+    c = f64(counts)
+    s = None if shear_1h is None else f64(shear_1h).ravel()
+    out = C.c_double()
+    check(lib().y3b_gaussian_loglike(C.byref(spec.struct), ptr(c), ptr(s), C.byref(out)))
+    return out.value
+
+
 def sigma_crit_inv(zl, zs, pz, delta_z, h0, dist_z, dist_da):
     zl, zs, pz, dz, da = map(f64, (zl, zs, pz, dist_z, dist_da))
     out = np.empty(len(zl))
@@ -307,6 +343,18 @@ class Engine:
         ex, dn = C.c_longlong(), C.c_longlong()
         check(lib().y3b_engine_stage_count(self._h, C.byref(ex), C.byref(dn)))
         return ex.value, dn.value
+
+    def set_likelihood(self, spec):
+        """Fuse a Gaussian likelihood (LikelihoodSpec, None: off) into every
+        later evaluation."""
+        self._like = spec
+        check(lib().y3b_engine_set_likelihood(self._h, None if spec is None
+                                              else C.byref(spec.struct)))
+
+    def loglike(self, n):
+        out = np.empty(n)
+        check(lib().y3b_engine_loglike(self._h, n, ptr(out), None))
+        return out
 
     def set_graphs(self, on=True):
         """CUDA-graph replay of repeated evaluations (on by default)."""
