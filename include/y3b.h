@@ -19,6 +19,9 @@
  *                           average_sigma_crit_inv.py:32-61
  *   y3b_nfw_mis             src/models/nfw_dsigma_mis.hh:95-114 and
  *                           src/models/nfw_sigma_mis.hh:53-66
+ *   y3b_prj_*               src/models/sigma_prj_frozen_t.hh:34-512
+ *                           (ShearPrjFrozenPhysics, module
+ *                           src/modules/sigma_prj_cpu/ShearPrjFrozenPhysics.cc)
  *   y3b_engine_*            the fused fast_mass form of the same integrals
  *                           (NumCountsFastMass / Shear1hFastMass, documented
  *                           as identical to the two modules above), with the
@@ -208,6 +211,53 @@ int y3b_selgl_weights(y3b_selgl* h, double* W, double* norm, double* lnm_eff,
                       double* mu2, double* lnm_x, double* lnm_w);
 int y3b_selgl_n_bins(const y3b_selgl* h);
 void y3b_selgl_destroy(y3b_selgl* h);
+
+/* ---------------------------------------------------------------------- */
+/* Frozen-physics projection shear <DeltaSigma_prj>(R | lambda bin, z_obs) */
+/* (ShearPrjFrozenPhysics, src/models/sigma_prj_frozen_t.hh:34-512).       */
+
+/* Module options (the constructor's keys and defaults). */
+typedef struct {
+  int n_lnm, n_per_seg, n_zring, n_zouter;  /* 24, 10, 20, 20 */
+  double zt_low, zt_high, lnm_low, lnm_high;
+  double R_max_cMpch;                       /* 30 */
+  int include_omega_z;                      /* 1 */
+  int n_lob; const double* lob_centers;     /* NULL: {25, 37.5, 52.5, 130} */
+  int n_gp;                                 /* grid points (wall of numbers): */
+  const int* lambda_bin;                    /*   richness bin                 */
+  const double *zo_low, *zo_high;           /*   z_obs bin edges              */
+  const double* radii;                      /*   R [Mpc/h]                    */
+} y3b_prj_config;
+
+/* One sample: cosmology, the counts' tables (HMF, distances/{z, d_a},
+ * optional average_sigma_crit_inv) and distances/d_c [Mpc] on distances/z,
+ * haloModel/{lnM, z, bias[n_hz][n_hl]}, xi_nl/{r, z, xi_nl[n_xz][n_xr]},
+ * b_sel_marginalised/{lob, zob, b_small, b_large [n_bzob][n_blob]}. */
+typedef struct {
+  y3b_cosmo cosmo;
+  y3b_tables t;
+  const double* dist_dc;
+  int n_hl, n_hz; const double *halo_lnM, *halo_z, *bias;
+  int n_xr, n_xz; const double *xi_r, *xi_z, *xi_nl;
+  int n_blob, n_bzob; const double *bsel_lob, *bsel_zob, *b_small, *b_large;
+} y3b_prj_sample;
+
+typedef struct y3b_prj y3b_prj;
+/* setup(): the grid points and their (richness bin, z_obs) slices. */
+int y3b_prj_create(const y3b_prj_config* cfg, y3b_prj** out);
+/* The single-kernel miscentring table NFW_DSIGMA_MIS reads
+ * (nfw_off_center/table_1000_1e-03_5e+03_{single_logx, single_logxmis,
+ * log_deltasigma_single}.txt), as y3b_selgl_set_mis_table; n_lx = 0
+ * returns to the direct quadrature of the fixed-offset kernel. */
+int y3b_prj_set_mis_table(y3b_prj* h, int n_lx, const double* logx, int n_lxm,
+                          const double* logxmis, const double* log_tab);
+/* set_sample() + evaluate() of every grid point -> out[n_gp][9]: DeltaSigma
+ * total, random, clustered; the tangential shear (times Sigma_crit^-1(z_obs),
+ * 0 without that table) total, random, clustered; and the shear_prj alias of
+ * the shear triple.  Host buffers; Y3B_ERR_DOMAIN if a line-of-sight z node
+ * lies outside distances/z. */
+int y3b_prj_eval(y3b_prj* h, const y3b_prj_sample* s, double* out);
+void y3b_prj_destroy(y3b_prj* h);
 
 /* ---------------------------------------------------------------------- */
 /* <Sigma_crit^-1>(z_l) (average_sigma_crit_inv.py:40-58), host buffers.   */

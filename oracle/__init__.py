@@ -107,6 +107,8 @@ def _declare(L):
     for name in ("y3o_dsigma_mis_unit", "y3o_sigma_mis_unit"):
         getattr(L, name).argtypes = [D, D, I, I, D]
         getattr(L, name).restype = D
+    L.y3o_dsigma_single_unit.argtypes = [D, D, I]
+    L.y3o_dsigma_single_unit.restype = D
     L.y3o_roffset.argtypes = [D, D]
     L.y3o_roffset.restype = D
     L.y3o_shear1h_mis.argtypes = [I, PD, PD, I, PD, I, PD, D, D, I, PD, D, D,

@@ -171,3 +171,72 @@ def nfw_dsigma_mis(data_root, omega_m, r, rmis, lnM):
                                   _p(lnM), _p(out), err, 512)
     _check(rc, err)
     return out
+
+
+class PrjCfg(C.Structure):
+    _fields_ = [("n_lnm", I), ("n_per_seg", I), ("n_zring", I), ("n_zouter", I),
+                ("zt_low", D), ("zt_high", D), ("lnm_low", D), ("lnm_high", D),
+                ("R_max_cMpch", D), ("include_omega_z", I), ("n_lob", I), ("lob_centers", PD),
+                ("n_gp", I), ("lambda_bin", PD), ("zo_low", PD), ("zo_high", PD),
+                ("radii", PD)]
+
+
+class PrjSample(C.Structure):
+    _fields_ = [("nd", I), ("dist_dc", PD), ("n_hl", I), ("n_hz", I), ("halo_lnM", PD),
+                ("halo_z", PD), ("bias", PD), ("n_xr", I), ("n_xz", I), ("xi_r", PD),
+                ("xi_z", PD), ("xi_nl", PD), ("n_blob", I), ("n_bzob", I), ("bsel_lob", PD),
+                ("bsel_zob", PD), ("b_small", PD), ("b_large", PD)]
+
+
+def shear_prj_frozen(cfg, cosmo, tables, prj, grid, data_root):
+    """ShearPrjFrozenPhysics (sigma_prj_frozen_t.hh): cfg dict (zt_low,
+    zt_high, lnm_low, lnm_high and optional n_lnm, n_per_seg, n_zring,
+    n_zouter, R_max_cMpch, include_omega_z, lob_centers); grid dict of the
+    grid-point arrays lambda_bin, zo_low, zo_high, radii; prj the tables of
+    synthetic.prj_tables.  Returns [n_gp, 9]."""
+    L = lib()
+    if not hasattr(L, "_prj_declared"):
+        L.y3r_shear_prj_frozen.argtypes = [C.POINTER(PrjCfg), C.c_char_p, C.POINTER(Sample),
+                                           C.POINTER(PrjSample), PD, C.c_char_p, I]
+        L._prj_declared = True
+    keep = []
+
+    def arr(a):
+        a = _f64(a)
+        keep.append(a)
+        return a
+
+    c = PrjCfg()
+    for k, d in (("n_lnm", 0), ("n_per_seg", 0), ("n_zring", 0), ("n_zouter", 0)):
+        setattr(c, k, int(cfg.get(k, d)))
+    for k in ("zt_low", "zt_high", "lnm_low", "lnm_high"):
+        setattr(c, k, float(cfg[k]))
+    c.R_max_cMpch = float(cfg.get("R_max_cMpch", -1.0))
+    c.include_omega_z = int(cfg.get("include_omega_z", -1))
+    if cfg.get("lob_centers") is not None:
+        lc = arr(cfg["lob_centers"])
+        c.n_lob, c.lob_centers = len(lc), _p(lc)
+    gp = {k: arr(grid[k]) for k in ("lambda_bin", "zo_low", "zo_high", "radii")}
+    c.n_gp = len(gp["radii"])
+    for k, v in gp.items():
+        setattr(c, k, _p(v))
+    inp = _Inputs(cosmo, tables, (np.array([0.0, 1.0]), np.array([0.0, 1.0]),
+                                  np.zeros((1, 2, 2))),
+                  sci=(tables["sci_z"], tables["sci_val"]) if "sci_z" in tables else None)
+    ps = PrjSample()
+    dc = arr(prj["dist_dc"])
+    ps.nd, ps.dist_dc = len(dc), _p(dc)
+    hl, hz, bi = arr(prj["halo_lnM"]), arr(prj["halo_z"]), arr(prj["bias"])
+    ps.n_hl, ps.n_hz, ps.halo_lnM, ps.halo_z, ps.bias = len(hl), len(hz), _p(hl), _p(hz), _p(bi)
+    xr, xz, xn = arr(prj["xi_r"]), arr(prj["xi_z"]), arr(prj["xi_nl"])
+    ps.n_xr, ps.n_xz, ps.xi_r, ps.xi_z, ps.xi_nl = len(xr), len(xz), _p(xr), _p(xz), _p(xn)
+    bl, bz = arr(prj["bsel_lob"]), arr(prj["bsel_zob"])
+    bs, bg = arr(prj["b_small"]), arr(prj["b_large"])
+    ps.n_blob, ps.n_bzob = len(bl), len(bz)
+    ps.bsel_lob, ps.bsel_zob, ps.b_small, ps.b_large = _p(bl), _p(bz), _p(bs), _p(bg)
+    out = np.empty((c.n_gp, 9))
+    err = C.create_string_buffer(512)
+    rc = L.y3r_shear_prj_frozen(C.byref(c), str(data_root).encode(), C.byref(inp.sample),
+                                C.byref(ps), _p(out), err, 512)
+    _check(rc, err)
+    return out

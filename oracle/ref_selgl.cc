@@ -13,6 +13,7 @@
 #include "ref_selgl.h"
 
 #include "models/n_operator_sel_gl_t.hh"
+#include "models/sigma_prj_frozen_t.hh"
 
 #include <cstdio>
 #include <cstdlib>
@@ -198,6 +199,67 @@ y3r_nfw_dsigma_mis(const char* data_root, double omega_m, int n,
     y3_cluster::NFW_DSIGMA_MIS f(4.0, 2.77533742639e+11, y3_cluster::GAMMA);
     f.set_rho_mult(omega_m);
     for (int i = 0; i != n; ++i) out[i] = f(r[i], rmis[i], lnM[i]);
+    return 0;
+  }
+  catch (std::exception const& e) {
+    return fail(err, errlen, e.what());
+  }
+}
+
+int
+y3r_shear_prj_frozen(const y3r_prj_cfg* c, const char* data_root, const y3r_sample* s,
+                     const y3r_prj_sample* ps, double* out, char* err, int errlen)
+{
+  try {
+    set_data_root(data_root);
+    char const* label = y3_cluster::ShearPrjFrozenPhysics::module_label();
+    cosmosis::DataBlock cfg, b;
+    if (c->n_lnm > 0) cfg.put_val(label, "n_lnm", c->n_lnm);
+    if (c->n_per_seg > 0) cfg.put_val(label, "n_per_seg", c->n_per_seg);
+    if (c->n_zring > 0) cfg.put_val(label, "n_zring", c->n_zring);
+    if (c->n_zouter > 0) cfg.put_val(label, "n_zouter", c->n_zouter);
+    cfg.put_val(label, "zt_low", c->zt_low);
+    cfg.put_val(label, "zt_high", c->zt_high);
+    cfg.put_val(label, "lnm_low", c->lnm_low);
+    cfg.put_val(label, "lnm_high", c->lnm_high);
+    if (c->R_max_cMpch >= 0) cfg.put_val(label, "R_max_cMpch", c->R_max_cMpch);
+    if (c->include_omega_z >= 0) cfg.put_val(label, "include_omega_z", c->include_omega_z);
+    if (c->lob_centers) cfg.put_val(label, "lob_centers", vec(c->lob_centers, c->n_lob));
+    cfg.put_val(label, "lambda_bin", vec(c->lambda_bin, c->n_gp));
+    cfg.put_val(label, "zo_low", vec(c->zo_low, c->n_gp));
+    cfg.put_val(label, "zo_high", vec(c->zo_high, c->n_gp));
+    cfg.put_val(label, "radii", vec(c->radii, c->n_gp));
+    put_sample(b, s);
+    b.put_val("distances", "d_c", vec(ps->dist_dc, ps->nd));
+    b.put_val("haloModel", "lnM", vec(ps->halo_lnM, ps->n_hl));
+    b.put_val("haloModel", "z", vec(ps->halo_z, ps->n_hz));
+    b.put_val("haloModel", "bias",
+              cosmosis::ndarray<double>(vec(ps->bias, ps->n_hl * ps->n_hz),
+                                        {static_cast<std::size_t>(ps->n_hz),
+                                         static_cast<std::size_t>(ps->n_hl)}));
+    b.put_val("xi_nl", "r", vec(ps->xi_r, ps->n_xr));
+    b.put_val("xi_nl", "z", vec(ps->xi_z, ps->n_xz));
+    b.put_val("xi_nl", "xi_nl",
+              cosmosis::ndarray<double>(vec(ps->xi_nl, ps->n_xr * ps->n_xz),
+                                        {static_cast<std::size_t>(ps->n_xz),
+                                         static_cast<std::size_t>(ps->n_xr)}));
+    b.put_val("b_sel_marginalised", "lob", vec(ps->bsel_lob, ps->n_blob));
+    b.put_val("b_sel_marginalised", "zob", vec(ps->bsel_zob, ps->n_bzob));
+    int const nbs = ps->n_blob * ps->n_bzob;
+    std::vector<std::size_t> ext{static_cast<std::size_t>(ps->n_bzob),
+                                 static_cast<std::size_t>(ps->n_blob)};
+    b.put_val("b_sel_marginalised", "b_small",
+              cosmosis::ndarray<double>(vec(ps->b_small, nbs), ext));
+    b.put_val("b_sel_marginalised", "b_large",
+              cosmosis::ndarray<double>(vec(ps->b_large, nbs), ext));
+    y3_cluster::ShearPrjFrozenPhysics m(cfg);
+    m.set_sample(b);
+    for (int i = 0; i != c->n_gp; ++i) {
+      y3_cluster::ShearPrjFrozenPhysics::grid_point_t pt{c->lambda_bin[i], c->zo_low[i],
+                                                         c->zo_high[i], c->radii[i]};
+      auto const v = m.evaluate(pt);
+      for (int k = 0; k != 9; ++k) out[(size_t)i * 9 + k] = v[k];
+    }
     return 0;
   }
   catch (std::exception const& e) {

@@ -71,6 +71,33 @@ int y3r_nfw_dsigma_mis(const char* data_root, double omega_m, int n,
                        const double* r, const double* rmis, const double* lnM,
                        double* out, char* err, int errlen);
 
+/* Inputs of the frozen-physics projection shear (ShearPrjFrozenPhysics,
+ * src/models/sigma_prj_frozen_t.hh:34-512) beyond the y3r_sample tables. */
+typedef struct {
+  int n_lnm, n_per_seg, n_zring, n_zouter;  /* <= 0: leave unset (24, 10, 20, 20) */
+  double zt_low, zt_high, lnm_low, lnm_high;
+  double R_max_cMpch;                       /* < 0: unset (30) */
+  int include_omega_z;                      /* < 0: unset (1) */
+  int n_lob; const double* lob_centers;     /* NULL: unset */
+  int n_gp;                                 /* grid points: lambda_bin, zo_low, zo_high, radii */
+  const double *lambda_bin, *zo_low, *zo_high, *radii;
+} y3r_prj_cfg;
+
+typedef struct {
+  int nd; const double* dist_dc;            /* distances/d_c on y3r_sample's distances/z */
+  int n_hl, n_hz; const double *halo_lnM, *halo_z, *bias;      /* bias [n_hz][n_hl] */
+  int n_xr, n_xz; const double *xi_r, *xi_z, *xi_nl;            /* xi_nl [n_xz][n_xr] */
+  int n_blob, n_bzob; const double *bsel_lob, *bsel_zob, *b_small, *b_large;  /* [n_bzob * n_blob] */
+} y3r_prj_sample;
+
+/* ShearPrjFrozenPhysics: set_sample, then evaluate every grid point -> out
+ * [n_gp][9] (dsigma total, rnd, cl; gt total, rnd, cl; the shear_prj alias of
+ * the gt triple).  data_root holds data/nfw_off_center/ with the single-
+ * kernel miscentring table files. */
+int y3r_shear_prj_frozen(const y3r_prj_cfg* cfg, const char* data_root,
+                         const y3r_sample* s, const y3r_prj_sample* ps, double* out,
+                         char* err, int errlen);
+
 #ifdef __cplusplus
 }
 #endif

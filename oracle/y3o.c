@@ -1028,3 +1028,26 @@ y3o_loglike(int n_bins, int n_R, const double* nc, const double* s1h,
   free(d);
   return -0.5 * chi2;
 }
+
+/* Miscentred Delta Sigma for an offset fixed at x_mis (the "single" kernel
+ * of NFW_DSIGMA_MIS, nfw_dsigma_mis.hh:53-55): the mean tangential shear on
+ * the circle of radius x around the offset centre,
+ *   (1/pi) int_0^pi dth DSigma(d) cos 2phi,  d^2 = x^2 + x_mis^2 - 2 x x_mis cos th,
+ * in units of 2 r_s delta_c rho; n_theta GL nodes on [0, pi]. */
+double
+y3o_dsigma_single_unit(double x, double xmis, int n_theta)
+{
+  double* th = (double*)malloc(sizeof(double) * n_theta);
+  double* wth = (double*)malloc(sizeof(double) * n_theta);
+  y3o_gl_nodes(0.0, M_PI, n_theta, th, wth);
+  double acc = 0.0;
+  for (int t = 0; t < n_theta; ++t) {
+    double ct = cos(th[t]);
+    double d2 = x * x + xmis * xmis - 2.0 * x * xmis * ct;
+    double a = x - xmis * ct;
+    acc += wth[t] * y3o_nfw_dsigma_unit(sqrt(d2)) * (2.0 * a * a / d2 - 1.0);
+  }
+  free(th);
+  free(wth);
+  return acc / M_PI;
+}

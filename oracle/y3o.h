@@ -89,6 +89,7 @@ double y3o_dsigma_mis_unit(double x, double xmis, int n_theta, int n_s,
 double y3o_sigma_mis_unit(double x, double xmis, int n_theta, int n_s,
                           double s_max);
 double y3o_roffset(double x, double tau);
+double y3o_dsigma_single_unit(double x, double xmis, int n_theta);
 void   y3o_mis_s_nodes(double x, double xmis, int n_s, double s_max,
                        double* sn, double* wsn);
 

@@ -33,6 +33,11 @@ What it writes (tests/golden/*.npz / *.json):
   y3_buzzard/likelihood_cp.py setup/execute on a seeded mock data vector
   (12 counts, 12 x 10 shear; diagonal and dense inverse covariances; linear
   and log space) for four seeded theory blocks.
+* prj_ref.npz -- the nine outputs of the reference's ShearPrjFrozenPhysics
+  (src/models/sigma_prj_frozen_t.hh, compiled by `make -C oracle ref`) for
+  12 slices x 10 radii on the fiducial synthetic tables (counts' tables plus
+  comoving distance, halo bias, xi_NL and the selection-bias asymptotes of
+  synthetic.prj_tables), with a stand-in single-kernel miscentring table.
 * selgl_ref.npz -- numcountssel/vals, SelGLCore weights and
   shear1hmissel/vals (exact and idea2) from the reference's own C++
   (src/models/n_operator_sel_gl_t.hh:75-361), compiled from its sources by
@@ -387,6 +392,53 @@ def likelihood_reference(ref):
     return out
 
 
+def prj_reference(ref):
+    """Runs the reference's compiled ShearPrjFrozenPhysics on the fiducial
+    synthetic tables: 12 (richness, z_obs) slices x 10 radii 0.2-5 Mpc/h,
+    default options.  The single-kernel miscentring table it reads is missing
+    from the snapshot; the fixture carries a stand-in on every 8th ln x and
+    every 5th ln x_mis node of the shipped single-kernel axis files, filled
+    by the oracle's ring average of the NFW profile (256 GL nodes)."""
+    import oracle as O
+    from oracle import ref as R
+    from y3_cluster_cpp_b200 import synthetic
+
+    p = synthetic.fiducial()
+    prj = synthetic.prj_tables(p, n_r=120)
+    cosmo = dict(omega_m=p.om, omega_nu=0.0, omega_lambda=1.0 - p.om, omega_k=0.0, h0=p.h0,
+                 hmf_s=0.0, hmf_q=1.0)
+    axes = os.path.join(ref, "data", "nfw_off_center", "table_1000_1e-03_5e+03_single_")
+    lx_full = np.loadtxt(axes + "logx.txt")
+    lxm_full = np.loadtxt(axes + "logxmis.txt")
+    logx = lx_full[np.r_[0:len(lx_full):8, len(lx_full) - 1]]
+    logxmis = lxm_full[np.r_[0:len(lxm_full):5, len(lxm_full) - 1]]
+    tab = np.array([[np.log(max(O.lib().y3o_dsigma_single_unit(np.exp(a), np.exp(b), 256), 1e-30))
+                     for a in logx] for b in logxmis])
+    R10 = np.logspace(np.log10(0.2), np.log10(5.0), 10)
+    grid = dict(lambda_bin=np.repeat(np.tile(np.arange(4), 3), 10).astype(float),
+                zo_low=np.repeat(np.repeat([0.2, 0.35, 0.5], 4), 10),
+                zo_high=np.repeat(np.repeat([0.35, 0.5, 0.65], 4), 10),
+                radii=np.tile(R10, 12))
+    cfg = dict(zt_low=0.1, zt_high=0.8, lnm_low=np.log(1e13), lnm_high=np.log(10 ** 15.5))
+    out = dict(omega_m=p.om, h0=p.h0, **{"t_" + k: np.asarray(v) for k, v in p.tables.items()},
+               **{"prj_" + k: np.asarray(v) for k, v in prj.items()},
+               **{"gp_" + k: v for k, v in grid.items()},
+               **{"cfg_" + k: v for k, v in cfg.items()},
+               single_logx=logx, single_logxmis=logxmis, single_log_tab=tab)
+    with tempfile.TemporaryDirectory() as d:
+        dd = os.path.join(d, "data", "nfw_off_center")
+        os.makedirs(dd)
+        stem = os.path.join(dd, "table_1000_1e-03_5e+03_")
+        np.savetxt(stem + "single_logx.txt", logx, fmt="%.17g")
+        np.savetxt(stem + "single_logxmis.txt", logxmis, fmt="%.17g")
+        np.savetxt(stem + "log_deltasigma_single.txt", np.ravel(tab), fmt="%.17g")
+        out["vals"] = R.shear_prj_frozen(cfg, cosmo, p.tables, prj, grid, d)
+        out["vals_no_omega"] = R.shear_prj_frozen(dict(cfg, include_omega_z=0, n_lnm=16,
+                                                       n_per_seg=8), cosmo, p.tables, prj,
+                                                  grid, d)
+    return out
+
+
 class _OptionsIndex(dict):
     """options[section, key] and options.get_bool(section, key, default)."""
 
@@ -419,6 +471,7 @@ def main(ref=None):
     np.savez_compressed(os.path.join(HERE, "sigma_crit_inv.npz"), **sigma_crit_inv_reference(ref))
     np.savez_compressed(os.path.join(HERE, "selgl_ref.npz"), **selgl_reference(ref))
     np.savez_compressed(os.path.join(HERE, "likelihood_ref.npz"), **likelihood_reference(ref))
+    np.savez_compressed(os.path.join(HERE, "prj_ref.npz"), **prj_reference(ref))
     print("wrote golden fixtures to", HERE)
 
 

@@ -1,0 +1,89 @@
+"""The frozen-physics projection shear (ShearPrjFrozenPhysics) on the GPU
+against the reference's own compiled class: the golden vectors of
+tests/golden/prj_ref.npz (written by tests/golden/make_golden.py) and, where
+the compiled reference library is present, the library itself on further
+walkers.  FP64 throughout; tolerance 1e-8 relative (observed ~1e-13)."""
+import os
+
+import numpy as np
+import pytest
+
+from y3_cluster_cpp_b200 import engine as E
+from y3_cluster_cpp_b200 import synthetic
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+TOL = 1e-8
+
+
+def _golden():
+    return np.load(os.path.join(GOLD, "prj_ref.npz"))
+
+
+def _inputs(g):
+    t = {k[2:]: g[k] for k in g.files if k.startswith("t_")}
+    prj = {k[4:]: g[k] for k in g.files if k.startswith("prj_")}
+    grid = {k[3:]: g[k] for k in g.files if k.startswith("gp_")}
+    grid["lambda_bin"] = grid["lambda_bin"].astype(int)
+    cfg = {k[4:]: float(g[k]) for k in g.files if k.startswith("cfg_")}
+    return t, prj, grid, cfg
+
+
+def _check(out, ref):
+    scale = np.max(np.abs(ref), axis=0)
+    np.testing.assert_allclose(out, ref, rtol=TOL, atol=TOL * 1e-3 * np.max(scale))
+
+
+@pytest.mark.parametrize("variant", ["default", "no_omega"])
+def test_prj_matches_compiled_reference_golden(gpu, variant):
+    g = _golden()
+    t, prj, grid, cfg = _inputs(g)
+    kw = dict(cfg)
+    if variant == "no_omega":
+        kw.update(include_omega_z=False, n_lnm=16, n_per_seg=8)
+    h = E.PrjShear(grid, **kw)
+    h.set_mis_table(g["single_logx"], g["single_logxmis"], g["single_log_tab"])
+    out = h.eval(E.cosmo(float(g["omega_m"]), float(g["h0"])), t, prj)
+    ref = g["vals" if variant == "default" else "vals_no_omega"]
+    assert np.all(np.isfinite(out)) and np.max(np.abs(ref[:, 0])) > 0
+    _check(out, ref)
+    # a second sample on the same handle
+    out2 = h.eval(E.cosmo(float(g["omega_m"]), float(g["h0"])), t, prj)
+    np.testing.assert_array_equal(out, out2)
+    h.close()
+
+
+def test_prj_quadrature_tracks_the_table(gpu):
+    """Without a table the single-kernel profile is integrated directly; it
+    agrees with the interpolated stand-in table to the table's own
+    interpolation error."""
+    g = _golden()
+    t, prj, grid, cfg = _inputs(g)
+    h = E.PrjShear(grid, **cfg)
+    out = h.eval(E.cosmo(float(g["omega_m"]), float(g["h0"])), t, prj)
+    ref = g["vals"]
+    np.testing.assert_allclose(out[:, :3], ref[:, :3], rtol=2e-2)
+    h.close()
+
+
+def test_prj_matches_live_reference_on_walkers(gpu, tmp_path):
+    from oracle import ref as R
+    if not R.available():
+        pytest.skip("compiled reference (make -C oracle ref) absent")
+    g = _golden()
+    _, _, grid, cfg = _inputs(g)
+    d = tmp_path / "data" / "nfw_off_center"
+    d.mkdir(parents=True)
+    stem = str(d / "table_1000_1e-03_5e+03_")
+    np.savetxt(stem + "single_logx.txt", g["single_logx"], fmt="%.17g")
+    np.savetxt(stem + "single_logxmis.txt", g["single_logxmis"], fmt="%.17g")
+    np.savetxt(stem + "log_deltasigma_single.txt", np.ravel(g["single_log_tab"]), fmt="%.17g")
+    h = E.PrjShear(grid, **cfg)
+    h.set_mis_table(g["single_logx"], g["single_logxmis"], g["single_log_tab"])
+    for p in synthetic.walkers(3, seed=4, densities=(1,)):
+        prj = synthetic.prj_tables(p, n_r=120)
+        cosmo = dict(omega_m=p.om, omega_nu=0.0, omega_lambda=1 - p.om, omega_k=0.0, h0=p.h0,
+                     hmf_s=0.0, hmf_q=1.0)
+        ref = R.shear_prj_frozen(cfg, cosmo, p.tables, prj, grid, str(tmp_path))
+        _check(h.eval(E.cosmo(p.om, p.h0), p.tables, prj), ref)
+    h.close()

@@ -114,6 +114,22 @@ class Likelihood(C.Structure):
                 ("shear_prj", PD)]
 
 
+class PrjConfig(C.Structure):
+    _fields_ = [("n_lnm", I), ("n_per_seg", I), ("n_zring", I), ("n_zouter", I),
+                ("zt_low", D), ("zt_high", D), ("lnm_low", D), ("lnm_high", D),
+                ("R_max_cMpch", D), ("include_omega_z", I), ("n_lob", I), ("lob_centers", PD),
+                ("n_gp", I), ("lambda_bin", PI), ("zo_low", PD), ("zo_high", PD),
+                ("radii", PD)]
+
+
+class PrjSample(C.Structure):
+    _fields_ = [("cosmo", Cosmo), ("t", Tables), ("dist_dc", PD),
+                ("n_hl", I), ("n_hz", I), ("halo_lnM", PD), ("halo_z", PD), ("bias", PD),
+                ("n_xr", I), ("n_xz", I), ("xi_r", PD), ("xi_z", PD), ("xi_nl", PD),
+                ("n_blob", I), ("n_bzob", I), ("bsel_lob", PD), ("bsel_zob", PD),
+                ("b_small", PD), ("b_large", PD)]
+
+
 class ServerStats(C.Structure):
     _fields_ = [("requests_done", C.c_longlong), ("points_done", C.c_longlong),
                 ("launches", C.c_longlong), ("max_launch_points", I), ("pool_points", I),
@@ -200,6 +216,11 @@ def _declare(L):
     L.y3b_engine_loglike.argtypes = [VP, I, PD, VP]
     L.y3b_engine_eval_loglike.argtypes = [VP, I, I, C.POINTER(Point), PD, PD]
     L.y3b_gaussian_loglike.argtypes = [C.POINTER(Likelihood), PD, PD, PD]
+    L.y3b_prj_create.argtypes = [C.POINTER(PrjConfig), C.POINTER(VP)]
+    L.y3b_prj_set_mis_table.argtypes = [VP, I, PD, I, PD, PD]
+    L.y3b_prj_eval.argtypes = [VP, C.POINTER(PrjSample), PD]
+    L.y3b_prj_destroy.argtypes = [VP]
+    L.y3b_prj_destroy.restype = None
     L.y3b_engine_profile.argtypes = [VP, I]
     L.y3b_engine_profile_read.argtypes = [VP, PD, PI]
 
@@ -238,5 +259,6 @@ EXPORTED = [
     "y3b_planner_destroy", "y3b_planner_submit", "y3b_planner_admit",
     "y3b_planner_next_batch", "y3b_planner_complete", "y3b_planner_cancel",
     "y3b_planner_free_points", "y3b_engine_set_likelihood", "y3b_engine_loglike",
-    "y3b_engine_eval_loglike", "y3b_gaussian_loglike",
+    "y3b_engine_eval_loglike", "y3b_gaussian_loglike", "y3b_prj_create",
+    "y3b_prj_set_mis_table", "y3b_prj_eval", "y3b_prj_destroy",
 ]

@@ -175,6 +175,72 @@ def gaussian_loglike(spec, counts, shear_1h=None):
     return out.value
 
 
+class PrjShear:
+    """Frozen-physics projection shear (ShearPrjFrozenPhysics): the grid
+    points (lambda_bin, zo_low, zo_high, radii) are fixed at construction,
+    eval() takes one sample's tables and returns [n_gp, 9]."""
+
+    def __init__(self, grid, zt_low=0.1, zt_high=0.8, lnm_low=np.log(1e13),
+                 lnm_high=np.log(10 ** 15.5), n_lnm=24, n_per_seg=10, n_zring=20, n_zouter=20,
+                 R_max_cMpch=30.0, include_omega_z=True, lob_centers=None):
+        self._keep = [np.ascontiguousarray(np.asarray(grid["lambda_bin"], dtype=np.int32))]
+        self._keep += [f64(grid[k]) for k in ("zo_low", "zo_high", "radii")]
+        c = A.PrjConfig()
+        c.n_lnm, c.n_per_seg, c.n_zring, c.n_zouter = n_lnm, n_per_seg, n_zring, n_zouter
+        c.zt_low, c.zt_high, c.lnm_low, c.lnm_high = zt_low, zt_high, lnm_low, lnm_high
+        c.R_max_cMpch, c.include_omega_z = R_max_cMpch, int(bool(include_omega_z))
+        if lob_centers is not None:
+            lc = f64(lob_centers)
+            self._keep.append(lc)
+            c.n_lob, c.lob_centers = len(lc), ptr(lc)
+        c.n_gp = len(self._keep[0])
+        c.lambda_bin = ptr(self._keep[0])
+        c.zo_low, c.zo_high, c.radii = (ptr(a) for a in self._keep[1:4])
+        h = C.c_void_p()
+        check(lib().y3b_prj_create(C.byref(c), C.byref(h)))
+        self._h = h
+        self.n_gp = c.n_gp
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().y3b_prj_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def set_mis_table(self, logx=None, logxmis=None, log_tab=None):
+        if logx is None:
+            check(lib().y3b_prj_set_mis_table(self._h, 0, None, 0, None, None))
+            return self
+        lx, lxm, tv = f64(logx), f64(logxmis), f64(log_tab)
+        check(lib().y3b_prj_set_mis_table(self._h, len(lx), ptr(lx), len(lxm), ptr(lxm),
+                                          ptr(tv)))
+        return self
+
+    def eval(self, cz, tables, prj):
+        keep = [f64(tables[k]) for k in ("hmf_m_h", "hmf_z", "dndlnmh", "dist_z", "dist_da")]
+        sci = [f64(tables["sci_z"]), f64(tables["sci_val"])] if "sci_z" in tables else None
+        t = A.Tables(len(keep[0]), ptr(keep[0]), len(keep[1]), ptr(keep[1]), ptr(keep[2]),
+                     len(keep[3]), ptr(keep[3]), ptr(keep[4]),
+                     len(sci[0]) if sci else 0, ptr(sci[0]) if sci else None,
+                     ptr(sci[1]) if sci else None)
+        s = A.PrjSample()
+        s.cosmo, s.t = cz, t
+        arrs = {k: f64(prj[k]) for k in ("dist_dc", "halo_lnM", "halo_z", "bias", "xi_r", "xi_z",
+                                         "xi_nl", "bsel_lob", "bsel_zob", "b_small", "b_large")}
+        s.dist_dc = ptr(arrs["dist_dc"])
+        s.n_hl, s.n_hz = len(arrs["halo_lnM"]), len(arrs["halo_z"])
+        s.halo_lnM, s.halo_z, s.bias = ptr(arrs["halo_lnM"]), ptr(arrs["halo_z"]), ptr(arrs["bias"])
+        s.n_xr, s.n_xz = len(arrs["xi_r"]), len(arrs["xi_z"])
+        s.xi_r, s.xi_z, s.xi_nl = ptr(arrs["xi_r"]), ptr(arrs["xi_z"]), ptr(arrs["xi_nl"])
+        s.n_blob, s.n_bzob = len(arrs["bsel_lob"]), len(arrs["bsel_zob"])
+        s.bsel_lob, s.bsel_zob = ptr(arrs["bsel_lob"]), ptr(arrs["bsel_zob"])
+        s.b_small, s.b_large = ptr(arrs["b_small"]), ptr(arrs["b_large"])
+        out = np.empty((self.n_gp, 9))
+        check(lib().y3b_prj_eval(self._h, C.byref(s), ptr(out)))
+        return out
+
+
 def sigma_crit_inv(zl, zs, pz, delta_z, h0, dist_z, dist_da):
     zl, zs, pz, dz, da = map(f64, (zl, zs, pz, dist_z, dist_da))
     out = np.empty(len(zl))

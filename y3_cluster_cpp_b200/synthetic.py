@@ -159,6 +159,32 @@ def make_tables(p: Point, with_sci=True):
     return t
 
 
+def prj_tables(p: Point, n_m=60, n_z=40, n_r=200):
+    """Tables the projection-shear observable reads besides the counts'
+    ones (seeded synthetic, smooth): comoving distance distances/d_c [Mpc],
+    the linear halo bias haloModel/{lnM, z, bias [n_z, n_m]} (peak-background
+    split of the synthetic sigma(M, z)), the nonlinear correlation function
+    xi_nl/{r [Mpc/h], z, xi_nl [n_z, n_r]} (power law (r / 5)^-1.8 D(z)^2 with
+    an exponential cut at 200 Mpc/h) and the selection-bias asymptotes
+    b_sel_marginalised/{lob, zob, b_small, b_large [n_zob x n_lob]}."""
+    dz, da = p.tables["dist_z"], p.tables["dist_da"]
+    lnM = np.linspace(np.log(1e12), np.log(10 ** 16), n_m)
+    z = np.linspace(0.0, 1.2, n_z)
+    dc = 1.686
+    sig = p.sigma8 * (np.exp(lnM)[None, :] / 2e14) ** -0.2 * growth(z, p.om)[:, None]
+    nu = dc / sig
+    bias = 1.0 + (nu * nu - 1.0) / dc
+    r = np.logspace(-2, np.log10(5000.0), n_r)
+    xi = (r[None, :] / 5.0) ** -1.8 * np.exp(-r[None, :] / 200.0) * growth(z, p.om)[:, None] ** 2
+    lob = np.array([25.0, 37.5, 52.5, 130.0])
+    zob = np.array([0.275, 0.425, 0.575])
+    b_small = 1.0 + 0.1 * np.arange(4)[None, :] + 0.2 * zob[:, None]
+    b_large = 2.0 + 0.3 * np.arange(4)[None, :] + 0.5 * zob[:, None]
+    return dict(dist_dc=da * (1 + dz), halo_lnM=lnM, halo_z=z, bias=bias, xi_r=r, xi_z=z,
+                xi_nl=xi, bsel_lob=lob, bsel_zob=zob, b_small=b_small.ravel(),
+                b_large=b_large.ravel())
+
+
 def fiducial(density=1, with_sci=True) -> Point:
     p = Point(density=density)
     p.tables = make_tables(p, with_sci)
