@@ -101,3 +101,22 @@ def test_fused_module_setup_validates_bins_on_cpu():
     assert not Module("NumCountsFastMass").setup(opts(sigma_z=[0.03] * 11 + [0.05]))
     assert not Module("NumCountsFastMass").setup(opts(bin_index=np.arange(13)))
     assert not Module("Shear1hFastMass").setup(opts())       # counts only
+
+
+def test_prj_module_rejects_incomplete_options_on_cpu():
+    """ShearPrjFrozenPhysics.so setup checks its options before any device
+    work: missing box or mismatched grid arrays give NULL, never a throw."""
+    import numpy as np
+    from y3_cluster_cpp_b200.cosmosis import DataBlock, Module
+    lab = "shear_prj_frozen_physics"
+    o = DataBlock()
+    o[lab, "lambda_bin"] = np.arange(3, dtype=np.int32)
+    o[lab, "zo_low"] = np.full(3, 0.2)
+    o[lab, "zo_high"] = np.full(3, 0.35)
+    o[lab, "radii"] = np.array([0.5, 1.0])           # one short
+    for k, v in dict(zt_low=0.1, zt_high=0.8, lnm_low=29.9, lnm_high=35.7).items():
+        o[lab, k] = v
+    assert not Module("ShearPrjFrozenPhysics").setup(o)
+    o2 = DataBlock()
+    o2[lab, "radii"] = np.array([0.5])
+    assert not Module("ShearPrjFrozenPhysics").setup(o2)   # no box, no grid

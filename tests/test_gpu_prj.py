@@ -87,3 +87,58 @@ def test_prj_matches_live_reference_on_walkers(gpu, tmp_path):
         ref = R.shear_prj_frozen(cfg, cosmo, p.tables, prj, grid, str(tmp_path))
         _check(h.eval(E.cosmo(p.om, p.h0), p.tables, prj), ref)
     h.close()
+
+
+def test_prj_module_setup_execute_matches_golden(gpu, tmp_path, monkeypatch):
+    """ShearPrjFrozenPhysics.so through setup / execute / cleanup on a
+    DataBlock, reading the single-kernel table from $Y3_CLUSTER_CPP_DIR as the
+    reference does: all nine output arrays against the compiled reference."""
+    from y3_cluster_cpp_b200.cosmosis import DataBlock, Module
+    g = _golden()
+    t, prj, grid, cfg = _inputs(g)
+    d = tmp_path / "data" / "nfw_off_center"
+    d.mkdir(parents=True)
+    stem = str(d / "table_1000_1e-03_5e+03_")
+    np.savetxt(stem + "single_logx.txt", g["single_logx"], fmt="%.17g")
+    np.savetxt(stem + "single_logxmis.txt", g["single_logxmis"], fmt="%.17g")
+    np.savetxt(stem + "log_deltasigma_single.txt", np.ravel(g["single_log_tab"]), fmt="%.17g")
+    monkeypatch.setenv("Y3_CLUSTER_CPP_DIR", str(tmp_path))
+    lab = "shear_prj_frozen_physics"
+    o = DataBlock()
+    for k, v in cfg.items():
+        o[lab, k] = v
+    o[lab, "lambda_bin"] = grid["lambda_bin"].astype(np.int32)
+    for k in ("zo_low", "zo_high", "radii"):
+        o[lab, k] = grid[k]
+    o[lab, "mis_profile"] = "table"
+    b = DataBlock()
+    om, h0 = float(g["omega_m"]), float(g["h0"])
+    for k, v in dict(omega_M=om, omega_lambda=1 - om, omega_k=0.0, h0=h0, omega_nu=0.0).items():
+        b["cosmological_parameters", k] = v
+    b["cluster_abundance", "hmf_s"] = 0.0
+    b["cluster_abundance", "hmf_q"] = 1.0
+    b["mass_function", "m_h"], b["mass_function", "z"] = t["hmf_m_h"], t["hmf_z"]
+    b["mass_function", "dndlnmh"] = t["dndlnmh"]
+    b["distances", "z"], b["distances", "d_a"] = t["dist_z"], t["dist_da"]
+    b["distances", "d_c"] = prj["dist_dc"]
+    b["average_sigma_crit_inv", "zlense"] = t["sci_z"]
+    b["average_sigma_crit_inv", "sci_average"] = t["sci_val"]
+    b["haloModel", "lnM"], b["haloModel", "z"] = prj["halo_lnM"], prj["halo_z"]
+    b["haloModel", "bias"] = prj["bias"]
+    b["xi_nl", "r"], b["xi_nl", "z"], b["xi_nl", "xi_nl"] = prj["xi_r"], prj["xi_z"], prj["xi_nl"]
+    b["b_sel_marginalised", "lob"] = prj["bsel_lob"]
+    b["b_sel_marginalised", "zob"] = prj["bsel_zob"]
+    nz, nl = len(prj["bsel_zob"]), len(prj["bsel_lob"])
+    b["b_sel_marginalised", "b_small"] = prj["b_small"].reshape(nz, nl)
+    b["b_sel_marginalised", "b_large"] = prj["b_large"].reshape(nz, nl)
+    m = Module("ShearPrjFrozenPhysics")
+    assert m.setup(o)
+    assert m.execute(b) == 0
+    ref = g["vals"]
+    cols = [("dsigma_prj_frozen_physics", "vals"), ("dsigma_prj_frozen_physics", "rnd"),
+            ("dsigma_prj_frozen_physics", "cl"), ("shear_prj_frozen_physics", "vals"),
+            ("shear_prj_frozen_physics", "rnd"), ("shear_prj_frozen_physics", "cl"),
+            ("shear_prj", "vals"), ("shear_prj", "rnd"), ("shear_prj", "cl")]
+    out = np.stack([b[s, n] for s, n in cols], axis=1)
+    _check(out, ref)
+    assert m.cleanup() == 0
