@@ -461,6 +461,35 @@ def module_latency(n_calls=40):
                 "sel_function S_stack tabulation (upstream module)": 215.0}}
 
 
+def prj_latency(n_calls=30):
+    """Per-sample latency of the frozen-physics projection shear
+    (y3b_prj_eval: host grids, table upload, device sums, 12 slices x 10
+    radii, default options, direct single-kernel quadrature), next to the
+    reference's published 82 ms per sample."""
+    import numpy as np
+
+    from y3_cluster_cpp_b200 import engine, synthetic
+    p = synthetic.fiducial()
+    prj = synthetic.prj_tables(p)
+    R10 = np.logspace(np.log10(0.2), np.log10(5.0), 10)
+    grid = dict(lambda_bin=np.repeat(np.tile(np.arange(4), 3), 10),
+                zo_low=np.repeat(np.repeat([0.2, 0.35, 0.5], 4), 10),
+                zo_high=np.repeat(np.repeat([0.35, 0.5, 0.65], 4), 10), radii=np.tile(R10, 12))
+    h = engine.PrjShear(grid)
+    cz = engine.cosmo(p.om, p.h0)
+    for _ in range(3):
+        h.eval(cz, p.tables, prj)
+    ts = []
+    for _ in range(n_calls):
+        t0 = time.perf_counter()
+        h.eval(cz, p.tables, prj)
+        ts.append(time.perf_counter() - t0)
+    h.close()
+    return {"observable": "ShearPrjFrozenPhysics, 12 slices x 10 radii, 24 lnM nodes",
+            "ms_per_sample": 1e3 * statistics.median(ts), "calls": n_calls,
+            "reference_published_ms": 82.0}
+
+
 def serving_run(a, rank, dev):
     """Serving workload: a Poisson request stream (mean gap 2 ms) of requests
     of 1..1024 points (log-uniform), points from the batched-config prior at
@@ -712,6 +741,7 @@ def run_ours(a):
     if a.serve_requests > 0:
         serving = serving_run(a, rank, dev)
     modlat = module_latency() if a.extra_workloads else None
+    prjlat = prj_latency() if a.extra_workloads else None
     extra = None
     if a.extra_workloads:
         from y3_cluster_cpp_b200 import synthetic as _syn
@@ -768,6 +798,8 @@ def run_ours(a):
             line["serving"] = serving
         if modlat is not None:
             line["module_execute"] = modlat
+        if prjlat is not None:
+            line["projection_shear"] = prjlat
         if extra is not None:
             line["other_workloads"] = extra
         if cpu is not None:
