@@ -732,9 +732,36 @@ def run_ours(a):
         engine.check(lib.y3b_engine_eval(eng.handle, engine.MIXED, B, PPt, TPt, CPt, None))
         e2e_t.append(time.perf_counter() - t_0)
     e2e_total = sharding.max_over_ranks(sum(e2e_t), dev)
-    e2e_value = world * B * len(e2e_t) / e2e_total
-    h2d = B * (C.sizeof(_capi.Point) + eng.stride * 8)
+    e2e64_value = world * B * len(e2e_t) / e2e_total
+    h2d64 = B * (C.sizeof(_capi.Point) + eng.stride * 8)
     d2h = B * n_bins * 8
+    # The same through an engine whose packed tables carry the HMF grid in
+    # FP32: the mixed form rounds that grid to FP32 on the device anyway, so
+    # its counts equal those above (up to the autotuner's choice of tile,
+    # which changes FP32 rounding only), for about half the bytes per point.
+    eng32 = engine.Engine([g], len(t0["hmf_m_h"]), len(t0["hmf_z"]), len(t0["dist_z"]),
+                          (pz, pc), max_points=B, n_sci=len(t0["sci_z"]), hmf_fp32=True)
+    tab32 = eng32.pack(uniq)
+    tables32_h = torch.empty((B, eng32.stride), dtype=torch.float64, pin_memory=True)
+    tables32_h.numpy()[:] = tab32[np.arange(B) % len(uniq)]
+    counts32_h = torch.empty((B, n_bins), dtype=torch.float64, pin_memory=True)
+    TPt32 = C.cast(C.c_void_p(tables32_h.data_ptr()), _capi.PD)
+    CPt32 = C.cast(C.c_void_p(counts32_h.data_ptr()), _capi.PD)
+    tables32_d = tables32_h.to(dev)
+    eng32.autotune(B, pts_d.data_ptr(), tables32_d.data_ptr(), counts_d.data_ptr())
+    del tables32_d
+    for _ in range(2):
+        engine.check(lib.y3b_engine_eval(eng32.handle, engine.MIXED, B, PPt, TPt32, CPt32, None))
+    diff32 = float(np.max(np.abs(counts32_h.numpy() / counts_h.numpy() - 1)))
+    e2e_t = []
+    for _ in range(max(3, a.steps // 2)):
+        t_0 = time.perf_counter()
+        engine.check(lib.y3b_engine_eval(eng32.handle, engine.MIXED, B, PPt, TPt32, CPt32, None))
+        e2e_t.append(time.perf_counter() - t_0)
+    e2e_total = sharding.max_over_ranks(sum(e2e_t), dev)
+    e2e_value = world * B * len(e2e_t) / e2e_total
+    h2d = B * (C.sizeof(_capi.Point) + eng32.stride * 8)
+    eng32.close()
 
     eng.close()
     serving = None
@@ -790,7 +817,11 @@ def run_ours(a):
                          "avg_launch_ms": gemm_ms},
             "stage_share": stage_share,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h,
+                    "tables": "per point, HMF grid in FP32 (hmf_fp32), pinned host",
+                    "max_rel_diff_vs_fp64_tables": diff32},
+            "e2e_fp64_tables": {"value": e2e64_value, "unit": UNIT, "h2d_bytes_per_step": h2d64,
+                                "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "clocks": clk,
         }

@@ -309,6 +309,10 @@ typedef struct {
   size_t hbm_budget;                    /* bytes of device memory the engine may hold (0: 150 GB) */
   int with_shear;
   y3b_shear_opts shear;
+  int hmf_fp32;                         /* 1: the packed tables carry mass_function/dndlnmh
+                                           in FP32 (the mixed form rounds it to FP32 on the
+                                           device anyway, so its results do not change);
+                                           such an engine evaluates the mixed form only */
 } y3b_engine_config;
 
 typedef struct {
@@ -329,7 +333,8 @@ int y3b_engine_create(const y3b_grid* grids, int n_grids,
 void y3b_engine_destroy(y3b_engine* e);
 /* Doubles per point in the packed table buffer (each section 16-byte
  * aligned): hmf_m_h[n_hm] | hmf_z[n_hz] | dndlnmh[n_hz*n_hm] | dist_z[n_dist]
- * | dist_da[n_dist] | sci_z[n_sci] | sci_val[n_sci]. */
+ * | dist_da[n_dist] | sci_z[n_sci] | sci_val[n_sci]; with hmf_fp32 the
+ * dndlnmh section holds n_hz*n_hm floats (half as many doubles). */
 size_t y3b_engine_table_stride(const y3b_engine* e);
 /* Offsets (in doubles) of the seven sections inside one point's block. */
 int y3b_engine_table_offsets(const y3b_engine* e, size_t* off7);

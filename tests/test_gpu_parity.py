@@ -539,3 +539,28 @@ def test_engine_fused_likelihood(gpu, dense, log_space):
         np.testing.assert_array_equal(out, ll)
     eng.set_likelihood(None)
     eng.close()
+
+
+def test_engine_fp32_hmf_tables_give_identical_mixed_results(gpu):
+    """An engine whose packed tables carry the HMF grid in FP32 (half the
+    bytes per point on the host-to-device path) returns bitwise the mixed-form
+    results of the FP64-table engine, which rounds the grid to FP32 on the
+    device; its FP64 form is refused."""
+    grids = [synthetic.grid(d) for d in (1, 2, 4)]
+    pts = synthetic.walkers(6, seed=12)
+    gi = {1: 0, 2: 1, 4: 2}
+    t = pts[0].tables
+    pz, pc = synthetic.plob_baseline()
+    e64 = E.Engine(grids, len(t["hmf_m_h"]), len(t["hmf_z"]), len(t["dist_z"]), (pz, pc),
+                   max_points=8, n_sci=len(t["sci_z"]))
+    e32 = E.Engine(grids, len(t["hmf_m_h"]), len(t["hmf_z"]), len(t["dist_z"]), (pz, pc),
+                   max_points=8, n_sci=len(t["sci_z"]), hmf_fp32=True)
+    assert e32.stride < e64.stride
+    a = e64.eval(pts, E.MIXED, grid_of=lambda p: gi[p.density])["counts"]
+    b = e32.eval(pts, E.MIXED, grid_of=lambda p: gi[p.density])["counts"]
+    np.testing.assert_array_equal(a, b)
+    with pytest.raises(E.A.Y3BError) as ex:
+        e32.eval(pts, E.FP64, grid_of=lambda p: gi[p.density])
+    assert ex.value.status == 1
+    e64.close()
+    e32.close()

@@ -94,7 +94,7 @@ class ShearOpts(C.Structure):
 class EngineConfig(C.Structure):
     _fields_ = [("n_hm", I), ("n_hz", I), ("n_dist", I), ("n_sci", I), ("plob", Plob),
                 ("max_points", I), ("hbm_budget", C.c_size_t), ("with_shear", I),
-                ("shear", ShearOpts)]
+                ("shear", ShearOpts), ("hmf_fp32", I)]
 
 
 class Point(C.Structure):

@@ -231,7 +231,15 @@ prep_kernel(PrepArgs a)
   // FP32 copy of the HMF grid for the mixed form, straight from global memory
   // while the bulk copy of the small tables is in flight (four loads in
   // flight per thread).
-  if (a.mixed) {
+  if (a.mixed && L.hmf_f32) {  // already FP32 in the packed tables
+    const float* __restrict__ dnf = reinterpret_cast<const float*>(src + L.off[2]);
+    const int nn = n_hz * n_hm;
+    for (int i = tid; i < nn; i += blockDim.x) {
+      const float v = __ldg(dnf + i);
+      h32[i] = v;
+      bad |= !isfinite(v);
+    }
+  } else if (a.mixed) {
     const double* __restrict__ dng = src + L.off[2];
     const int nn = n_hz * n_hm;
     for (int i0 = tid; i0 < nn; i0 += 4 * blockDim.x) {
@@ -1248,7 +1256,9 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
   L.n_hz = cfg->n_hz;
   L.n_dist = cfg->n_dist;
   L.n_sci = cfg->n_sci;
-  size_t sizes[7] = {(size_t)cfg->n_hm,   (size_t)cfg->n_hz,   (size_t)cfg->n_hz * cfg->n_hm,
+  L.hmf_f32 = cfg->hmf_fp32 != 0;
+  const size_t n_dn = (size_t)cfg->n_hz * cfg->n_hm;
+  size_t sizes[7] = {(size_t)cfg->n_hm,   (size_t)cfg->n_hz,   L.hmf_f32 ? (n_dn + 1) / 2 : n_dn,
                      (size_t)cfg->n_dist, (size_t)cfg->n_dist, (size_t)cfg->n_sci,
                      (size_t)cfg->n_sci};
   size_t o = 0;
@@ -1483,6 +1493,10 @@ enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_t
   double* Wg = e->Wg.get() + w_off * e->nB_max * e->w_stride;
   double* Phi = e->Phi.get() ? e->Phi.get() + w_off * e->nI_max * e->shear.n_R * e->w_stride
                              : nullptr;
+  if (prec == Y3B_FP64 && e->lay.hmf_f32) {
+    set_error("an engine with FP32 dndlnmh tables (hmf_fp32) evaluates the mixed form only");
+    return Y3B_ERR_INVALID;
+  }
   Y3B_CUDA(cudaMemsetAsync(e->status.get(), 0, sizeof(int), s));
   // The stage counters cover one evaluation call: zeroed by its first chunk.
   if (w_off == 0 && prec == Y3B_MIXED)

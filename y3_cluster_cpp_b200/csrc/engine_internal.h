@@ -66,6 +66,7 @@ struct PointDev {  // mirrors y3b_point
 
 struct TableLayout {
   int n_hm, n_hz, n_dist, n_sci;
+  int hmf_f32;     // dndlnmh section in FP32 (mixed form only)
   size_t stride;   // doubles per point
   size_t off[7];   // m_h, hmf_z, dndlnmh, dist_z, dist_da, sci_z, sci_val
 };

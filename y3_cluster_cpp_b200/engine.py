@@ -286,8 +286,9 @@ class Engine:
     SECTIONS = ("hmf_m_h", "hmf_z", "dndlnmh", "dist_z", "dist_da", "sci_z", "sci_val")
 
     def __init__(self, grids, n_hm, n_hz, n_dist, plob, max_points=256, n_sci=0,
-                 shear=None, hbm_budget=0):
+                 shear=None, hbm_budget=0, hmf_fp32=False):
         self._keep = []
+        self.hmf_fp32 = bool(hmf_fp32)
         self.grids = list(grids)
         G = (A.Grid * len(grids))(*[make_grid(g) for g in grids])
         cfg = A.EngineConfig()
@@ -296,6 +297,7 @@ class Engine:
         cfg.max_points = max_points
         cfg.hbm_budget = hbm_budget
         cfg.with_shear = 1 if shear is not None else 0
+        cfg.hmf_fp32 = int(self.hmf_fp32)
         if shear is not None:
             so = cfg.shear
             so.n_R = len(shear["R"])
@@ -346,7 +348,10 @@ class Engine:
                 v = np.asarray(t[sec], dtype=np.float64).ravel()
                 if v.size != s:
                     raise ValueError(f"point {i}: {sec} has {v.size} values, engine expects {s}")
-                buf[i, o:o + s] = v
+                if sec == "dndlnmh" and self.hmf_fp32:  # n floats in the section's doubles
+                    buf[i, o:o + (s + 1) // 2].view(np.float32)[:s] = v.astype(np.float32)
+                else:
+                    buf[i, o:o + s] = v
         return buf
 
     @staticmethod
