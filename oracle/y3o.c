@@ -323,6 +323,25 @@ phi_diff(double a, double b) /* Phi(b) - Phi(a), b >= a, cancellation-free */
   return 1.0 - 0.5 * erfc(-a / SQRT2) - 0.5 * erfc(b / SQRT2);
 }
 
+/* ln(Phi(b) - Phi(a)) where the difference itself underflows (mu about 38
+ * sigma or more outside [lam_lo, lam_hi]; the direct quotient is then 0/0):
+ * with Q(x) = erfc(x / sqrt 2) / 2 = erfcx(x / sqrt 2) exp(-x^2 / 2) / 2,
+ * ln(Q(a) - Q(b)) = ln Q(a) + log1p(-Q(b) / Q(a)) for 0 < a < b, and the
+ * mirror image for a < b < 0. */
+static double
+ln_phi_diff(double a, double b)
+{
+  if (a > 0.0) {
+    double ra = y3o_erfcx(a / SQRT2), rb = y3o_erfcx(b / SQRT2);
+    return log(0.5 * ra) - 0.5 * a * a + log1p(-(rb / ra) * exp(-0.5 * (b - a) * (b + a)));
+  }
+  if (b < 0.0) {
+    double ra = y3o_erfcx(-a / SQRT2), rb = y3o_erfcx(-b / SQRT2);
+    return log(0.5 * rb) - 0.5 * b * b + log1p(-(ra / rb) * exp(-0.5 * (b - a) * (b + a)));
+  }
+  return log(phi_diff(a, b));
+}
+
 static double
 lognormal_mu(const double* mor, double lnM, double z)
 {
@@ -927,11 +946,14 @@ y3o_direct_eval(const y3o_direct_grid* g, int n_plob, const double* plob_z,
     for (int q = 0; q < nz; ++q) {
       double mu = mor->A + mor->B * (xm[k] - log(mor->Mpiv)) + mor->C * log1p(xz[q]);
       double D = phi_diff((ll_lo - mu) / sig, (ll_hi - mu) / sig);
+      /* below 1e-280 the quotient is taken in logs (its limit, not 0/0) */
+      double lnD = D > 1e-280 ? 0.0 : ln_phi_diff((ll_lo - mu) / sig, (ll_hi - mu) / sig);
       double n = y3o_hmf(hax, n_hm, hmf_z, n_hz, dndlnmh, c->hmf_s, c->hmf_q, xm[k], xz[q]);
       for (int i = 0; i < nI; ++i) S[i] = 0.0;
       for (int t = 0; t < nt; ++t) {
         double d = (xl[t] - mu) / sig;
-        double p = exp(-0.5 * d * d) / (SQRT2PI * sig * D);
+        double p = D > 1e-280 ? exp(-0.5 * d * d) / (SQRT2PI * sig * D)
+                              : exp(-0.5 * d * d - lnD) / (SQRT2PI * sig);
         for (int i = 0; i < nI; ++i)
           S[i] += wl[t] * Ki[((size_t)i * nz + q) * nt + t] * p;
       }

@@ -403,6 +403,33 @@ def test_engine_window_with_mass_piled_at_a_domain_edge(gpu, lam_t):
     eng.close()
 
 
+@pytest.mark.parametrize("sigma", [0.09, 0.07])
+def test_engine_mor_far_outside_the_lam_t_domain(gpu, sigma):
+    """With lam_t_lo = 44.7 and sigma_int = 0.09 (0.07) the lowest-mass cells'
+    mu sits about 40 (50) sigma below ln lam_t_lo: the MOR's in-range mass D
+    underflows FP64 and the Gaussian at every lam_t node underflows too, while
+    their quotient (the density piled at the domain edge) is moderate.  Both
+    forms carry that quotient without an inf or a NaN: FP64 within 1e-9 of the
+    oracle, the mixed form within 1e-4 or a clean Y3B_ERR_RANGE."""
+    g = synthetic.grid(4, lam_t_lo=44.7, lam_t_hi=1000.0)
+    eng = _engine([g])
+    p = synthetic.fiducial()
+    p.sigma = sigma
+    pz, pc = synthetic.plob_baseline()
+    ref, _, _ = O.direct_eval(g, pz, pc, p.mor, O.cosmo(p.om, p.h0), p.tables)
+    assert np.all(np.isfinite(ref)) and np.all(ref > 0)
+    r64 = eng.eval([p], E.FP64, grid_of=lambda _: 0)["counts"][0]
+    np.testing.assert_allclose(r64, ref, rtol=TOL64)
+    try:
+        rmx = eng.eval([p], E.MIXED, grid_of=lambda _: 0)["counts"][0]
+    except E.A.Y3BError as e:
+        assert e.status == E.A.ERR_RANGE
+    else:
+        assert np.all(np.isfinite(rmx))
+        np.testing.assert_allclose(rmx, ref, rtol=TOLMIX)
+    eng.close()
+
+
 @pytest.mark.parametrize("case", [dict(sigma=0.05), dict(sigma=0.1), dict(C=2.0),
                                   dict(sigma=0.05, C=2.0)])
 def test_mixed_form_exponent_range_guard(gpu, case):

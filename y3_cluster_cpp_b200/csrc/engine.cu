@@ -128,6 +128,26 @@ mor_norm(double a, double b)
   return mor_norm_slow(a, b);
 }
 
+// ln D for the same D, finite where D itself underflows FP64 (mu more than
+// ~38 sigma outside the lam_t domain).  With Q(x) = erfc(x / sqrt 2) / 2 =
+// erfcx(x / sqrt 2) exp(-x^2 / 2) / 2: for 0 < a < b, D = Q(a) - Q(b) and
+// ln D = ln Q(a) + log1p(-Q(b) / Q(a)); for a < b < 0, D = Q(-b) - Q(-a)
+// likewise; otherwise mu lies inside the domain and D is not small.
+__device__ __noinline__ double
+ln_mor_norm(double a, double b)
+{
+  constexpr double kInvSqrt2 = 0.70710678118654752440;
+  if (a > 0.0) {
+    const double ra = erfcx(a * kInvSqrt2), rb = erfcx(b * kInvSqrt2);
+    return log(0.5 * ra) - 0.5 * a * a + log1p(-(rb / ra) * exp(-0.5 * (b - a) * (b + a)));
+  }
+  if (b < 0.0) {
+    const double ra = erfcx(-a * kInvSqrt2), rb = erfcx(-b * kInvSqrt2);
+    return log(0.5 * rb) - 0.5 * b * b + log1p(-(ra / rb) * exp(-0.5 * (b - a) * (b + a)));
+  }
+  return log(mor_norm(a, b));
+}
+
 // The mixed form reads D(mu) from a per-point FP64 table: D and dD/dmu at
 // kDTab equally spaced mu over the point's range of alpha_k + beta_q, cubic
 // Hermite interpolation (absolute error ~1e-9 for sigma-scaled spacing 0.03;
@@ -403,6 +423,7 @@ prep_kernel(PrepArgs a)
   const double ll_lo = Gp->ll_lo, ll_hi = Gp->ll_hi;
   if (!a.mixed) {
     double* __restrict__ P0 = s64 + Gp->o_P0;
+    const double xl0 = Gp->xl[0], xl1 = Gp->xl[Gp->n_t - 1];
     for (int idx = tid; idx < n_z * n_m; idx += blockDim.x) {
       const int q = idx / n_m, k = idx - q * n_m;
       const double t = k_t[k], u = q_u[q];
@@ -412,7 +433,18 @@ prep_kernel(PrepArgs a)
                         (1.0 - t) * u * r1[0] + t * u * r1[1]) *
                        k_f[k];
       const double mu = k_alpha[k] + q_beta[q];
-      P0[idx] = n * norm0 / mor_norm((ll_lo - mu) * inv_s, (ll_hi - mu) * inv_s);
+      const double aa = (ll_lo - mu) * inv_s, bb = (ll_hi - mu) * inv_s;
+      // A mu outside the lam_t nodes' span [xl_0, xl_last] carries the
+      // factor exp(-v^2 / 2 s^2) of its distance v to the span here, and the
+      // lam_t sum takes exp(-((l - mu)^2 - v^2) / 2 s^2): both stay finite
+      // however far outside mu lies (D alone underflows near 38 sigma).
+      const double c = fmin(fmax(mu, xl0), xl1);
+      if (c == mu) {
+        P0[idx] = n * norm0 / mor_norm(aa, bb);
+      } else {
+        const double v = (c - mu) * inv_s;
+        P0[idx] = n * norm0 * exp(-0.5 * v * v - ln_mor_norm(aa, bb));
+      }
     }
     return;
   }
@@ -475,67 +507,11 @@ prep_kernel(PrepArgs a)
     dtab[kDTab + j] =
       hmu * inv_s * (exp(-0.5 * aa * aa) - exp(-0.5 * bb * bb)) / kSqrt2Pi;
   }
-  __syncthreads();
-  // One warp per z row; lanes over lnM, four lnM rows per lane in flight
-  // (independent chains for the schedulers), FP32 in the common path.  The
-  // few cells whose MOR is cut by the lam_t domain (mu within 5.6 sigma of an
-  // edge) are scaled by the FP64 D(mu) afterwards.
-  const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
-  for (int q = warp; q < n_z; q += nw) {
-    const float u = (float)q_u[q];
-    const float bb = (float)(q_beta[q] - B0);
-    const float hx = -bb * c2, hy = -0.5f * bb * bb * c2;  // H = 2^(a hx + hy)
-    const float sat_lo = mu_sat_lo - bb, sat_hi = mu_sat_hi - bb;
-    const float* hr0 = h32 + q_y[q] * n_hm;
-    const float* hr1 = hr0 + n_hm;
-    // Tile-blocked: [lnM tile of 128][z][128], so a tile's block is contiguous.
-    float* yrow = Yt + (size_t)q * kGemmRows;
-    for (int k0 = mt0 * kGemmRows; k0 < (mt0 + 1) * kGemmRows; k0 += 128) {
-      float y[4];
-      unsigned slow = 0u;
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int k = k0 + lane + 32 * r;
-        y[r] = 0.f;
-        if (k < n_m) {
-          const float t = kt_f[k];
-          const int xi = k_x[k];
-          const float r0 = fmaf(t, hr0[xi + 1] - hr0[xi], hr0[xi]);
-          const float r1 = fmaf(t, hr1[xi + 1] - hr1[xi], hr1[xi]);
-          const float n = fmaf(u, r1 - r0, r0) * kf_f[k];
-          const float aa = ka_f[k];
-          y[r] = n * fast_exp2(fmaf(aa, hx, hy)) * norm0f;
-          slow |= (aa > sat_lo && aa < sat_hi) ? 0u : (1u << r);
-        }
-      }
-      while (slow) {
-        const int r = __ffs(slow) - 1;
-        slow &= slow - 1u;
-        const int k = k0 + lane + 32 * r;
-        const double mu = k_alpha[k] + q_beta[q];
-        const double uu = (mu - mu0) * inv_hmu;
-        const int j = min(max((int)uu, 0), kDTab - 2);
-        const double t = uu - j, t2 = t * t, t3 = t2 * t;
-        double D = (2.0 * t3 - 3.0 * t2 + 1.0) * dtab[j] + (t3 - 2.0 * t2 + t) * dtab[kDTab + j] +
-                   (3.0 * t2 - 2.0 * t3) * dtab[j + 1] + (t3 - t2) * dtab[kDTab + j + 1];
-        if (D < 1e-3) D = mor_norm_slow((ll_lo - mu) * inv_s, (ll_hi - mu) * inv_s);
-        y[r] *= __frcp_rn((float)D);  // Y is FP32, so is the quotient
-      }
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int k = k0 + lane + 32 * r;
-        if (k < n_m_pad) yrow[(size_t)(k >> 7) * n_z * kGemmRows + (k & (kGemmRows - 1))] = y[r];
-      }
-    }
-  }
-  // F(t, k) = 2^-((delta_t - a_k) sqrt(c1))^2 for the contraction, split into
-  // bf16 hi + lo and written in its shared-memory stage layout: block
-  // (lnM tile, stage) of kFStageBytes, hi planes then lo planes, each plane
-  // 8 lam_t nodes x 128 rows of 16 bytes.  Rows past n_m are zero.
   float* dt_f = reinterpret_cast<float*>(
     (reinterpret_cast<uintptr_t>(dtab + 2 * kDTab) + 15) & ~uintptr_t(15));  // [n_t_pad]
   for (int t = tid; t < n_t_pad; t += blockDim.x) dt_f[t] = t < n_t ? (float)(Gp->xl[t] - L0) : 0.f;
   __syncthreads();
+  const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
   // lam_t window of the contraction per lnM tile.  Each (k, q) cell's
   // density exp(-(l - mu)^2 / 2 s^2) / D is renormalised to the lam_t domain
   // [ll_lo, ll_hi], where it peaks at c = clamp(mu, ll_lo, ll_hi); it is below
@@ -595,6 +571,114 @@ prep_kernel(PrepArgs a)
     }
   }
   __syncthreads();
+  // Row scale of the tile.  F(t, k) = 2^-((delta_t - a_k)^2 c1) underflows
+  // FP32 on every issued node when a_k lies far outside the issued nodes'
+  // span [e_lo, e_hi] (mu many sigma outside the lam_t domain), while its
+  // Y(k, q) = n H / D overflows: the product, the renormalised density at
+  // the domain edge, is moderate.  With c_k = clamp(a_k, e_lo, e_hi) and
+  // v_k = c_k - a_k the row carries F'(t, k) = F 2^(v_k^2 c1) =
+  // 2^-((delta_t - c_k)(delta_t - c_k + 2 v_k) c1) <= 1 and
+  // Y'(k, q) = Y 2^-(v_k^2 c1), computed from ln D in FP64.  Rows inside
+  // the span keep v_k = 0 and the unscaled factors bit for bit.
+  const float sc1 = sqrtf((float)(1.4426950408889634 * 0.5 / (sig * sig)));
+  __shared__ float row_am[kGemmRows], row_vs2[kGemmRows], row_vvf[kGemmRows];
+  __shared__ double row_vv[kGemmRows];
+  {
+    const int t_first = swin[2 * mt0] * 16, t_last = min(swin[2 * mt0 + 1] * 16, n_t) - 1;
+    const double c_lo = t_last >= t_first ? (double)dt_f[t_first] : -1e300;
+    const double c_hi = t_last >= t_first ? (double)dt_f[t_last] : 1e300;
+    const double c1d = 1.4426950408889634 * 0.5 / (sig * sig);
+    for (int r = tid; r < kGemmRows; r += blockDim.x) {
+      const int k = mt0 * kGemmRows + r;
+      float am = 1e18f, vs2 = 0.f;
+      double vv = 0.0;
+      if (k < n_m) {
+        const double ak = k_alpha[k] - A0;
+        if (ak < c_lo || ak > c_hi) {
+          const float cf = ak < c_lo ? dt_f[t_first] : dt_f[t_last];
+          const double v = (double)cf - ak;
+          am = cf * sc1;
+          vs2 = (float)(2.0 * v) * sc1;
+          vv = v * v * c1d;
+        } else {
+          am = ka_f[k] * sc1;
+        }
+      }
+      row_am[r] = am;
+      row_vs2[r] = vs2;
+      row_vv[r] = vv;
+      row_vvf[r] = (float)vv;
+    }
+  }
+  __syncthreads();
+  // One warp per z row; lanes over lnM, four lnM rows per lane in flight
+  // (independent chains for the schedulers), FP32 in the common path.  The
+  // few cells whose MOR is cut by the lam_t domain (mu within 5.6 sigma of an
+  // edge) are scaled by the FP64 D(mu) afterwards.
+  const double c2d = 1.4426950408889634 / (sig * sig);
+  for (int q = warp; q < n_z; q += nw) {
+    const float u = (float)q_u[q];
+    const float bb = (float)(q_beta[q] - B0);
+    const float hx = -bb * c2, hy = -0.5f * bb * bb * c2;  // H = 2^(a hx + hy)
+    const float sat_lo = mu_sat_lo - bb, sat_hi = mu_sat_hi - bb;
+    const float* hr0 = h32 + q_y[q] * n_hm;
+    const float* hr1 = hr0 + n_hm;
+    // Tile-blocked: [lnM tile of 128][z][128], so a tile's block is contiguous.
+    float* yrow = Yt + (size_t)q * kGemmRows;
+    for (int k0 = mt0 * kGemmRows; k0 < (mt0 + 1) * kGemmRows; k0 += 128) {
+      float y[4], nv[4];
+      unsigned slow = 0u;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int k = k0 + lane + 32 * r;
+        y[r] = 0.f;
+        nv[r] = 0.f;
+        if (k < n_m) {
+          const float t = kt_f[k];
+          const int xi = k_x[k];
+          const float r0 = fmaf(t, hr0[xi + 1] - hr0[xi], hr0[xi]);
+          const float r1 = fmaf(t, hr1[xi + 1] - hr1[xi], hr1[xi]);
+          const float n = fmaf(u, r1 - r0, r0) * kf_f[k];
+          const float aa = ka_f[k];
+          nv[r] = n;
+          y[r] = n * fast_exp2(fmaf(aa, hx, hy) - row_vvf[k & (kGemmRows - 1)]) * norm0f;
+          slow |= (aa > sat_lo && aa < sat_hi) ? 0u : (1u << r);
+        }
+      }
+      while (slow) {
+        const int r = __ffs(slow) - 1;
+        slow &= slow - 1u;
+        const int k = k0 + lane + 32 * r;
+        const double mu = k_alpha[k] + q_beta[q];
+        const double uu = (mu - mu0) * inv_hmu;
+        const int j = min(max((int)uu, 0), kDTab - 2);
+        const double t = uu - j, t2 = t * t, t3 = t2 * t;
+        const double D = (2.0 * t3 - 3.0 * t2 + 1.0) * dtab[j] + (t3 - 2.0 * t2 + t) * dtab[kDTab + j] +
+                         (3.0 * t2 - 2.0 * t3) * dtab[j + 1] + (t3 - t2) * dtab[kDTab + j + 1];
+        // log2 of H 2^-(v^2 c1) / D in FP64: its terms can each pass 2^127
+        // in a row far outside the lam_t domain while their sum stays small.
+        const double ad = k_alpha[k] - A0, bd = q_beta[q] - B0;
+        double ex = -(ad * bd + 0.5 * bd * bd) * c2d - row_vv[k & (kGemmRows - 1)];
+        double scale = 1.0;
+        if (D >= 1e-3)
+          scale = 1.0 / D;
+        else
+          ex -= 1.4426950408889634 * ln_mor_norm((ll_lo - mu) * inv_s, (ll_hi - mu) * inv_s);
+        const float yf = (float)((double)nv[r] * norm0 * exp2(ex) * scale);
+        if (!(fabsf(yf) <= 3.402823466e38f)) {  // not representable: report, never a NaN
+          set_err(a.status, kDevRange);
+          y[r] = 0.f;
+        } else {
+          y[r] = yf;
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int k = k0 + lane + 32 * r;
+        if (k < n_m_pad) yrow[(size_t)(k >> 7) * n_z * kGemmRows + (k & (kGemmRows - 1))] = y[r];
+      }
+    }
+  }
   // Exponent range of the factorised form: G = 2^(delta b c2) over the
   // issued stages and H = 2^(-(a b + b^2/2) c2) must stay well inside FP32 /
   // BF16 (2^-126 .. 2^127).  |a| <= (max alpha - min alpha) / 2 and
@@ -615,7 +699,12 @@ prep_kernel(PrepArgs a)
   // The window of each contraction tile (lnM tile, richness-bin group).
   for (int l = mt0 * Gp->n_bg + tid; l < (mt0 + 1) * Gp->n_bg; l += blockDim.x)
     a.win_tile[(size_t)p * a.win_stride + l] = swin[2 * mt0] | (swin[2 * mt0 + 1] << 16);
-  const float sc1 = sqrtf((float)(1.4426950408889634 * 0.5 / (sig * sig)));
+  // F'(t, k) for the contraction (the row scale above), split into bf16
+  // hi + lo and written in its shared-memory stage layout: block
+  // (lnM tile, stage) of kFStageBytes, hi planes then lo planes, each plane
+  // 8 lam_t nodes x 128 rows of 16 bytes.  Rows past n_m are zero; the
+  // exponent is clamped at 0 so the padded nodes past n_t (whose G is zero)
+  // stay finite.
   const float2 sc2 = make_float2(sc1, sc1);
   uint8_t* fb = a.fbuf + (size_t)p * a.f_stride;
   const int nk = n_t_pad / 16, n_g8 = n_t_pad / 8;
@@ -623,8 +712,8 @@ prep_kernel(PrepArgs a)
     const int m = mt0 * kGemmRows + it % kGemmRows, t8 = it / kGemmRows;
     // Only the stages inside each tile's window are ever read (warp-uniform).
     if ((t8 >> 1) < swin[2 * (m >> 7)] || (t8 >> 1) >= swin[2 * (m >> 7) + 1]) continue;
-    const float am = m < n_m ? ka_f[m] * sc1 : 1e18f;
-    const float2 nam2 = make_float2(-am, -am);
+    const float am = row_am[m & (kGemmRows - 1)], vs = row_vs2[m & (kGemmRows - 1)];
+    const float2 nam2 = make_float2(-am, -am), vs2 = make_float2(vs, vs);
     const float4 d0 = *reinterpret_cast<const float4*>(dt_f + t8 * 8);
     const float4 d1 = *reinterpret_cast<const float4*>(dt_f + t8 * 8 + 4);
     const float2 dd[4] = {make_float2(d0.x, d0.y), make_float2(d0.z, d0.w),
@@ -633,8 +722,8 @@ prep_kernel(PrepArgs a)
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const float2 x = __ffma2_rn(dd[u], sc2, nam2);
-      const float2 e = __fmul2_rn(x, x);
-      v[u] = make_float2(fast_exp2(-e.x), fast_exp2(-e.y));
+      const float2 e = __fmul2_rn(x, __fadd2_rn(x, vs2));
+      v[u] = make_float2(fast_exp2(-fmaxf(e.x, 0.f)), fast_exp2(-fmaxf(e.y, 0.f)));
     }
     uint8_t* st = fb + ((size_t)(m >> 7) * nk + (t8 >> 1)) * kFStageBytes + (t8 & 1) * 2048 +
                   (m & 127) * 16;
@@ -644,7 +733,9 @@ prep_kernel(PrepArgs a)
 
 // ---------------------------------------------------------------------------
 // FP64 plain form.  CTA = (z node q, point); thread k sums over lam_t with one
-// FP64 exp per node: V_i(q, k) = P0_kq sum_t u_t K_i(t, q) exp(-(l_t - mu)^2/2s^2).
+// FP64 exp per node: V_i(q, k) = P0_kq sum_t u_t K_i(t, q) exp(-(l_t - mu)^2/2s^2)
+// (with the edge factor exp(-v^2 / 2 s^2) moved into P0 for mu outside the
+// nodes' span).
 __global__ void __launch_bounds__(256)
 direct_main_kernel(const GridDev* grids, const PointDev* pts, double* s64all, int grid_mask)
 {
@@ -668,11 +759,14 @@ direct_main_kernel(const GridDev* grids, const PointDev* pts, double* s64all, in
   const double inv2s2 = 0.5 / (pt.sigma * pt.sigma);
   for (int k = threadIdx.x; k < G.n_m; k += blockDim.x) {
     const double mu = s64[G.o_alpha + k] + beta;
+    // (l - mu)^2 - v^2 = w (w + 2 v), w = l - c, v = c - mu, c = mu clamped
+    // to the nodes' span (v = 0 and w = l - mu inside it).
+    const double c = fmin(fmax(mu, xl[0]), xl[n_t - 1]), v2 = 2.0 * (c - mu);
     double S[kMaxLamBins];
     for (int i = 0; i < nI; ++i) S[i] = 0.0;
     for (int t = 0; t < n_t; ++t) {
-      const double d = xl[t] - mu;
-      const double e = exp(-d * d * inv2s2);
+      const double w = xl[t] - c;
+      const double e = exp(-w * (w + v2) * inv2s2);
       for (int i = 0; i < nI; ++i) S[i] += wk[i * n_t + t] * e;
     }
     const double P0 = s64[G.o_P0 + (size_t)q * G.n_m + k];
