@@ -518,12 +518,20 @@ def serving_run(a, rank, dev):
     rng = np.random.default_rng(3 + rank)
     total = int(sizes.sum())
     tables_h = torch.empty((total, eng.stride), dtype=torch.float64, pin_memory=True).numpy()
-    reqs, o = [], 0
+    # The same requests with the HMF grid in FP32 in the packed tables (the
+    # mixed form's wire format: fewer host-to-device bytes per point).
+    eng32 = engine.Engine(grids, len(t0["hmf_m_h"]), len(t0["hmf_z"]), len(t0["dist_z"]),
+                          (pz, pc), max_points=2048, n_sci=len(t0["sci_z"]), hmf_fp32=True)
+    tab_pool32 = eng32.pack(pool)
+    tables32_h = torch.empty((total, eng32.stride), dtype=torch.float64, pin_memory=True).numpy()
+    reqs, reqs32, o = [], [], 0
     for n in sizes:
         idx = rng.integers(0, len(pool), n)
         tables_h[o:o + n] = tab_pool[idx]
+        tables32_h[o:o + n] = tab_pool32[idx]
         pts = eng.points_array([pool[i] for i in idx], grid_of=lambda p: gi[p.density])
         reqs.append((pts, tables_h[o:o + n]))
+        reqs32.append((pts, tables32_h[o:o + n]))
         o += n
 
     # plain per-request FP64 GPU form, in arrival order (one request at a time)
@@ -553,8 +561,16 @@ def serving_run(a, rank, dev):
         sat = serve.run_closed_loop(srv, reqs, outstanding)
         s2 = srv.stats()
     eng.close()
+    with serve.Server(eng32, pool_points=8192, max_batch=2048, precision=engine.MIXED) as srv:
+        srv.wait(srv.submit(*reqs32[0]))
+        s3 = srv.stats()
+        sat32 = serve.run_closed_loop(srv, reqs32, outstanding)
+        s4 = srv.stats()
+    eng32.close()
     err = max(float(np.max(np.abs(r["counts"] / c - 1)))
-              for rr in (run, sat) for r, c in zip(rr["results"], fp64_counts))
+              for rr in (run, sat, sat32) for r, c in zip(rr["results"], fp64_counts))
+    sat32_tp = total / sat32["wall_s"]
+    sat32_launches = s4["launches"] - s3["launches"]
     launches = s1["launches"] - s0["launches"]
     sat_launches = s2["launches"] - s1["launches"]
     sat_tp = total / sat["wall_s"]
@@ -577,7 +593,14 @@ def serving_run(a, rank, dev):
                           "launches": sat_launches,
                           "mean_launch_points": total / max(sat_launches, 1),
                           "speedup_vs_fp64_per_request": sat_tp / fp64_capacity,
-                          "host_table_bytes_per_point": eng.stride * 8}}
+                          "host_table_bytes_per_point": eng.stride * 8},
+            "saturated_fp32_hmf_tables": {
+                "outstanding_requests": outstanding, "throughput": sat32_tp, "unit": UNIT,
+                **serve.percentiles_ms(sat32["latency_s"]),
+                "launches": sat32_launches,
+                "mean_launch_points": total / max(sat32_launches, 1),
+                "speedup_vs_fp64_per_request": sat32_tp / fp64_capacity,
+                "host_table_bytes_per_point": eng32.stride * 8}}
 
 
 def run_ours(a):

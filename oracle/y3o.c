@@ -337,7 +337,7 @@ ln_phi_diff(double a, double b)
   }
   if (b < 0.0) {
     double ra = y3o_erfcx(-a / SQRT2), rb = y3o_erfcx(-b / SQRT2);
-    return log(0.5 * rb) - 0.5 * b * b + log1p(-(ra / rb) * exp(-0.5 * (b - a) * (b + a)));
+    return log(0.5 * rb) - 0.5 * b * b + log1p(-(ra / rb) * exp(-0.5 * (a - b) * (a + b)));
   }
   return log(phi_diff(a, b));
 }

@@ -128,6 +128,17 @@ mor_norm(double a, double b)
   return mor_norm_slow(a, b);
 }
 
+// v 2^e for an integer-valued e: two power-of-two factors, each a normal
+// FP32 value, so the product is exact wherever it is a normal or subnormal
+// FP32 number (e is clamped to [-252, 254], far past both ends of the range).
+__device__ __forceinline__ float
+mul_pow2(float v, double e)
+{
+  const int ei = (int)fmin(fmax(e, -252.0), 254.0);
+  const int e1 = ei >> 1, e2 = ei - e1;
+  return (v * __int_as_float((e1 + 127) << 23)) * __int_as_float((e2 + 127) << 23);
+}
+
 // ln D for the same D, finite where D itself underflows FP64 (mu more than
 // ~38 sigma outside the lam_t domain).  With Q(x) = erfc(x / sqrt 2) / 2 =
 // erfcx(x / sqrt 2) exp(-x^2 / 2) / 2: for 0 < a < b, D = Q(a) - Q(b) and
@@ -143,16 +154,15 @@ ln_mor_norm(double a, double b)
   }
   if (b < 0.0) {
     const double ra = erfcx(-a * kInvSqrt2), rb = erfcx(-b * kInvSqrt2);
-    return log(0.5 * rb) - 0.5 * b * b + log1p(-(ra / rb) * exp(-0.5 * (b - a) * (b + a)));
+    return log(0.5 * rb) - 0.5 * b * b + log1p(-(ra / rb) * exp(-0.5 * (a - b) * (a + b)));
   }
   return log(mor_norm(a, b));
 }
 
-// The mixed form reads D(mu) from a per-point FP64 table: D and dD/dmu at
-// kDTab equally spaced mu over the point's range of alpha_k + beta_q, cubic
-// Hermite interpolation (absolute error ~1e-9 for sigma-scaled spacing 0.03;
-// below D = 1e-3 the direct FP64 value is used, so the relative error stays
-// small in deep tails).
+// The mixed form reads log2 D(mu) from a per-point FP64 table: log2 D and
+// its derivative at kDTab equally spaced mu over the point's range of
+// alpha_k + beta_q, cubic Hermite interpolation (log D is smooth, so the
+// relative error of D stays ~1e-9 from the domain's interior to deep tails).
 constexpr int kDTab = 1024;
 
 constexpr int kEvalChunks = 8;  // chunks of a large host-buffer evaluation
@@ -183,7 +193,7 @@ prep_smem_bytes(const TableLayout& L, int n_hz, int n_hm, int n_m, int n_z, int 
 // prep kernel admits; FP32 and BF16 hold 2^-126 .. 2^127.
 constexpr double kMaxExp2 = 100.0;
 
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256, 3)
 prep_kernel(PrepArgs a)
 {
   extern __shared__ __align__(16) double psh[];
@@ -468,7 +478,7 @@ prep_kernel(PrepArgs a)
   const float norm0f = (float)norm0;
   // Y is FP32: where mu is more than 5.6 sigma inside the lam_t domain,
   // 1 - D < 2^-26 and (float)D is exactly 1, the saturated scale.  The FP32
-  // test keeps a 1e-3 margin; everything else reads the FP64 table of D.
+  // test keeps a 1e-3 margin; everything else reads the FP64 table of log2 D.
   const float mu_sat_lo = (float)(ll_lo + 5.6 * sig - L0) + 1e-3f;
   const float mu_sat_hi = (float)(ll_hi - 5.6 * sig - L0) - 1e-3f;
   // FP32 copies of the per-k vectors, reusing the FP64 arrays' space is not
@@ -481,31 +491,35 @@ prep_kernel(PrepArgs a)
     kf_f[k] = (float)k_f[k];
     ka_f[k] = (float)(k_alpha[k] - A0);
   }
-  // D(mu) and h dD/dmu = h (phi(a) - phi(b)) / s on the table nodes.
+  // log2 D(mu) and h dlog2D/dmu on the table nodes, FP64.  ln D comes from
+  // ln_mor_norm (finite however far mu lies outside the domain) and
+  // dlnD/dmu = (phi(a) - phi(b)) / (s D), taken in logs.  Only nodes next to
+  // a mu that fails the FP32 saturation test are read (the test's margin is
+  // 1e-3 plus FP32 rounding, and the nodes used lie within hmu of mu): the
+  // interior nodes hold log2 D = 0 without an erfc.
+  constexpr double kLog2e = 1.4426950408889634;
   double* dtab = reinterpret_cast<double*>(
     (reinterpret_cast<uintptr_t>(ka_f + n_m) + 7) & ~uintptr_t(7));  // [2 kDTab]
   const double mu0 = red[2];
   const double hmu = red[3] > red[2] ? (red[3] - red[2]) / (kDTab - 1) : 1.0;
   const double inv_hmu = 1.0 / hmu;
-  // Only nodes next to a mu that fails the FP32 saturation test are read (the
-  // test's margin is 1e-3 plus FP32 rounding, and the nodes used lie within
-  // hmu of mu): the interior nodes hold D = 1, dD = 0 without an erfc.
   const int j_sat0 =
     (int)fmin(fmax(ceil((ll_lo + 5.6 * sig + 0.01 - mu0) * inv_hmu) + 2.0, 0.0), (double)kDTab);
   const int j_sat1 =
     (int)fmin(fmax(floor((ll_hi - 5.6 * sig - 0.01 - mu0) * inv_hmu) - 2.0, 0.0), (double)kDTab);
   const int n_lo = min(j_sat0 + 1, kDTab), n_hi = kDTab - max(j_sat1, n_lo);
   for (int j = n_lo + tid; j < kDTab - n_hi; j += blockDim.x) {
-    dtab[j] = 1.0;
+    dtab[j] = 0.0;
     dtab[kDTab + j] = 0.0;
   }
   for (int r = tid; r < n_lo + n_hi; r += blockDim.x) {
     const int j = r < n_lo ? r : kDTab - n_hi + (r - n_lo);
     const double mu = mu0 + j * hmu;
     const double aa = (ll_lo - mu) * inv_s, bb = (ll_hi - mu) * inv_s;
-    dtab[j] = mor_norm(aa, bb);
-    dtab[kDTab + j] =
-      hmu * inv_s * (exp(-0.5 * aa * aa) - exp(-0.5 * bb * bb)) / kSqrt2Pi;
+    const double lnD = ln_mor_norm(aa, bb);
+    dtab[j] = kLog2e * lnD;
+    dtab[kDTab + j] = hmu * inv_s * kLog2e *
+                      (exp(-0.5 * aa * aa - lnD) - exp(-0.5 * bb * bb - lnD)) / kSqrt2Pi;
   }
   float* dt_f = reinterpret_cast<float*>(
     (reinterpret_cast<uintptr_t>(dtab + 2 * kDTab) + 15) & ~uintptr_t(15));  // [n_t_pad]
@@ -523,6 +537,7 @@ prep_kernel(PrepArgs a)
   // mu, so the tile's window runs from the lower end for its smallest mu to
   // the upper end for its largest; stages outside add less than the rounding
   // of the split-BF16 products.  The stage count is rounded up to pairs.
+  __shared__ float tile_af[2];
   {
     constexpr double kWin = 5.0;
     const int nk = n_t_pad / 16;
@@ -567,6 +582,10 @@ prep_kernel(PrepArgs a)
         }
         swin[2 * mt] = lo;
         swin[2 * mt + 1] = hi;
+        // The tile's range of a_k = alpha_k - A0 as FP32: rounding is
+        // monotone, so these are the min and max of its rows' FP32 a_k.
+        tile_af[0] = (float)(amn - A0);
+        tile_af[1] = (float)(amx - A0);
       }
     }
   }
@@ -581,8 +600,12 @@ prep_kernel(PrepArgs a)
   // Y'(k, q) = Y 2^-(v_k^2 c1), computed from ln D in FP64.  Rows inside
   // the span keep v_k = 0 and the unscaled factors bit for bit.
   const float sc1 = sqrtf((float)(1.4426950408889634 * 0.5 / (sig * sig)));
-  __shared__ float row_am[kGemmRows], row_vs2[kGemmRows], row_vvf[kGemmRows];
+  __shared__ float row_am[kGemmRows], row_vs2[kGemmRows], row_vvf[kGemmRows], row_t[kGemmRows];
+  __shared__ int row_x[kGemmRows];
   __shared__ double row_vv[kGemmRows];
+  __shared__ int tile_scaled;
+  if (tid == 0) tile_scaled = 0;
+  __syncthreads();
   {
     const int t_first = swin[2 * mt0] * 16, t_last = min(swin[2 * mt0 + 1] * 16, n_t) - 1;
     const double c_lo = t_last >= t_first ? (double)dt_f[t_first] : -1e300;
@@ -608,75 +631,103 @@ prep_kernel(PrepArgs a)
       row_vs2[r] = vs2;
       row_vv[r] = vv;
       row_vvf[r] = (float)vv;
+      row_t[r] = k < n_m ? kt_f[k] : 0.f;
+      row_x[r] = k < n_m ? k_x[k] : 0;
+      if (vv != 0.0) tile_scaled = 1;
     }
   }
   __syncthreads();
-  // One warp per z row; lanes over lnM, four lnM rows per lane in flight
-  // (independent chains for the schedulers), FP32 in the common path.  The
-  // few cells whose MOR is cut by the lam_t domain (mu within 5.6 sigma of an
-  // edge) are scaled by the FP64 D(mu) afterwards.
-  const double c2d = 1.4426950408889634 / (sig * sig);
-  for (int q = warp; q < n_z; q += nw) {
-    const float u = (float)q_u[q];
-    const float bb = (float)(q_beta[q] - B0);
-    const float hx = -bb * c2, hy = -0.5f * bb * bb * c2;  // H = 2^(a hx + hy)
-    const float sat_lo = mu_sat_lo - bb, sat_hi = mu_sat_hi - bb;
-    const float* hr0 = h32 + q_y[q] * n_hm;
-    const float* hr1 = hr0 + n_hm;
-    // Tile-blocked: [lnM tile of 128][z][128], so a tile's block is contiguous.
-    float* yrow = Yt + (size_t)q * kGemmRows;
-    for (int k0 = mt0 * kGemmRows; k0 < (mt0 + 1) * kGemmRows; k0 += 128) {
-      float y[4], nv[4];
-      unsigned slow = 0u;
+  // Y(k, q) = n(M_k, z_q) kf_k H(k, q) 2^-(v_k^2 c1) / (sqrt(2 pi) s D_kq).
+  // Warp w takes a contiguous run of z rows and lane the tile rows
+  // lane + 32 j (j < 4).  Each lane keeps, in registers, the two HMF z rows
+  // around the current z_q interpolated in mass and scaled by
+  // kf_k / (sqrt(2 pi) s), and advances them with q (the z nodes ascend).  A
+  // z row whose tile cells all have mu more than 5.6 sigma inside the domain
+  // (D = 1 in FP32) is FP32 only; otherwise each unsaturated cell takes
+  // log2 D from the FP64 table and forms 2^(log2 H - v^2 c1 - log2 D) in
+  // FP64, applied as an exact power of two times 2^(fraction) in FP32.
+  const double c2d = kLog2e / (sig * sig);
+  {
+    const int qs = (n_z + nw - 1) / nw, qa = warp * qs, qb = min(n_z, qa + qs);
+    // Per row: mass-interpolation weight and cell, kf_k / (sqrt(2 pi) s)
+    // (0 past n_m), a_k; the row scale v_k^2 c1 is read only in tiles that
+    // have such rows.
+    float* rt_s = row_t;
+    int* rx_s = row_x;
+    float rn[4], rk[4], R0[4], R1[4];
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int k = k0 + lane + 32 * r;
-        y[r] = 0.f;
-        nv[r] = 0.f;
-        if (k < n_m) {
-          const float t = kt_f[k];
-          const int xi = k_x[k];
-          const float r0 = fmaf(t, hr0[xi + 1] - hr0[xi], hr0[xi]);
-          const float r1 = fmaf(t, hr1[xi + 1] - hr1[xi], hr1[xi]);
-          const float n = fmaf(u, r1 - r0, r0) * kf_f[k];
-          const float aa = ka_f[k];
-          nv[r] = n;
-          y[r] = n * fast_exp2(fmaf(aa, hx, hy) - row_vvf[k & (kGemmRows - 1)]) * norm0f;
-          slow |= (aa > sat_lo && aa < sat_hi) ? 0u : (1u << r);
-        }
-      }
-      while (slow) {
-        const int r = __ffs(slow) - 1;
-        slow &= slow - 1u;
-        const int k = k0 + lane + 32 * r;
-        const double mu = k_alpha[k] + q_beta[q];
-        const double uu = (mu - mu0) * inv_hmu;
-        const int j = min(max((int)uu, 0), kDTab - 2);
-        const double t = uu - j, t2 = t * t, t3 = t2 * t;
-        const double D = (2.0 * t3 - 3.0 * t2 + 1.0) * dtab[j] + (t3 - 2.0 * t2 + t) * dtab[kDTab + j] +
-                         (3.0 * t2 - 2.0 * t3) * dtab[j + 1] + (t3 - t2) * dtab[kDTab + j + 1];
-        // log2 of H 2^-(v^2 c1) / D in FP64: its terms can each pass 2^127
-        // in a row far outside the lam_t domain while their sum stays small.
-        const double ad = k_alpha[k] - A0, bd = q_beta[q] - B0;
-        double ex = -(ad * bd + 0.5 * bd * bd) * c2d - row_vv[k & (kGemmRows - 1)];
-        double scale = 1.0;
-        if (D >= 1e-3)
-          scale = 1.0 / D;
-        else
-          ex -= 1.4426950408889634 * ln_mor_norm((ll_lo - mu) * inv_s, (ll_hi - mu) * inv_s);
-        const float yf = (float)((double)nv[r] * norm0 * exp2(ex) * scale);
-        if (!(fabsf(yf) <= 3.402823466e38f)) {  // not representable: report, never a NaN
-          set_err(a.status, kDevRange);
-          y[r] = 0.f;
+    for (int j = 0; j < 4; ++j) {
+      const int r = lane + 32 * j, k = mt0 * kGemmRows + r;
+      const bool ok = k < n_m;
+      rn[j] = ok ? kf_f[k] * norm0f : 0.f;
+      rk[j] = ok ? ka_f[k] : 0.f;
+      R0[j] = R1[j] = 0.f;
+    }
+    const float tmin = tile_af[0], tmax = tile_af[1];
+    const bool scaled = tile_scaled != 0;
+    float* __restrict__ yblk = Yt + (size_t)mt0 * n_z * kGemmRows;
+    int ycur = -2;
+    for (int q = qa; q < qb; ++q) {
+      const int yq = q_y[q];
+      if (yq != ycur) {  // warp-uniform
+        const float* h1 = h32 + (size_t)(yq + 1) * n_hm;
+        if (yq == ycur + 1) {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int x = rx_s[lane + 32 * j];
+            R0[j] = R1[j];
+            R1[j] = fmaf(rt_s[lane + 32 * j], h1[x + 1] - h1[x], h1[x]) * rn[j];
+          }
         } else {
-          y[r] = yf;
+          const float* h0 = h1 - n_hm;
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int x = rx_s[lane + 32 * j];
+            const float t = rt_s[lane + 32 * j];
+            R0[j] = fmaf(t, h0[x + 1] - h0[x], h0[x]) * rn[j];
+            R1[j] = fmaf(t, h1[x + 1] - h1[x], h1[x]) * rn[j];
+          }
+        }
+        ycur = yq;
+      }
+      const float u = (float)q_u[q];
+      const float bb = (float)(q_beta[q] - B0);
+      const float hx = -bb * c2, hy = -0.5f * bb * bb * c2;  // H = 2^(a hx + hy)
+      const float sat_lo = mu_sat_lo - bb, sat_hi = mu_sat_hi - bb;
+      float y[4], nv[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        nv[j] = fmaf(u, R1[j] - R0[j], R0[j]);
+        const float e = fmaf(rk[j], hx, hy);
+        y[j] = nv[j] * fast_exp2(scaled ? e - row_vvf[lane + 32 * j] : e);
+      }
+      if (!(tmin > sat_lo && tmax < sat_hi)) {  // some cell of this z row is unsaturated
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int r = lane + 32 * j, k = mt0 * kGemmRows + r;
+          if (k >= n_m || (rk[j] > sat_lo && rk[j] < sat_hi)) continue;
+          const double mu = k_alpha[k] + q_beta[q];
+          const double uu = (mu - mu0) * inv_hmu;
+          const int jj = min(max((int)uu, 0), kDTab - 2);
+          const double t = uu - jj, t2 = t * t, t3 = t2 * t;
+          const double l2d = (2.0 * t3 - 3.0 * t2 + 1.0) * dtab[jj] +
+                             (t3 - 2.0 * t2 + t) * dtab[kDTab + jj] +
+                             (3.0 * t2 - 2.0 * t3) * dtab[jj + 1] +
+                             (t3 - t2) * dtab[kDTab + jj + 1];
+          const double ad = k_alpha[k] - A0, bd = q_beta[q] - B0;
+          const double ex = -(ad * bd + 0.5 * bd * bd) * c2d - row_vv[r] - l2d;
+          const double ei = rint(ex);
+          const float yf = mul_pow2(nv[j] * fast_exp2((float)(ex - ei)), ei);
+          if (!(fabsf(yf) <= 3.402823466e38f)) {  // not representable: report, never a NaN
+            set_err(a.status, kDevRange);
+            y[j] = 0.f;
+          } else {
+            y[j] = yf;
+          }
         }
       }
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int k = k0 + lane + 32 * r;
-        if (k < n_m_pad) yrow[(size_t)(k >> 7) * n_z * kGemmRows + (k & (kGemmRows - 1))] = y[r];
-      }
+      for (int j = 0; j < 4; ++j) yblk[(size_t)q * kGemmRows + lane + 32 * j] = y[j];
     }
   }
   // Exponent range of the factorised form: G = 2^(delta b c2) over the
@@ -702,16 +753,16 @@ prep_kernel(PrepArgs a)
   // F'(t, k) for the contraction (the row scale above), split into bf16
   // hi + lo and written in its shared-memory stage layout: block
   // (lnM tile, stage) of kFStageBytes, hi planes then lo planes, each plane
-  // 8 lam_t nodes x 128 rows of 16 bytes.  Rows past n_m are zero; the
-  // exponent is clamped at 0 so the padded nodes past n_t (whose G is zero)
-  // stay finite.
+  // 8 lam_t nodes x 128 rows of 16 bytes.  Rows past n_m are zero.  The
+  // exponent is >= 0 on every real node; the padded nodes past n_t (whose G
+  // is zero) take its magnitude, so F' <= 1 stays finite there too.
   const float2 sc2 = make_float2(sc1, sc1);
   uint8_t* fb = a.fbuf + (size_t)p * a.f_stride;
-  const int nk = n_t_pad / 16, n_g8 = n_t_pad / 8;
-  for (int it = tid; it < kGemmRows * n_g8; it += blockDim.x) {
+  const int nk = n_t_pad / 16;
+  // Only the stages inside the tile's window are ever read.
+  for (int it = swin[2 * mt0] * 2 * kGemmRows + tid; it < swin[2 * mt0 + 1] * 2 * kGemmRows;
+       it += blockDim.x) {
     const int m = mt0 * kGemmRows + it % kGemmRows, t8 = it / kGemmRows;
-    // Only the stages inside each tile's window are ever read (warp-uniform).
-    if ((t8 >> 1) < swin[2 * (m >> 7)] || (t8 >> 1) >= swin[2 * (m >> 7) + 1]) continue;
     const float am = row_am[m & (kGemmRows - 1)], vs = row_vs2[m & (kGemmRows - 1)];
     const float2 nam2 = make_float2(-am, -am), vs2 = make_float2(vs, vs);
     const float4 d0 = *reinterpret_cast<const float4*>(dt_f + t8 * 8);
@@ -723,7 +774,7 @@ prep_kernel(PrepArgs a)
     for (int u = 0; u < 4; ++u) {
       const float2 x = __ffma2_rn(dd[u], sc2, nam2);
       const float2 e = __fmul2_rn(x, __fadd2_rn(x, vs2));
-      v[u] = make_float2(fast_exp2(-fmaxf(e.x, 0.f)), fast_exp2(-fmaxf(e.y, 0.f)));
+      v[u] = make_float2(fast_exp2(-fabsf(e.x)), fast_exp2(-fabsf(e.y)));
     }
     uint8_t* st = fb + ((size_t)(m >> 7) * nk + (t8 >> 1)) * kFStageBytes + (t8 & 1) * 2048 +
                   (m & 127) * 16;
