@@ -269,7 +269,11 @@ int y3b_sigma_crit_inv(int n_zl, const double* zl, int n_zs, const double* zs,
 /* Miscentred NFW profiles at n points: out[i] = 2 r_s delta_c rho 1e-12 *
  * <profile>(r[i]/r_s, rmis[i]/r_s), r_s from lnM[i], concentration conc and
  * rho (NFW_DSIGMA_MIS(c, rho) / NFW_SIGMA_MIS(c, rho) operator()).
- * which = 0: DeltaSigma_mis, 1: Sigma_mis.  Host buffers. */
+ * which = 0: DeltaSigma_mis, 1: Sigma_mis (both for offsets drawn from the
+ * gamma kernel), 2: DeltaSigma for a single offset rmis (the "single" kernel:
+ * mean tangential shear on the circle of radius r around the offset centre,
+ * n_theta GL nodes on [0, pi]; n_s and s_max are checked but unused).  Host
+ * buffers. */
 int y3b_nfw_mis(int which, int n, const double* r, const double* rmis,
                 const double* lnM, double conc, double rho, int n_theta,
                 int n_s, double s_max, double* out);

@@ -348,6 +348,26 @@ struct NfwUnit<float> {
   }
 };
 
+// Single-offset miscentred DeltaSigma (the "single" kernel of
+// NFW_DSIGMA_MIS, nfw_dsigma_mis.hh:53-55) in units of 2 r_s delta_c rho:
+// the mean tangential shear on the circle of radius x around the offset
+// centre, (1/pi) int_0^pi dth DSigma(d) (2 a^2 / d^2 - 1) with
+// d^2 = x^2 + x_mis^2 - 2 x x_mis cos th, a = x - x_mis cos th.  Returns the
+// sum over the GL nodes t0, t0 + dt, ... of [0, pi] (without the 1/pi), so
+// a warp can split the nodes.
+__device__ __forceinline__ double
+dsigma_single_partial(const double* th, const double* wth, int n, double x, double xm, int t0,
+                      int dt)
+{
+  double acc = 0.0;
+  for (int t = t0; t < n; t += dt) {
+    const double ct = cos(th[t]);
+    const double d2 = x * x + xm * xm - 2.0 * x * xm * ct, a = x - xm * ct;
+    acc += wth[t] * NfwUnit<double>::dsigma(sqrt(d2)) * (2.0 * a * a / d2 - 1.0);
+  }
+  return acc;
+}
+
 __device__ __forceinline__ double
 nfw_rs(double lnM, double c, double rho)
 {

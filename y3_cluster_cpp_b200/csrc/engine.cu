@@ -164,27 +164,27 @@ ln_mor_norm(double a, double b)
 // alpha_k + beta_q, cubic Hermite interpolation (log D is smooth, so the
 // relative error of D stays ~1e-9 from the domain's interior to deep tails).
 constexpr int kDTab = 1024;
+constexpr int kYfHdr = 8;        // floats of yf_kernel's FP32 header
+constexpr int kYfRowFields = 8;  // fields of yf_kernel's per-row block
 
 constexpr int kEvalChunks = 8;  // chunks of a large host-buffer evaluation
 
-// Per-point prep, one CTA per point.  The point's packed tables are staged
-// into shared memory with one bulk (TMA) copy completing on an mbarrier;
-// then, per point:
-//   FP64: cz_q = v_q dV(z_q) Omega(z_q), czs_q = cz_q Sci(z_q), alpha_k,
-//         beta_q (s64), and for the FP64 form P0 = n(M_k,z_q) / (sqrt(2 pi)
-//         s D_kq);
-//   mixed form: a_k, b_q, delta_t, c1, c2, C_j(q), C^g_j(q) and
-//         Y = n H / (sqrt(2 pi) s D) in FP32 (D in FP64 where not exactly 1).
-// Shared memory: table block | FP32 dn/dlnM | per-k and per-q vectors.
+// Per-point prep, one CTA per point.  The point's packed tables (without the
+// HMF grid, which is read from global memory) are staged into shared memory
+// with bulk (TMA) copies completing on an mbarrier; then, per point:
+//   both forms: cz_q = v_q dV(z_q) Omega(z_q), czs_q = cz_q Sci(z_q),
+//         alpha_k, beta_q (s64);
+//   FP64 form: P0 = n(M_k,z_q) / (sqrt(2 pi) s D_kq);
+//   mixed form: a_k, b_q, delta_t, c1, c2, C_j(q), C^g_j(q) for the
+//         contraction, the lam_t windows, and yf_kernel's inputs (row
+//         blocks, z rows, the log2 D table).
+// Shared memory: table block | per-k and per-q vectors | FP32 delta_t.
 __host__ __device__ inline size_t
-prep_smem_bytes(const TableLayout& L, int n_hz, int n_hm, int n_m, int n_z, int n_t_pad)
+prep_smem_bytes(const TableLayout& L, int n_m, int n_z, int n_t_pad)
 {
   size_t b = (L.off[2] + L.stride - L.off[3]) * 8;         // table block without dn/dlnM
-  b += (((size_t)n_hz * n_hm * 4) + 15) & ~size_t(15);     // FP32 dn/dlnM
   b += (size_t)n_m * (8 + 8 + 8 + 4);                      // alpha, t, kf, xi
   b += (size_t)n_z * (8 + 8 + 4);                          // beta, u, yi
-  b += (size_t)n_m * 12;                                   // FP32 t, kf, alpha - A0
-  b += 8 + 2 * (size_t)kDTab * 8;                          // D(mu) table (mixed form)
   b += 16 + (size_t)n_t_pad * 4;                           // FP32 delta_t (mixed form)
   return b + 64;
 }
@@ -193,7 +193,7 @@ prep_smem_bytes(const TableLayout& L, int n_hz, int n_hm, int n_m, int n_z, int 
 // prep kernel admits; FP32 and BF16 hold 2^-126 .. 2^127.
 constexpr double kMaxExp2 = 100.0;
 
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, 4)
 prep_kernel(PrepArgs a)
 {
   extern __shared__ __align__(16) double psh[];
@@ -205,23 +205,14 @@ prep_kernel(PrepArgs a)
   }
   const GridDev* __restrict__ Gp = a.grids + pt.grid;
   const int n_m = Gp->n_m, n_z = Gp->n_z, n_m_pad = Gp->n_m_pad, tid = threadIdx.x;
-  // The mixed form runs one CTA per (point, 128-row lnM tile): each computes
-  // its tile's Y rows, stage window and F blocks, and the tile-0 CTA also
-  // writes the point's shared factors.  The FP64 form runs one CTA per point.
-  const int mt0 = blockIdx.y;
-  if (mt0 >= n_m_pad / kGemmRows || (!a.mixed && mt0 > 0)) return;
-  const bool lead = mt0 == 0;
   const TableLayout& L = a.lay;
   const int n_hm = L.n_hm, n_hz = L.n_hz;
   // The small tables (HMF axes, distances, Sigma_crit) are staged in shared
-  // memory; the n_hz x n_hm HMF grid is read once from global memory (FP32
-  // copy for the mixed form), which keeps a CTA small enough for several to
-  // share an SM.
+  // memory; the n_hz x n_hm HMF grid stays in global memory (the FP64 form
+  // reads it there, yf_kernel stages the mixed form's FP32 copy).
   const size_t head = L.off[2], tail = L.stride - L.off[3];
   double* tab = psh;                                                  // [head + tail]
-  float* h32 = reinterpret_cast<float*>(tab + head + tail);           // [n_hz n_hm]
-  double* k_alpha = reinterpret_cast<double*>(
-    reinterpret_cast<uint8_t*>(h32) + ((((size_t)n_hz * n_hm * 4) + 15) & ~size_t(15)));
+  double* k_alpha = tab + head + tail;
   double* k_t = k_alpha + n_m;
   double* k_f = k_t + n_m;
   double* q_beta = k_f + n_m;
@@ -258,35 +249,6 @@ prep_kernel(PrepArgs a)
         "l"(src + L.off[3]), "r"((uint32_t)(tail * sizeof(double))), "r"(smem_addr(&bar))
         : "memory");
   }
-  // FP32 copy of the HMF grid for the mixed form, straight from global memory
-  // while the bulk copy of the small tables is in flight (four loads in
-  // flight per thread).
-  if (a.mixed && L.hmf_f32) {  // already FP32 in the packed tables
-    const float* __restrict__ dnf = reinterpret_cast<const float*>(src + L.off[2]);
-    const int nn = n_hz * n_hm;
-    for (int i = tid; i < nn; i += blockDim.x) {
-      const float v = __ldg(dnf + i);
-      h32[i] = v;
-      bad |= !isfinite(v);
-    }
-  } else if (a.mixed) {
-    const double* __restrict__ dng = src + L.off[2];
-    const int nn = n_hz * n_hm;
-    for (int i0 = tid; i0 < nn; i0 += 4 * blockDim.x) {
-      double v[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int i = i0 + u * blockDim.x;
-        v[u] = i < nn ? __ldg(dng + i) : 0.0;
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int i = i0 + u * blockDim.x;
-        if (i < nn) h32[i] = (float)v[u];
-        bad |= !isfinite(v[u]);
-      }
-    }
-  }
   {
     long long t0 = clock64();
     uint32_t ok = 0;
@@ -310,7 +272,7 @@ prep_kernel(PrepArgs a)
   }
   // Every table entry must be finite: the staged sections (not their
   // alignment padding) and, for the FP64 form, the HMF grid in global memory
-  // (the mixed form checked it while converting).
+  // (yf_kernel checks the mixed form's copy of it).
   {
     const int len[7] = {n_hm, n_hz, 0, L.n_dist, L.n_dist, L.n_sci, L.n_sci};
     for (int sct = 0; sct < 7; ++sct) {
@@ -345,7 +307,7 @@ prep_kernel(PrepArgs a)
     const double x = xm[k];
     const double alpha = pt.B * (x - lnMpiv);
     k_alpha[k] = alpha;
-    if (lead) s64[Gp->o_alpha + k] = alpha;
+    s64[Gp->o_alpha + k] = alpha;
     const double xx = fmin(fmax(x, mh[0]), mh[n_hm - 1]);
     const int xi = bsearch_cell(mh, n_hm, xx);
     k_x[k] = xi;
@@ -359,7 +321,7 @@ prep_kernel(PrepArgs a)
     const double z = xz[q];
     const double beta = pt.A + pt.C * log1p(z);
     q_beta[q] = beta;
-    if (lead) s64[o_beta + q] = beta;
+    s64[o_beta + q] = beta;
     const double zz = fmin(fmax(z, hz[0]), hz[n_hz - 1]);
     const int yi = bsearch_cell(hz, n_hz, zz);
     q_y[q] = yi;
@@ -369,7 +331,6 @@ prep_kernel(PrepArgs a)
       set_err(a.status, kDevDomain);
       dv = 0.0;
     }
-    if (!lead) continue;
     const double cz = Gp->wz[q] * dv * Gp->omz[q];
     const double czs = cz * (L.n_sci > 1 ? interp1d_clamp(sz, sv, L.n_sci, z) : 1.0);
     s64[o_cz + q] = cz;
@@ -420,10 +381,8 @@ prep_kernel(PrepArgs a)
       red[3] = amax + bmax;
       red[4] = bmin;
       red[5] = bmax;
-      if (lead) {
-        s64[Gp->o_scal] = red[0];
-        s64[Gp->o_scal + 1] = red[1];
-      }
+      s64[Gp->o_scal] = red[0];
+      s64[Gp->o_scal + 1] = red[1];
     }
   }
   __syncthreads();
@@ -458,90 +417,112 @@ prep_kernel(PrepArgs a)
     }
     return;
   }
-  // Mixed form: factor vectors and Y(k, q).
+  // Mixed form: the contraction's factor vectors and, for yf_kernel, the
+  // per-tile row blocks, the z rows, the log2 D table and the windows.
   const double L0 = A0 + B0;
-  const int n_t = Gp->n_t, n_t_pad = Gp->n_t_pad;
-  if (lead) {
-    for (int k = tid; k < n_m_pad; k += blockDim.x)
-      s32[Gp->f_a + k] = k < n_m ? (float)(k_alpha[k] - A0) : 0.f;
-    for (int q = tid; q < n_z; q += blockDim.x) s32[Gp->f_b + q] = (float)(q_beta[q] - B0);
-    for (int t = tid; t < n_t_pad; t += blockDim.x)
-      s32[Gp->f_delta + t] = t < n_t ? (float)(Gp->xl[t] - L0) : 0.f;
-  }
-  if (lead && tid == 0) {
-    const double log2e = 1.4426950408889634;
-    s32[Gp->f_scal] = (float)(log2e * 0.5 / (sig * sig));  // c1: F = exp2(-(d - a)^2 c1)
-    s32[Gp->f_scal + 1] = (float)(log2e / (sig * sig));    // c2: G = exp2(d b c2)
-  }
-  float* __restrict__ Yt = s32 + Gp->f_Yt;
-  const float c2 = (float)(1.4426950408889634 / (sig * sig));
-  const float norm0f = (float)norm0;
+  const int n_t = Gp->n_t, n_t_pad = Gp->n_t_pad, n_mt = n_m_pad / kGemmRows;
+  for (int k = tid; k < n_m_pad; k += blockDim.x)
+    s32[Gp->f_a + k] = k < n_m ? (float)(k_alpha[k] - A0) : 0.f;
+  for (int q = tid; q < n_z; q += blockDim.x) s32[Gp->f_b + q] = (float)(q_beta[q] - B0);
+  for (int t = tid; t < n_t_pad; t += blockDim.x)
+    s32[Gp->f_delta + t] = t < n_t ? (float)(Gp->xl[t] - L0) : 0.f;
+  constexpr double kLog2e = 1.4426950408889634;
+  const double c1d = kLog2e * 0.5 / (sig * sig), c2d = kLog2e / (sig * sig);
+  const float sc1 = sqrtf((float)c1d);
   // Y is FP32: where mu is more than 5.6 sigma inside the lam_t domain,
   // 1 - D < 2^-26 and (float)D is exactly 1, the saturated scale.  The FP32
-  // test keeps a 1e-3 margin; everything else reads the FP64 table of log2 D.
+  // test keeps a 1e-3 margin; everything else reads the table of log2 D.
   const float mu_sat_lo = (float)(ll_lo + 5.6 * sig - L0) + 1e-3f;
   const float mu_sat_hi = (float)(ll_hi - 5.6 * sig - L0) - 1e-3f;
-  // FP32 copies of the per-k vectors, reusing the FP64 arrays' space is not
-  // possible (they are read below), so they go after them in h32's tail.
-  float* kt_f = reinterpret_cast<float*>(q_y + n_z);  // [n_m]
-  float* kf_f = kt_f + n_m;                            // [n_m]
-  float* ka_f = kf_f + n_m;                            // [n_m] alpha - A0
-  for (int k = tid; k < n_m; k += blockDim.x) {
-    kt_f[k] = (float)k_t[k];
-    kf_f[k] = (float)k_f[k];
-    ka_f[k] = (float)(k_alpha[k] - A0);
-  }
-  // log2 D(mu) and h dlog2D/dmu on the table nodes, FP64.  ln D comes from
-  // ln_mor_norm (finite however far mu lies outside the domain) and
-  // dlnD/dmu = (phi(a) - phi(b)) / (s D), taken in logs.  Only nodes next to
-  // a mu that fails the FP32 saturation test are read (the test's margin is
-  // 1e-3 plus FP32 rounding, and the nodes used lie within hmu of mu): the
-  // interior nodes hold log2 D = 0 without an erfc.
-  constexpr double kLog2e = 1.4426950408889634;
-  double* dtab = reinterpret_cast<double*>(
-    (reinterpret_cast<uintptr_t>(ka_f + n_m) + 7) & ~uintptr_t(7));  // [2 kDTab]
+  // log2 D(mu) and h dlog2D/dmu on kDTab equally spaced mu over the point's
+  // range of alpha_k + beta_q, evaluated in FP64 and stored in FP32 for
+  // yf_kernel's cubic Hermite.  ln D comes from ln_mor_norm (finite however
+  // far mu lies outside the domain) and dlnD/dmu = (phi(a) - phi(b)) / (s D),
+  // taken in logs.  Only nodes next to a mu that fails the FP32 saturation
+  // test are read (the test's margin is 1e-3 plus FP32 rounding, and the
+  // nodes used lie within hmu of mu): the interior nodes hold 0 without an
+  // erfc.
   const double mu0 = red[2];
   const double hmu = red[3] > red[2] ? (red[3] - red[2]) / (kDTab - 1) : 1.0;
   const double inv_hmu = 1.0 / hmu;
-  const int j_sat0 =
-    (int)fmin(fmax(ceil((ll_lo + 5.6 * sig + 0.01 - mu0) * inv_hmu) + 2.0, 0.0), (double)kDTab);
-  const int j_sat1 =
-    (int)fmin(fmax(floor((ll_hi - 5.6 * sig - 0.01 - mu0) * inv_hmu) - 2.0, 0.0), (double)kDTab);
-  const int n_lo = min(j_sat0 + 1, kDTab), n_hi = kDTab - max(j_sat1, n_lo);
-  for (int j = n_lo + tid; j < kDTab - n_hi; j += blockDim.x) {
-    dtab[j] = 0.0;
-    dtab[kDTab + j] = 0.0;
+  {
+    float* dt32 = s32 + Gp->f_dt32;
+    const int j_sat0 =
+      (int)fmin(fmax(ceil((ll_lo + 5.6 * sig + 0.01 - mu0) * inv_hmu) + 2.0, 0.0), (double)kDTab);
+    const int j_sat1 =
+      (int)fmin(fmax(floor((ll_hi - 5.6 * sig - 0.01 - mu0) * inv_hmu) - 2.0, 0.0), (double)kDTab);
+    const int n_lo = min(j_sat0 + 1, kDTab), n_hi = kDTab - max(j_sat1, n_lo);
+    for (int j = n_lo + tid; j < kDTab - n_hi; j += blockDim.x) {
+      dt32[j] = 0.f;
+      dt32[kDTab + j] = 0.f;
+    }
+    for (int r = tid; r < n_lo + n_hi; r += blockDim.x) {
+      const int j = r < n_lo ? r : kDTab - n_hi + (r - n_lo);
+      const double mu = mu0 + j * hmu;
+      const double aa = (ll_lo - mu) * inv_s, bb = (ll_hi - mu) * inv_s;
+      const double lnD = ln_mor_norm(aa, bb);
+      dt32[j] = (float)(kLog2e * lnD);
+      dt32[kDTab + j] = (float)(hmu * inv_s * kLog2e *
+                                (exp(-0.5 * aa * aa - lnD) - exp(-0.5 * bb * bb - lnD)) / kSqrt2Pi);
+    }
   }
-  for (int r = tid; r < n_lo + n_hi; r += blockDim.x) {
-    const int j = r < n_lo ? r : kDTab - n_hi + (r - n_lo);
-    const double mu = mu0 + j * hmu;
-    const double aa = (ll_lo - mu) * inv_s, bb = (ll_hi - mu) * inv_s;
-    const double lnD = ln_mor_norm(aa, bb);
-    dtab[j] = kLog2e * lnD;
-    dtab[kDTab + j] = hmu * inv_s * kLog2e *
-                      (exp(-0.5 * aa * aa - lnD) - exp(-0.5 * bb * bb - lnD)) / kSqrt2Pi;
+  if (tid == 0) {
+    s32[Gp->f_scal] = (float)c1d;      // c1: F = exp2(-(d - a)^2 c1)
+    s32[Gp->f_scal + 1] = (float)c2d;  // c2: G = exp2(d b c2)
+    float* fh = s32 + Gp->f_hdr;
+    fh[0] = (float)c2d;
+    fh[1] = mu_sat_lo;
+    fh[2] = mu_sat_hi;
+    fh[3] = sc1;
+    fh[4] = (float)(mu0 - L0);
+    fh[5] = (float)inv_hmu;
+    fh[6] = 0.f;
+    fh[7] = 0.f;
+    double* th = s64 + Gp->o_thdr;
+    th[0] = A0;
+    th[1] = B0;
+    th[2] = mu0;
+    th[3] = inv_hmu;
+    th[4] = c2d;
+    th[5] = ll_lo;
+    th[6] = ll_hi;
+    th[7] = inv_s;
+  }
+  {  // z rows: HMF z cell, its weight, b_q = beta_q - B0
+    const int nzp = Gp->nzp;
+    int* qy = reinterpret_cast<int*>(s32 + Gp->f_q);
+    float* qu = s32 + Gp->f_q + nzp;
+    float* qb = qu + nzp;
+    for (int q = tid; q < nzp; q += blockDim.x) {
+      qy[q] = q < n_z ? q_y[q] : 0;
+      qu[q] = q < n_z ? (float)q_u[q] : 0.f;
+      qb[q] = q < n_z ? (float)(q_beta[q] - B0) : 0.f;
+    }
   }
   float* dt_f = reinterpret_cast<float*>(
-    (reinterpret_cast<uintptr_t>(dtab + 2 * kDTab) + 15) & ~uintptr_t(15));  // [n_t_pad]
+    (reinterpret_cast<uintptr_t>(q_y + n_z) + 15) & ~uintptr_t(15));  // [n_t_pad]
   for (int t = tid; t < n_t_pad; t += blockDim.x) dt_f[t] = t < n_t ? (float)(Gp->xl[t] - L0) : 0.f;
+  __shared__ float tile_af[16];  // per lnM tile: min and max of its rows' FP32 a_k
+  __shared__ int tile_sc[8];     // per lnM tile: some row carries a scale
+  for (int mt = tid; mt < 8; mt += blockDim.x) tile_sc[mt] = 0;
   __syncthreads();
   const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
-  // lam_t window of the contraction per lnM tile.  Each (k, q) cell's
-  // density exp(-(l - mu)^2 / 2 s^2) / D is renormalised to the lam_t domain
-  // [ll_lo, ll_hi], where it peaks at c = clamp(mu, ll_lo, ll_hi); it is below
-  // 4e-6 of that peak outside mu -+ R(mu), R = sqrt((c - mu)^2 + (5 s)^2).
-  // For mu inside the domain that is mu -+ 5 s (Gaussian mass 3e-7 per side);
-  // for mu below ll_lo (above ll_hi) the window reaches from the domain edge
-  // to where the renormalised density has fallen by the same factor, so cells
-  // whose in-range mass D is small keep all of it.  mu -+ R(mu) increase with
-  // mu, so the tile's window runs from the lower end for its smallest mu to
-  // the upper end for its largest; stages outside add less than the rounding
-  // of the split-BF16 products.  The stage count is rounded up to pairs.
-  __shared__ float tile_af[2];
+  // lam_t window of the contraction per lnM tile, one warp per tile.  Each
+  // (k, q) cell's density exp(-(l - mu)^2 / 2 s^2) / D is renormalised to the
+  // lam_t domain [ll_lo, ll_hi], where it peaks at c = clamp(mu, ll_lo,
+  // ll_hi); it is below 4e-6 of that peak outside mu -+ R(mu),
+  // R = sqrt((c - mu)^2 + (5 s)^2).  For mu inside the domain that is
+  // mu -+ 5 s (Gaussian mass 3e-7 per side); for mu below ll_lo (above
+  // ll_hi) the window reaches from the domain edge to where the renormalised
+  // density has fallen by the same factor, so cells whose in-range mass D is
+  // small keep all of it.  mu -+ R(mu) increase with mu, so the tile's window
+  // runs from the lower end for its smallest mu to the upper end for its
+  // largest; stages outside add less than the rounding of the split-BF16
+  // products.  The stage count is rounded up to pairs.
   {
     constexpr double kWin = 5.0;
     const int nk = n_t_pad / 16;
-    for (int mt = mt0 + warp; mt == mt0; mt += nw) {  // this CTA's tile, warp 0
+    for (int mt = warp; mt < n_mt; mt += nw) {
       double amn = 1e300, amx = -1e300;
       for (int k = mt * kGemmRows + lane; k < min(n_m, (mt + 1) * kGemmRows); k += 32) {
         amn = fmin(amn, k_alpha[k]);
@@ -584,91 +565,261 @@ prep_kernel(PrepArgs a)
         swin[2 * mt + 1] = hi;
         // The tile's range of a_k = alpha_k - A0 as FP32: rounding is
         // monotone, so these are the min and max of its rows' FP32 a_k.
-        tile_af[0] = (float)(amn - A0);
-        tile_af[1] = (float)(amx - A0);
+        tile_af[2 * mt] = (float)(amn - A0);
+        tile_af[2 * mt + 1] = (float)(amx - A0);
       }
     }
   }
   __syncthreads();
-  // Row scale of the tile.  F(t, k) = 2^-((delta_t - a_k)^2 c1) underflows
-  // FP32 on every issued node when a_k lies far outside the issued nodes'
-  // span [e_lo, e_hi] (mu many sigma outside the lam_t domain), while its
+  // Row scale.  F(t, k) = 2^-((delta_t - a_k)^2 c1) underflows FP32 on every
+  // issued node when a_k lies far outside the issued nodes' span [e_lo, e_hi]
+  // of its tile (mu many sigma outside the lam_t domain), while its
   // Y(k, q) = n H / D overflows: the product, the renormalised density at
   // the domain edge, is moderate.  With c_k = clamp(a_k, e_lo, e_hi) and
   // v_k = c_k - a_k the row carries F'(t, k) = F 2^(v_k^2 c1) =
   // 2^-((delta_t - c_k)(delta_t - c_k + 2 v_k) c1) <= 1 and
-  // Y'(k, q) = Y 2^-(v_k^2 c1), computed from ln D in FP64.  Rows inside
-  // the span keep v_k = 0 and the unscaled factors bit for bit.
-  const float sc1 = sqrtf((float)(1.4426950408889634 * 0.5 / (sig * sig)));
-  __shared__ float row_am[kGemmRows], row_vs2[kGemmRows], row_vvf[kGemmRows], row_t[kGemmRows];
-  __shared__ int row_x[kGemmRows];
-  __shared__ double row_vv[kGemmRows];
-  __shared__ int tile_scaled;
-  if (tid == 0) tile_scaled = 0;
-  __syncthreads();
-  {
-    const int t_first = swin[2 * mt0] * 16, t_last = min(swin[2 * mt0 + 1] * 16, n_t) - 1;
-    const double c_lo = t_last >= t_first ? (double)dt_f[t_first] : -1e300;
-    const double c_hi = t_last >= t_first ? (double)dt_f[t_last] : 1e300;
-    const double c1d = 1.4426950408889634 * 0.5 / (sig * sig);
-    for (int r = tid; r < kGemmRows; r += blockDim.x) {
-      const int k = mt0 * kGemmRows + r;
-      float am = 1e18f, vs2 = 0.f;
-      double vv = 0.0;
-      if (k < n_m) {
-        const double ak = k_alpha[k] - A0;
-        if (ak < c_lo || ak > c_hi) {
-          const float cf = ak < c_lo ? dt_f[t_first] : dt_f[t_last];
-          const double v = (double)cf - ak;
-          am = cf * sc1;
-          vs2 = (float)(2.0 * v) * sc1;
-          vv = v * v * c1d;
-        } else {
-          am = ka_f[k] * sc1;
-        }
+  // Y'(k, q) = Y 2^-(v_k^2 c1), formed from ln D in FP64.  Rows inside the
+  // span keep v_k = 0 and the unscaled factors bit for bit.  Row block of
+  // yf_kernel, per tile [field][128]: t, cell, kf / (sqrt(2 pi) s), a,
+  // F centre c sqrt(c1), 2 v sqrt(c1), v^2 c1, valid.
+  for (int r = tid; r < n_m_pad; r += blockDim.x) {
+    const int mt = r / kGemmRows, k = r;
+    const int t_first = swin[2 * mt] * 16, t_last = min(swin[2 * mt + 1] * 16, n_t) - 1;
+    float am = 1e18f, vs2 = 0.f;
+    double vv = 0.0;
+    if (k < n_m) {
+      const double ak = k_alpha[k] - A0;
+      const double c_lo = t_last >= t_first ? (double)dt_f[t_first] : -1e300;
+      const double c_hi = t_last >= t_first ? (double)dt_f[t_last] : 1e300;
+      if (ak < c_lo || ak > c_hi) {
+        const float cf = ak < c_lo ? dt_f[t_first] : dt_f[t_last];
+        const double v = (double)cf - ak;
+        am = cf * sc1;
+        vs2 = (float)(2.0 * v) * sc1;
+        vv = v * v * c1d;
+      } else {
+        am = (float)ak * sc1;
       }
-      row_am[r] = am;
-      row_vs2[r] = vs2;
-      row_vv[r] = vv;
-      row_vvf[r] = (float)vv;
-      row_t[r] = k < n_m ? kt_f[k] : 0.f;
-      row_x[r] = k < n_m ? k_x[k] : 0;
-      if (vv != 0.0) tile_scaled = 1;
+    }
+    float* rw = s32 + Gp->f_rows + (size_t)mt * kYfRowFields * kGemmRows + (r & (kGemmRows - 1));
+    const bool ok = k < n_m;
+    rw[0 * kGemmRows] = ok ? (float)k_t[k] : 0.f;
+    rw[1 * kGemmRows] = __int_as_float(ok ? k_x[k] : 0);
+    rw[2 * kGemmRows] = ok ? (float)(k_f[k] * norm0) : 0.f;
+    rw[3 * kGemmRows] = ok ? (float)(k_alpha[k] - A0) : 0.f;
+    rw[4 * kGemmRows] = am;
+    rw[5 * kGemmRows] = vs2;
+    rw[6 * kGemmRows] = (float)vv;
+    rw[7 * kGemmRows] = __int_as_float(ok ? 1 : 0);
+    s64[Gp->o_vv + r] = vv;
+    if (vv != 0.0) tile_sc[mt] = 1;
+  }
+  __syncthreads();
+  // Per tile: yf_kernel's info, the exponent-range guard and the windows of
+  // the contraction tiles (lnM tile, richness-bin group).  G = 2^(delta b c2)
+  // over the issued stages and H = 2^(-(a b + b^2/2) c2) must stay well
+  // inside FP32 / BF16 (2^-126 .. 2^127).  |a| <= (max alpha - min alpha) / 2
+  // and |b| <= (max beta - min beta) / 2 after centring, so the bound below
+  // holds for every factor; a point beyond it reports kDevRange (its FP64
+  // form is unaffected).
+  for (int mt = tid; mt < n_mt; mt += blockDim.x) {
+    float* ti = s32 + Gp->f_tinfo + 4 * mt;
+    ti[0] = tile_af[2 * mt];
+    ti[1] = tile_af[2 * mt + 1];
+    ti[2] = __int_as_float(tile_sc[mt]);
+    ti[3] = __int_as_float(swin[2 * mt] | (swin[2 * mt + 1] << 16));
+    double dmax = 0.0;
+    const int t0 = swin[2 * mt] * 16, t1 = min(swin[2 * mt + 1] * 16, n_t) - 1;
+    if (t1 >= t0) dmax = fmax(fabs((double)dt_f[t0]), fabs((double)dt_f[t1]));
+    const double bmax = 0.5 * (red[5] - red[4]);
+    const double amax = 0.5 * ((red[3] - red[2]) - (red[5] - red[4]));
+    const double e = c2d * bmax * fmax(dmax, amax + 0.5 * bmax);
+    if (!(e <= kMaxExp2)) set_err(a.status, kDevRange);
+  }
+  for (int l = tid; l < Gp->tiles_pp; l += blockDim.x) {
+    const int mt = l / Gp->n_bg;
+    a.win_tile[(size_t)p * a.win_stride + l] = swin[2 * mt] | (swin[2 * mt + 1] << 16);
+  }
+}
+
+// Bulk async copy global -> shared completing on mbarrier `bar` (16-byte
+// aligned addresses, a size that is a multiple of 16).
+__device__ __forceinline__ void
+bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+  asm volatile(
+    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+      smem_addr(dst)),
+    "l"(src), "r"(bytes), "r"(smem_addr(bar))
+    : "memory");
+}
+
+// Shared memory of yf_kernel: HMF grid in FP32 | row block | row scale |
+// tile info | headers | z rows | log2 D table | delta_t.
+__host__ __device__ inline size_t
+yf_h32_bytes(const TableLayout& L)
+{
+  const size_t n_dn = (size_t)L.n_hz * L.n_hm;
+  return L.hmf_f32 ? ((n_dn + 1) / 2 + 1) / 2 * 16 : (n_dn * 4 + 15) & ~size_t(15);
+}
+
+__host__ __device__ inline size_t
+yf_smem_bytes(const TableLayout& L, int nzp_max, int n_t_pad_max)
+{
+  return yf_h32_bytes(L) + (size_t)kYfRowFields * kGemmRows * 4 + kGemmRows * 8 + 16 +
+         kYfHdr * 4 + 8 * 8 + 3 * (size_t)nzp_max * 4 + 2 * (size_t)kDTab * 4 +
+         (size_t)n_t_pad_max * 4;
+}
+
+// Mixed form, one CTA per (point, 128-row lnM tile): Y(k, q) of the tile's
+// rows and its F(t, k) stage blocks, from the inputs the prep kernel wrote,
+// staged into shared memory by bulk copies on one mbarrier (the HMF grid
+// too when the packed tables hold it in FP32; an FP64 grid is converted
+// while the copies fly).
+__global__ void __launch_bounds__(256, 3)
+yf_kernel(PrepArgs a)
+{
+  extern __shared__ __align__(16) uint8_t ysh[];
+  const int p = blockIdx.x, mt0 = blockIdx.y, tid = threadIdx.x;
+  const PointDev pt = a.pts[p];
+  if (!grid_in_mask(a.grid_mask, pt.grid)) return;  // the prep kernel reported it
+  const GridDev* __restrict__ Gp = a.grids + pt.grid;
+  const int n_m = Gp->n_m, n_z = Gp->n_z, n_t_pad = Gp->n_t_pad, nzp = Gp->nzp;
+  if (mt0 >= Gp->n_m_pad / kGemmRows) return;
+  const TableLayout& L = a.lay;
+  const int n_hm = L.n_hm, n_hz = L.n_hz;
+  float* s32 = a.s32 + (size_t)p * Gp->s32_stride;
+  const double* s64 = a.s64 + (size_t)p * Gp->s64_stride;
+  const double* src = a.tables + (size_t)(a.slot ? a.slot[p] : p) * L.stride;
+  size_t o = 0;
+  float* h32 = reinterpret_cast<float*>(ysh);  // [n_hz n_hm]
+  o += yf_h32_bytes(L);
+  float* rows = reinterpret_cast<float*>(ysh + o);  // [kYfRowFields][128]
+  o += kYfRowFields * kGemmRows * 4;
+  double* row_vv = reinterpret_cast<double*>(ysh + o);  // [128]
+  o += kGemmRows * 8;
+  const int* tinfo = reinterpret_cast<const int*>(ysh + o);  // [4]
+  o += 16;
+  const float* fh = reinterpret_cast<const float*>(ysh + o);  // [kYfHdr]
+  o += kYfHdr * 4;
+  const double* th = reinterpret_cast<const double*>(ysh + o);  // [8]
+  o += 8 * 8;
+  const int* qy = reinterpret_cast<const int*>(ysh + o);  // [3][nzp]
+  const float* qu = reinterpret_cast<const float*>(qy + nzp);
+  const float* qb = qu + nzp;
+  o += 3 * (size_t)nzp * 4;
+  const float* dt32 = reinterpret_cast<const float*>(ysh + o);  // [2][kDTab]
+  o += 2 * (size_t)kDTab * 4;
+  const float* dt_f = reinterpret_cast<const float*>(ysh + o);  // [n_t_pad]
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int timed_out;
+  int bad = 0;
+  const size_t n_dn = (size_t)n_hz * n_hm;
+  const uint32_t h_bytes = L.hmf_f32 ? (uint32_t)yf_h32_bytes(L) : 0u;
+  const uint32_t bytes = h_bytes + kYfRowFields * kGemmRows * 4 + kGemmRows * 8 + 16 + kYfHdr * 4 +
+                         64 + 12u * nzp + 8u * kDTab + 4u * n_t_pad;
+  if (tid == 0) {
+    timed_out = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar)),
+                 "r"(bytes)
+                 : "memory");
+    if (h_bytes) bulk_copy_g2s(h32, src + L.off[2], h_bytes, &bar);
+    bulk_copy_g2s(rows, s32 + Gp->f_rows + (size_t)mt0 * kYfRowFields * kGemmRows,
+                  kYfRowFields * kGemmRows * 4, &bar);
+    bulk_copy_g2s(row_vv, s64 + Gp->o_vv + (size_t)mt0 * kGemmRows, kGemmRows * 8, &bar);
+    bulk_copy_g2s((void*)tinfo, s32 + Gp->f_tinfo + 4 * mt0, 16, &bar);
+    bulk_copy_g2s((void*)fh, s32 + Gp->f_hdr, kYfHdr * 4, &bar);
+    bulk_copy_g2s((void*)th, s64 + Gp->o_thdr, 64, &bar);
+    bulk_copy_g2s((void*)qy, s32 + Gp->f_q, 12u * nzp, &bar);
+    bulk_copy_g2s((void*)dt32, s32 + Gp->f_dt32, 8u * kDTab, &bar);
+    bulk_copy_g2s((void*)dt_f, s32 + Gp->f_delta, 4u * n_t_pad, &bar);
+  }
+  if (!L.hmf_f32) {  // FP64 grid: convert while the copies are in flight
+    const double* __restrict__ dng = src + L.off[2];
+    const int nn = (int)n_dn;
+    for (int i0 = tid; i0 < nn; i0 += 4 * blockDim.x) {
+      double v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = i0 + u * blockDim.x;
+        v[u] = i < nn ? __ldg(dng + i) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = i0 + u * blockDim.x;
+        if (i < nn) h32[i] = (float)v[u];
+        bad |= !isfinite(v[u]) || !isfinite((float)v[u]);
+      }
+    }
+  }
+  {
+    long long t0 = clock64();
+    uint32_t ok = 0;
+    while (!ok) {
+      asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(&bar))
+        : "memory");
+      if (!ok && clock64() - t0 > 2000000000LL) {
+        timed_out = 1;
+        break;
+      }
     }
   }
   __syncthreads();
+  if (timed_out) {  // uniform exit; the copies only target this CTA's shared memory
+    if (tid == 0) set_err(a.status, kDevTimeout);
+    return;
+  }
+  if (L.hmf_f32)
+    for (int i = tid; i < (int)n_dn; i += blockDim.x) bad |= !isfinite(h32[i]);
+  if (__syncthreads_or(bad)) {
+    if (tid == 0) set_err(a.status, kDevNonFinite);
+    return;
+  }
+  const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+  const float c2 = fh[0], mu_sat_lo = fh[1], mu_sat_hi = fh[2], sc1 = fh[3];
+  const float mu0c = fh[4], inv_hmu_f = fh[5];
+  constexpr double kLog2e = 1.4426950408889634;
   // Y(k, q) = n(M_k, z_q) kf_k H(k, q) 2^-(v_k^2 c1) / (sqrt(2 pi) s D_kq).
   // Warp w takes a contiguous run of z rows and lane the tile rows
   // lane + 32 j (j < 4).  Each lane keeps, in registers, the two HMF z rows
   // around the current z_q interpolated in mass and scaled by
   // kf_k / (sqrt(2 pi) s), and advances them with q (the z nodes ascend).  A
   // z row whose tile cells all have mu more than 5.6 sigma inside the domain
-  // (D = 1 in FP32) is FP32 only; otherwise each unsaturated cell takes
-  // log2 D from the FP64 table and forms 2^(log2 H - v^2 c1 - log2 D) in
-  // FP64, applied as an exact power of two times 2^(fraction) in FP32.
-  const double c2d = kLog2e / (sig * sig);
+  // (D = 1 in FP32) is FP32 only.  Otherwise an unsaturated cell takes
+  // log2 D from the table by a cubic Hermite in FP32 where D >= 2^-8 (its
+  // relative error there ~1e-6); deeper in a tail, and in rows that carry a
+  // scale, it forms 2^(log2 H - v^2 c1 - log2 D) in FP64 from ln D itself,
+  // applied as an exact power of two times 2^(fraction) in FP32.
   {
-    const int qs = (n_z + nw - 1) / nw, qa = warp * qs, qb = min(n_z, qa + qs);
-    // Per row: mass-interpolation weight and cell, kf_k / (sqrt(2 pi) s)
-    // (0 past n_m), a_k; the row scale v_k^2 c1 is read only in tiles that
-    // have such rows.
-    float* rt_s = row_t;
-    int* rx_s = row_x;
+    const float* rt_s = rows;
+    const int* rx_s = reinterpret_cast<const int*>(rows + kGemmRows);
+    const float* rn_s = rows + 2 * kGemmRows;
+    const float* ra_s = rows + 3 * kGemmRows;
+    const float* rvf_s = rows + 6 * kGemmRows;
+    const int* rok_s = reinterpret_cast<const int*>(rows + 7 * kGemmRows);
+    const int qs = (n_z + nw - 1) / nw, qa = warp * qs, qb_end = min(n_z, qa + qs);
     float rn[4], rk[4], R0[4], R1[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const int r = lane + 32 * j, k = mt0 * kGemmRows + r;
-      const bool ok = k < n_m;
-      rn[j] = ok ? kf_f[k] * norm0f : 0.f;
-      rk[j] = ok ? ka_f[k] : 0.f;
+      rn[j] = rn_s[lane + 32 * j];
+      rk[j] = ra_s[lane + 32 * j];
       R0[j] = R1[j] = 0.f;
     }
-    const float tmin = tile_af[0], tmax = tile_af[1];
-    const bool scaled = tile_scaled != 0;
-    float* __restrict__ yblk = Yt + (size_t)mt0 * n_z * kGemmRows;
+    const float tmin = __int_as_float(tinfo[0]), tmax = __int_as_float(tinfo[1]);
+    const bool scaled = tinfo[2] != 0;
+    float* __restrict__ yblk = s32 + Gp->f_Yt + (size_t)mt0 * n_z * kGemmRows;
     int ycur = -2;
-    for (int q = qa; q < qb; ++q) {
-      const int yq = q_y[q];
+    for (int q = qa; q < qb_end; ++q) {
+      const int yq = qy[q];
       if (yq != ycur) {  // warp-uniform
         const float* h1 = h32 + (size_t)(yq + 1) * n_hm;
         if (yq == ycur + 1) {
@@ -690,32 +841,37 @@ prep_kernel(PrepArgs a)
         }
         ycur = yq;
       }
-      const float u = (float)q_u[q];
-      const float bb = (float)(q_beta[q] - B0);
+      const float u = qu[q], bb = qb[q];
       const float hx = -bb * c2, hy = -0.5f * bb * bb * c2;  // H = 2^(a hx + hy)
       const float sat_lo = mu_sat_lo - bb, sat_hi = mu_sat_hi - bb;
-      float y[4], nv[4];
+      float y[4], nv[4], e[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         nv[j] = fmaf(u, R1[j] - R0[j], R0[j]);
-        const float e = fmaf(rk[j], hx, hy);
-        y[j] = nv[j] * fast_exp2(scaled ? e - row_vvf[lane + 32 * j] : e);
+        e[j] = scaled ? fmaf(rk[j], hx, hy) - rvf_s[lane + 32 * j] : fmaf(rk[j], hx, hy);
+        y[j] = nv[j] * fast_exp2(e[j]);
       }
       if (!(tmin > sat_lo && tmax < sat_hi)) {  // some cell of this z row is unsaturated
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          const int r = lane + 32 * j, k = mt0 * kGemmRows + r;
-          if (k >= n_m || (rk[j] > sat_lo && rk[j] < sat_hi)) continue;
-          const double mu = k_alpha[k] + q_beta[q];
-          const double uu = (mu - mu0) * inv_hmu;
-          const int jj = min(max((int)uu, 0), kDTab - 2);
-          const double t = uu - jj, t2 = t * t, t3 = t2 * t;
-          const double l2d = (2.0 * t3 - 3.0 * t2 + 1.0) * dtab[jj] +
-                             (t3 - 2.0 * t2 + t) * dtab[kDTab + jj] +
-                             (3.0 * t2 - 2.0 * t3) * dtab[jj + 1] +
-                             (t3 - t2) * dtab[kDTab + jj + 1];
-          const double ad = k_alpha[k] - A0, bd = q_beta[q] - B0;
-          const double ex = -(ad * bd + 0.5 * bd * bd) * c2d - row_vv[r] - l2d;
+          const int r = lane + 32 * j;
+          if (!rok_s[r] || (rk[j] > sat_lo && rk[j] < sat_hi)) continue;
+          const float uu = (rk[j] + bb - mu0c) * inv_hmu_f;
+          const int jj = min(max((int)floorf(uu), 0), kDTab - 2);
+          const float t = uu - (float)jj, t2 = t * t, t3 = t2 * t;
+          const float l2d = (2.f * t3 - 3.f * t2 + 1.f) * dt32[jj] +
+                            (t3 - 2.f * t2 + t) * dt32[kDTab + jj] +
+                            (3.f * t2 - 2.f * t3) * dt32[jj + 1] + (t3 - t2) * dt32[kDTab + jj + 1];
+          if (l2d >= -8.f && row_vv[r] == 0.0) {
+            y[j] = nv[j] * fast_exp2(e[j] - l2d);
+            continue;
+          }
+          const int k = mt0 * kGemmRows + r;
+          const double alpha = s64[Gp->o_alpha + k], beta = s64[Gp->o_beta + q];
+          const double mu = alpha + beta;
+          const double lnD = ln_mor_norm((th[5] - mu) * th[7], (th[6] - mu) * th[7]);
+          const double ad = alpha - th[0], bd = beta - th[1];
+          const double ex = -(ad * bd + 0.5 * bd * bd) * th[4] - row_vv[r] - kLog2e * lnD;
           const double ei = rint(ex);
           const float yf = mul_pow2(nv[j] * fast_exp2((float)(ex - ei)), ei);
           if (!(fabsf(yf) <= 3.402823466e38f)) {  // not representable: report, never a NaN
@@ -730,40 +886,23 @@ prep_kernel(PrepArgs a)
       for (int j = 0; j < 4; ++j) yblk[(size_t)q * kGemmRows + lane + 32 * j] = y[j];
     }
   }
-  // Exponent range of the factorised form: G = 2^(delta b c2) over the
-  // issued stages and H = 2^(-(a b + b^2/2) c2) must stay well inside FP32 /
-  // BF16 (2^-126 .. 2^127).  |a| <= (max alpha - min alpha) / 2 and
-  // |b| <= (max beta - min beta) / 2 after centring, so the bound below holds
-  // for every factor; a point beyond it reports kDevRange (its FP64 form is
-  // unaffected).
-  if (tid == 0) {
-    double dmax = 0.0;
-    {
-      const int t0 = swin[2 * mt0] * 16, t1 = min(swin[2 * mt0 + 1] * 16, n_t) - 1;
-      if (t1 >= t0) dmax = fmax(dmax, fmax(fabs((double)dt_f[t0]), fabs((double)dt_f[t1])));
-    }
-    const double bmax = 0.5 * (red[5] - red[4]);
-    const double amax = 0.5 * ((red[3] - red[2]) - (red[5] - red[4]));
-    const double e = 1.4426950408889634 / (sig * sig) * bmax * fmax(dmax, amax + 0.5 * bmax);
-    if (!(e <= kMaxExp2)) set_err(a.status, kDevRange);
-  }
-  // The window of each contraction tile (lnM tile, richness-bin group).
-  for (int l = mt0 * Gp->n_bg + tid; l < (mt0 + 1) * Gp->n_bg; l += blockDim.x)
-    a.win_tile[(size_t)p * a.win_stride + l] = swin[2 * mt0] | (swin[2 * mt0 + 1] << 16);
   // F'(t, k) for the contraction (the row scale above), split into bf16
   // hi + lo and written in its shared-memory stage layout: block
   // (lnM tile, stage) of kFStageBytes, hi planes then lo planes, each plane
   // 8 lam_t nodes x 128 rows of 16 bytes.  Rows past n_m are zero.  The
   // exponent is >= 0 on every real node; the padded nodes past n_t (whose G
-  // is zero) take its magnitude, so F' <= 1 stays finite there too.
+  // is zero) take its magnitude, so F' <= 1 stays finite there too.  Only
+  // the stages inside the tile's window are ever read.
+  (void)n_m;
+  const int win = tinfo[3], w_lo = win & 0xFFFF, w_hi = win >> 16;
+  const float* row_am = rows + 4 * kGemmRows;
+  const float* row_vs2 = rows + 5 * kGemmRows;
   const float2 sc2 = make_float2(sc1, sc1);
   uint8_t* fb = a.fbuf + (size_t)p * a.f_stride;
   const int nk = n_t_pad / 16;
-  // Only the stages inside the tile's window are ever read.
-  for (int it = swin[2 * mt0] * 2 * kGemmRows + tid; it < swin[2 * mt0 + 1] * 2 * kGemmRows;
-       it += blockDim.x) {
-    const int m = mt0 * kGemmRows + it % kGemmRows, t8 = it / kGemmRows;
-    const float am = row_am[m & (kGemmRows - 1)], vs = row_vs2[m & (kGemmRows - 1)];
+  for (int it = w_lo * 2 * kGemmRows + tid; it < w_hi * 2 * kGemmRows; it += blockDim.x) {
+    const int r = it % kGemmRows, t8 = it / kGemmRows;
+    const float am = row_am[r], vs = row_vs2[r];
     const float2 nam2 = make_float2(-am, -am), vs2 = make_float2(vs, vs);
     const float4 d0 = *reinterpret_cast<const float4*>(dt_f + t8 * 8);
     const float4 d1 = *reinterpret_cast<const float4*>(dt_f + t8 * 8 + 4);
@@ -776,8 +915,7 @@ prep_kernel(PrepArgs a)
       const float2 e = __fmul2_rn(x, __fadd2_rn(x, vs2));
       v[u] = make_float2(fast_exp2(-fabsf(e.x)), fast_exp2(-fabsf(e.y)));
     }
-    uint8_t* st = fb + ((size_t)(m >> 7) * nk + (t8 >> 1)) * kFStageBytes + (t8 & 1) * 2048 +
-                  (m & 127) * 16;
+    uint8_t* st = fb + ((size_t)mt0 * nk + (t8 >> 1)) * kFStageBytes + (t8 & 1) * 2048 + r * 16;
     store_split8(st, st + kFStageBytes / 2, v);
   }
 }
@@ -1082,7 +1220,7 @@ struct y3b_engine {
   unsigned long long graph_clock = 0;
   size_t s64_stride = 0, s32_stride = 0;
   int w_stride = 0, nB_max = 0, nI_max = 0, nz_max = 0, nt_max = 0;
-  size_t prep_smem = 0, direct_smem = 0;
+  size_t prep_smem = 0, yf_smem = 0, direct_smem = 0;
   size_t device_bytes = 0;
   int last_n = 0;
   std::vector<std::array<double, 2>> zt_node_range;  // per grid: min, max z_t node
@@ -1277,16 +1415,33 @@ build_grid(y3b_engine* e, int gi)
   o += pad2((size_t)g.n_z * g.n_m);
   g.o_V = o;
   o += pad2((size_t)g.nI * g.n_z * g.n_m);
+  g.o_thdr = o;
+  o += 8;
+  g.o_vv = o;
+  o += pad2(g.n_m_pad);
   g.s64_stride = o;
+  // FP32 scratch: every section a multiple of 4 floats (16 bytes), so that
+  // the bulk copies of yf_kernel and the contraction start aligned.
+  g.nzp = (g.n_z + 3) & ~3;
   size_t f = 0;
   g.f_a = f;
   f += g.n_m_pad;
   g.f_b = f;
-  f += (g.n_z + 3) & ~3;
+  f += g.nzp;
   g.f_delta = f;
   f += g.n_t_pad;
   g.f_scal = f;
   f += 4;
+  g.f_hdr = f;
+  f += kYfHdr;
+  g.f_tinfo = f;
+  f += 4 * (size_t)(g.n_m_pad / kGemmRows);
+  g.f_q = f;
+  f += 3 * (size_t)g.nzp;
+  g.f_dt32 = f;
+  f += 2 * (size_t)kDTab;
+  g.f_rows = f;
+  f += (size_t)kYfRowFields * g.n_m_pad;
   g.f_Yt = f;
   f += (size_t)g.n_z * g.n_m_pad;
   g.f_CN = f;
@@ -1428,9 +1583,10 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
   }
   int ntp_max = 0;
   for (const auto& g : e->grids) ntp_max = std::max(ntp_max, g.n_t_pad);
-  e->prep_smem = prep_smem_bytes(L, L.n_hz, L.n_hm, e->w_stride, e->nz_max, ntp_max);
+  e->prep_smem = prep_smem_bytes(L, e->w_stride, e->nz_max, ntp_max);
+  e->yf_smem = yf_smem_bytes(L, (e->nz_max + 3) & ~3, ntp_max);
   e->direct_smem = ((size_t)e->nI_max * e->nt_max + e->nt_max) * 8;
-  if (e->prep_smem > 200 * 1024 || e->direct_smem > 200 * 1024) {
+  if (e->prep_smem > 200 * 1024 || e->yf_smem > 200 * 1024 || e->direct_smem > 200 * 1024) {
     set_error("y3b_engine_create: per-point tables too large for shared-memory staging");
     return fail(Y3B_ERR_UNSUPPORTED);
   }
@@ -1565,9 +1721,13 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
   if (rc) return fail(rc);
   Y3B_CUDA(cudaFuncSetAttribute(prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)e->prep_smem));
-  // Four 256-thread CTAs per SM (the register limit) need ~57 KB of shared
-  // memory each at 256 lnM x 128 z nodes: ask for the largest carveout.
+  Y3B_CUDA(cudaFuncSetAttribute(yf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)e->yf_smem));
+  // Several 256-thread CTAs per SM (three for yf_kernel, the register limit,
+  // at ~37 KB each at 256 lnM x 128 z nodes): ask for the largest carveout.
   Y3B_CUDA(cudaFuncSetAttribute(prep_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                (int)cudaSharedmemCarveoutMaxShared));
+  Y3B_CUDA(cudaFuncSetAttribute(yf_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                 (int)cudaSharedmemCarveoutMaxShared));
   Y3B_CUDA(cudaFuncSetAttribute(direct_main_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)e->direct_smem));
@@ -1674,9 +1834,14 @@ enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_t
   }
   {
     StageTimer t(e, s, 0);
-    prep_kernel<<<dim3(n, mixed ? e->max_mtiles : 1), 256, e->prep_smem, s>>>(pa);
+    prep_kernel<<<n, 256, e->prep_smem, s>>>(pa);
     count_launch();
-    const cudaError_t perr = cudaGetLastError();
+    cudaError_t perr = cudaGetLastError();
+    if (mixed && perr == cudaSuccess) {
+      yf_kernel<<<dim3(n, e->max_mtiles), 256, e->yf_smem, s>>>(pa);
+      count_launch();
+      perr = cudaGetLastError();
+    }
     if (mixed) Y3B_CUDA(cudaStreamWaitEvent(s, e->plan_join, 0));
     Y3B_CUDA(perr);
   }

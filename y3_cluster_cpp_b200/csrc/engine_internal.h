@@ -53,8 +53,13 @@ struct GridDev {
   size_t s64_stride;  // doubles per point in the FP64 scratch
   size_t o_scal, o_kx, o_kt, o_kf, o_qy, o_qu;  // A0/B0, HMF cells and weights
   size_t o_cz, o_czs, o_alpha, o_beta, o_P0, o_V;
+  size_t o_thdr, o_vv;  // mixed form: FP64 header and row scale v_k^2 c1 of yf_kernel
   size_t s32_stride;  // floats per point in the FP32 scratch
   size_t f_a, f_b, f_delta, f_scal, f_Yt, f_CN, f_CG;
+  // mixed form, prep -> yf_kernel: FP32 header, per-tile info, z rows,
+  // log2 D table, per-tile row block
+  size_t f_hdr, f_tinfo, f_q, f_dt32, f_rows;
+  int nzp;  // n_z rounded up to 4
 };
 
 struct PointDev {  // mirrors y3b_point

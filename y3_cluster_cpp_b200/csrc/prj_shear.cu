@@ -165,13 +165,7 @@ dsigma_single(const PrjTables& T, double R, double Rmis, double lnM)
   if (T.n_lx) {
     unit = exp(interp2d_clamp(T.lx, T.n_lx, T.lxm, T.n_lxm, T.ltab, log(x), log(xm)));
   } else {  // mean tangential shear on the circle x around the offset centre
-    unit = 0.0;
-    for (int t = 0; t < T.n_th; ++t) {
-      const double ct = cos(T.th[t]);
-      const double d2 = x * x + xm * xm - 2.0 * x * xm * ct, a = x - xm * ct;
-      unit += T.wth[t] * NfwUnit<double>::dsigma(sqrt(d2)) * (2.0 * a * a / d2 - 1.0);
-    }
-    unit /= kPiP;
+    unit = dsigma_single_partial(T.th, T.wth, T.n_th, x, xm, 0, 1) / kPiP;
   }
   return nfw_norm(lnM, kConc, kRhoCrit) * T.omega_m * unit;
 }

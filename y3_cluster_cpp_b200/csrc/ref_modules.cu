@@ -411,7 +411,10 @@ nfw_mis_kernel(int which, int n, const double* r, const double* rmis, const doub
   const int lane = threadIdx.x & 31;
   if (w >= n) return;
   const double rs = nfw_rs(lnM[w], conc, rho);
-  double v = mis_partial<double>(q, r[w] / rs, rmis[w] / rs, which == 0, lane);
+  double v = which == 2
+               ? dsigma_single_partial(q.th, q.wth, q.n_theta, r[w] / rs, rmis[w] / rs, lane, 32) /
+                   kPi
+               : mis_partial<double>(q, r[w] / rs, rmis[w] / rs, which == 0, lane);
   v = warp_sum(v);
   if (lane == 0) out[w] = nfw_norm(lnM[w], conc, rho) * v;
 }
@@ -859,7 +862,7 @@ y3b_nfw_mis(int which, int n, const double* r, const double* rmis, const double*
 {
   using namespace y3b;
   clear_error();
-  if (n < 0 || (n > 0 && (!r || !rmis || !lnM || !out)) || (which != 0 && which != 1) ||
+  if (n < 0 || (n > 0 && (!r || !rmis || !lnM || !out)) || which < 0 || which > 2 ||
       !(conc > 0.0) || !(rho > 0.0)) {
     set_error("y3b_nfw_mis: invalid arguments");
     return Y3B_ERR_INVALID;

@@ -250,11 +250,15 @@ def sigma_crit_inv(zl, zs, pz, delta_z, h0, dist_z, dist_da):
 
 
 def nfw_mis(which, r, rmis, lnM, conc, rho, n_theta=64, n_s=128, s_max=20.0):
-    """which='dsigma' (NFW_DSIGMA_MIS) or 'sigma' (NFW_SIGMA_MIS)."""
+    """which='dsigma' (NFW_DSIGMA_MIS, gamma kernel), 'sigma' (NFW_SIGMA_MIS)
+    or 'dsigma_single' (NFW_DSIGMA_MIS for the single offset rmis)."""
+    kinds = {"dsigma": 0, "sigma": 1, "dsigma_single": 2}
+    if which not in kinds:
+        raise ValueError(f"nfw_mis: which must be one of {sorted(kinds)}")
     r, rmis, lnM = np.broadcast_arrays(f64(r), f64(rmis), f64(lnM))
     r, rmis, lnM = f64(r), f64(rmis), f64(lnM)
     out = np.empty(r.shape)
-    check(lib().y3b_nfw_mis(0 if which == "dsigma" else 1, r.size, ptr(r), ptr(rmis), ptr(lnM),
+    check(lib().y3b_nfw_mis(kinds[which], r.size, ptr(r), ptr(rmis), ptr(lnM),
                             conc, rho, n_theta, n_s, s_max, ptr(out)))
     return out
 
