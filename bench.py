@@ -627,17 +627,27 @@ def run_ours(a):
     g = synthetic.grid(a.density)
     t0 = uniq[0].tables
     pz, pc = synthetic.plob_baseline()
+    # Two engines on the same points: `eng32` is the mixed form with the HMF
+    # grid in FP32 in its packed tables (the form's wire format: it rounds
+    # that grid to FP32 on the device anyway, so its counts equal those from
+    # FP64 tables); `eng` takes FP64 tables and gives the FP64 reference.
     eng = engine.Engine([g], len(t0["hmf_m_h"]), len(t0["hmf_z"]), len(t0["dist_z"]), (pz, pc),
                         max_points=B, n_sci=len(t0["sci_z"]))
+    eng32 = engine.Engine([g], len(t0["hmf_m_h"]), len(t0["hmf_z"]), len(t0["dist_z"]),
+                          (pz, pc), max_points=B, n_sci=len(t0["sci_z"]), hmf_fp32=True)
     n_bins = eng.n_bins
     tab_u = eng.pack(uniq)
     tables_h = torch.empty((B, eng.stride), dtype=torch.float64, pin_memory=True)
     tables_h.numpy()[:] = tab_u[np.arange(B) % len(uniq)]
+    tab32 = eng32.pack(uniq)
+    tables32_h = torch.empty((B, eng32.stride), dtype=torch.float64, pin_memory=True)
+    tables32_h.numpy()[:] = tab32[np.arange(B) % len(uniq)]
     parr = eng.points_array(pts, grid_of=lambda _: 0)
     pts_h = torch.empty(C.sizeof(parr), dtype=torch.uint8, pin_memory=True)
     C.memmove(pts_h.data_ptr(), C.addressof(parr), C.sizeof(parr))
     counts_h = torch.empty((B, n_bins), dtype=torch.float64, pin_memory=True)
     tables_d = tables_h.to(dev)
+    tables32_d = tables32_h.to(dev)
     pts_d = pts_h.to(dev)
     counts_d = torch.empty((B, n_bins), dtype=torch.float64, device=dev)
     # A dedicated (non-default) stream: the library launches on it and the
@@ -647,11 +657,16 @@ def run_ours(a):
     sp = stream.cuda_stream
 
     def step(prec, n=B):
-        eng.eval_device(prec, n, pts_d.data_ptr(), tables_d.data_ptr(), counts_d.data_ptr(),
-                        0, sp)
+        if prec == engine.FP64:
+            eng.eval_device(prec, n, pts_d.data_ptr(), tables_d.data_ptr(), counts_d.data_ptr(),
+                            0, sp)
+        else:
+            eng32.eval_device(prec, n, pts_d.data_ptr(), tables32_d.data_ptr(),
+                              counts_d.data_ptr(), 0, sp)
 
     # ---- autotuner: ring depth and bins per tile, on this batch (untimed) ----
-    tuning = eng.autotune(B, pts_d.data_ptr(), tables_d.data_ptr(), counts_d.data_ptr())
+    tuning = eng32.autotune(B, pts_d.data_ptr(), tables32_d.data_ptr(), counts_d.data_ptr())
+    eng.autotune(B, pts_d.data_ptr(), tables_d.data_ptr(), counts_d.data_ptr())
 
     # ---- accuracy of the mixed form vs FP64 on this batch (untimed) ----
     step(engine.FP64)
@@ -692,16 +707,16 @@ def run_ours(a):
     if world > 1:
         torch.distributed.barrier()
     launches = engine.launch_count() - launches0
-    eng.sync(sp)
+    eng32.sync(sp)
     clk = clocks.stop()
     # Stage times (CUDA events the library records around each stage on the
     # same stream; plain launches, as stage timing bypasses the graph).
-    eng.profile(True)
+    eng32.profile(True)
     for _ in range(max(3, a.steps // 2)):
         flush.zero_()
         step(engine.MIXED)
-    prof = eng.profile_read()
-    eng.profile(False)
+    prof = eng32.profile_read()
+    eng32.profile(False)
     step_ms = [st.elapsed_time(en) for st, en in zip(starts, ends)]
     total_ms = sharding.max_over_ranks(sum(step_ms), dev)
     value = world * B * a.steps / (total_ms / 1e3)
@@ -715,7 +730,7 @@ def run_ours(a):
     # (lnM, z) pair of a tile is below 4e-6 of its peak; the tensor pipe
     # issues this fraction of the dense stages.
     torch.cuda.synchronize(dev)
-    st_ex, st_dn = eng.stage_count()
+    st_ex, st_dn = eng32.stage_count()
     issued = st_ex / max(st_dn, 1)
     stage_share = {k: prof[k] / max(sum(prof[x] for x in ("prep", "contraction", "shear",
                                                              "final")), 1e-12)
@@ -758,21 +773,13 @@ def run_ours(a):
     e2e64_value = world * B * len(e2e_t) / e2e_total
     h2d64 = B * (C.sizeof(_capi.Point) + eng.stride * 8)
     d2h = B * n_bins * 8
-    # The same through an engine whose packed tables carry the HMF grid in
-    # FP32: the mixed form rounds that grid to FP32 on the device anyway, so
-    # its counts equal those above (up to the autotuner's choice of tile,
-    # which changes FP32 rounding only), for about half the bytes per point.
-    eng32 = engine.Engine([g], len(t0["hmf_m_h"]), len(t0["hmf_z"]), len(t0["dist_z"]),
-                          (pz, pc), max_points=B, n_sci=len(t0["sci_z"]), hmf_fp32=True)
-    tab32 = eng32.pack(uniq)
-    tables32_h = torch.empty((B, eng32.stride), dtype=torch.float64, pin_memory=True)
-    tables32_h.numpy()[:] = tab32[np.arange(B) % len(uniq)]
+    # The same through the engine whose packed tables carry the HMF grid in
+    # FP32 (the headline e2e): its counts equal those above up to the
+    # autotuner's choice of tile, which changes FP32 rounding only, for about
+    # half the bytes per point.
     counts32_h = torch.empty((B, n_bins), dtype=torch.float64, pin_memory=True)
     TPt32 = C.cast(C.c_void_p(tables32_h.data_ptr()), _capi.PD)
     CPt32 = C.cast(C.c_void_p(counts32_h.data_ptr()), _capi.PD)
-    tables32_d = tables32_h.to(dev)
-    eng32.autotune(B, pts_d.data_ptr(), tables32_d.data_ptr(), counts_d.data_ptr())
-    del tables32_d
     for _ in range(2):
         engine.check(lib.y3b_engine_eval(eng32.handle, engine.MIXED, B, PPt, TPt32, CPt32, None))
     diff32 = float(np.max(np.abs(counts32_h.numpy() / counts_h.numpy() - 1)))
@@ -821,6 +828,7 @@ def run_ours(a):
             "config": {"workload": WORKLOAD, "points_per_step_per_gpu": B,
                        "distinct_walker_tables": len(uniq), "density": a.density,
                        "l2": "flushed between timed steps (256 MB write)",
+                       "tables": "device-resident packed tables, HMF grid in FP32 (hmf_fp32)",
                        "tuning": tuning, "cuda_graph": True,
                        "parallelism": f"walker-sharded x{world}"},
             "max_rel_err_vs_fp64": max_rel,
