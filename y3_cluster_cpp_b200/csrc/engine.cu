@@ -435,8 +435,9 @@ prep_kernel(PrepArgs a)
   const float mu_sat_lo = (float)(ll_lo + 5.6 * sig - L0) + 1e-3f;
   const float mu_sat_hi = (float)(ll_hi - 5.6 * sig - L0) - 1e-3f;
   // log2 D(mu) and h dlog2D/dmu on kDTab equally spaced mu over the point's
-  // range of alpha_k + beta_q, evaluated in FP64 and stored in FP32 for
-  // yf_kernel's cubic Hermite.  ln D comes from ln_mor_norm (finite however
+  // range of alpha_k + beta_q, evaluated and stored in FP64 and, rounded, in
+  // FP32 for yf_kernel's cubic Hermite (FP32 where |log2 D| <= 16, FP64
+  // deeper in a tail).  ln D comes from ln_mor_norm (finite however
   // far mu lies outside the domain) and dlnD/dmu = (phi(a) - phi(b)) / (s D),
   // taken in logs.  Only nodes next to a mu that fails the FP32 saturation
   // test are read (the test's margin is 1e-3 plus FP32 rounding, and the
@@ -447,6 +448,7 @@ prep_kernel(PrepArgs a)
   const double inv_hmu = 1.0 / hmu;
   {
     float* dt32 = s32 + Gp->f_dt32;
+    double* dt64 = s64 + Gp->o_dt64;
     const int j_sat0 =
       (int)fmin(fmax(ceil((ll_lo + 5.6 * sig + 0.01 - mu0) * inv_hmu) + 2.0, 0.0), (double)kDTab);
     const int j_sat1 =
@@ -455,15 +457,21 @@ prep_kernel(PrepArgs a)
     for (int j = n_lo + tid; j < kDTab - n_hi; j += blockDim.x) {
       dt32[j] = 0.f;
       dt32[kDTab + j] = 0.f;
+      dt64[j] = 0.0;
+      dt64[kDTab + j] = 0.0;
     }
     for (int r = tid; r < n_lo + n_hi; r += blockDim.x) {
       const int j = r < n_lo ? r : kDTab - n_hi + (r - n_lo);
       const double mu = mu0 + j * hmu;
       const double aa = (ll_lo - mu) * inv_s, bb = (ll_hi - mu) * inv_s;
       const double lnD = ln_mor_norm(aa, bb);
-      dt32[j] = (float)(kLog2e * lnD);
-      dt32[kDTab + j] = (float)(hmu * inv_s * kLog2e *
-                                (exp(-0.5 * aa * aa - lnD) - exp(-0.5 * bb * bb - lnD)) / kSqrt2Pi);
+      const double l2 = kLog2e * lnD;
+      const double dl2 =
+        hmu * inv_s * kLog2e * (exp(-0.5 * aa * aa - lnD) - exp(-0.5 * bb * bb - lnD)) / kSqrt2Pi;
+      dt64[j] = l2;
+      dt64[kDTab + j] = dl2;
+      dt32[j] = (float)l2;
+      dt32[kDTab + j] = (float)dl2;
     }
   }
   if (tid == 0) {
@@ -787,7 +795,6 @@ yf_kernel(PrepArgs a)
   const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
   const float c2 = fh[0], mu_sat_lo = fh[1], mu_sat_hi = fh[2], sc1 = fh[3];
   const float mu0c = fh[4], inv_hmu_f = fh[5];
-  constexpr double kLog2e = 1.4426950408889634;
   // Y(k, q) = n(M_k, z_q) kf_k H(k, q) 2^-(v_k^2 c1) / (sqrt(2 pi) s D_kq).
   // Warp w takes a contiguous run of z rows and lane the tile rows
   // lane + 32 j (j < 4).  Each lane keeps, in registers, the two HMF z rows
@@ -795,10 +802,11 @@ yf_kernel(PrepArgs a)
   // kf_k / (sqrt(2 pi) s), and advances them with q (the z nodes ascend).  A
   // z row whose tile cells all have mu more than 5.6 sigma inside the domain
   // (D = 1 in FP32) is FP32 only.  Otherwise an unsaturated cell takes
-  // log2 D from the table by a cubic Hermite in FP32 where D >= 2^-8 (its
+  // log2 D from the table by a cubic Hermite in FP32 where D >= 2^-16 (its
   // relative error there ~1e-6); deeper in a tail, and in rows that carry a
-  // scale, it forms 2^(log2 H - v^2 c1 - log2 D) in FP64 from ln D itself,
-  // applied as an exact power of two times 2^(fraction) in FP32.
+  // scale, by the Hermite of the FP64 table (read through L1), and forms
+  // 2^(log2 H - v^2 c1 - log2 D) in FP64, applied as an exact power of two
+  // times 2^(fraction) in FP32.
   {
     const float* rt_s = rows;
     const int* rx_s = reinterpret_cast<const int*>(rows + kGemmRows);
@@ -862,16 +870,23 @@ yf_kernel(PrepArgs a)
           const float l2d = (2.f * t3 - 3.f * t2 + 1.f) * dt32[jj] +
                             (t3 - 2.f * t2 + t) * dt32[kDTab + jj] +
                             (3.f * t2 - 2.f * t3) * dt32[jj + 1] + (t3 - t2) * dt32[kDTab + jj + 1];
-          if (l2d >= -8.f && row_vv[r] == 0.0) {
+          if (l2d >= -16.f && rvf_s[r] == 0.f) {
             y[j] = nv[j] * fast_exp2(e[j] - l2d);
             continue;
           }
           const int k = mt0 * kGemmRows + r;
-          const double alpha = s64[Gp->o_alpha + k], beta = s64[Gp->o_beta + q];
+          const double alpha = __ldg(s64 + Gp->o_alpha + k), beta = __ldg(s64 + Gp->o_beta + q);
           const double mu = alpha + beta;
-          const double lnD = ln_mor_norm((th[5] - mu) * th[7], (th[6] - mu) * th[7]);
+          const double ud = (mu - th[2]) * th[3];
+          const int jd = min(max((int)floor(ud), 0), kDTab - 2);
+          const double td = ud - jd, td2 = td * td, td3 = td2 * td;
+          const double* d64 = s64 + Gp->o_dt64;
+          const double l2 = (2.0 * td3 - 3.0 * td2 + 1.0) * __ldg(d64 + jd) +
+                            (td3 - 2.0 * td2 + td) * __ldg(d64 + kDTab + jd) +
+                            (3.0 * td2 - 2.0 * td3) * __ldg(d64 + jd + 1) +
+                            (td3 - td2) * __ldg(d64 + kDTab + jd + 1);
           const double ad = alpha - th[0], bd = beta - th[1];
-          const double ex = -(ad * bd + 0.5 * bd * bd) * th[4] - row_vv[r] - kLog2e * lnD;
+          const double ex = -(ad * bd + 0.5 * bd * bd) * th[4] - row_vv[r] - l2;
           const double ei = rint(ex);
           const float yf = mul_pow2(nv[j] * fast_exp2((float)(ex - ei)), ei);
           if (!(fabsf(yf) <= 3.402823466e38f)) {  // not representable: report, never a NaN
@@ -1419,6 +1434,8 @@ build_grid(y3b_engine* e, int gi)
   o += 8;
   g.o_vv = o;
   o += pad2(g.n_m_pad);
+  g.o_dt64 = o;
+  o += 2 * (size_t)kDTab;
   g.s64_stride = o;
   // FP32 scratch: every section a multiple of 4 floats (16 bytes), so that
   // the bulk copies of yf_kernel and the contraction start aligned.

@@ -54,6 +54,7 @@ struct GridDev {
   size_t o_scal, o_kx, o_kt, o_kf, o_qy, o_qu;  // A0/B0, HMF cells and weights
   size_t o_cz, o_czs, o_alpha, o_beta, o_P0, o_V;
   size_t o_thdr, o_vv;  // mixed form: FP64 header and row scale v_k^2 c1 of yf_kernel
+  size_t o_dt64;        // mixed form: FP64 log2 D table (deep tails)
   size_t s32_stride;  // floats per point in the FP32 scratch
   size_t f_a, f_b, f_delta, f_scal, f_Yt, f_CN, f_CG;
   // mixed form, prep -> yf_kernel: FP32 header, per-tile info, z rows,
