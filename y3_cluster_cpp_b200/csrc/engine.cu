@@ -623,30 +623,54 @@ prep_kernel(PrepArgs a)
     if (vv != 0.0) tile_sc[mt] = 1;
   }
   __syncthreads();
-  // Per tile: yf_kernel's info, the exponent-range guard and the windows of
-  // the contraction tiles (lnM tile, richness-bin group).  G = 2^(delta b c2)
-  // over the issued stages and H = 2^(-(a b + b^2/2) c2) must stay well
-  // inside FP32 / BF16 (2^-126 .. 2^127).  |a| <= (max alpha - min alpha) / 2
-  // and |b| <= (max beta - min beta) / 2 after centring, so the bound below
-  // holds for every factor; a point beyond it reports kDevRange (its FP64
-  // form is unaffected).
+  // Per tile: the stages each contraction tile (lnM tile, richness-bin group)
+  // issues, yf_kernel's info and the exponent-range guard.  A contraction
+  // tile issues the MOR window intersected with the stages where its bins'
+  // kernels K_i(t, q) reach 1e-12 of their maximum (outside, every term is
+  // below that fraction of the bin's kernel): the count rounded up to pairs
+  // inside [0, nk); where the two do not meet (the tile's MOR density lies
+  // where none of its bins' kernels does, so its terms are negligible) one
+  // pair at the window's start, which keeps its accumulator defined.
+  // yf_kernel writes F over the hull of the lnM tile's issued ranges.
+  // G = 2^(delta b c2) over the issued stages and H = 2^(-(a b + b^2/2) c2)
+  // must stay well inside FP32 / BF16 (2^-126 .. 2^127).  |a| <=
+  // (max alpha - min alpha) / 2 and |b| <= (max beta - min beta) / 2 after
+  // centring, so the bound below holds for every factor; a point beyond it
+  // reports kDevRange (its FP64 form is unaffected).
   for (int mt = tid; mt < n_mt; mt += blockDim.x) {
+    const int nk = n_t_pad / 16, lo = swin[2 * mt], hi = swin[2 * mt + 1];
+    int h_lo = nk, h_hi = 0;
+    for (int bg = 0; bg < Gp->n_bg; ++bg) {
+      const int i0 = bg * Gp->nIc, i1 = min(Gp->nI, i0 + Gp->nIc);
+      int klo = n_t, khi = -1;
+      for (int i = i0; i < i1; ++i) {
+        klo = min(klo, Gp->kt_lo[i]);
+        khi = max(khi, Gp->kt_hi[i]);
+      }
+      int s0 = max(lo, klo / 16), s1 = min(hi, khi / 16 + 1);
+      if (s1 <= s0) {
+        s0 = lo;
+        s1 = lo + 2;
+      }
+      if ((s1 - s0) & 1) {
+        if (s1 < nk) ++s1; else --s0;
+      }
+      h_lo = min(h_lo, s0);
+      h_hi = max(h_hi, s1);
+      a.win_tile[(size_t)p * a.win_stride + mt * Gp->n_bg + bg] = s0 | (s1 << 16);
+    }
     float* ti = s32 + Gp->f_tinfo + 4 * mt;
     ti[0] = tile_af[2 * mt];
     ti[1] = tile_af[2 * mt + 1];
     ti[2] = __int_as_float(tile_sc[mt]);
-    ti[3] = __int_as_float(swin[2 * mt] | (swin[2 * mt + 1] << 16));
+    ti[3] = __int_as_float(h_lo | (h_hi << 16));
     double dmax = 0.0;
-    const int t0 = swin[2 * mt] * 16, t1 = min(swin[2 * mt + 1] * 16, n_t) - 1;
+    const int t0 = h_lo * 16, t1 = min(h_hi * 16, n_t) - 1;
     if (t1 >= t0) dmax = fmax(fabs((double)dt_f[t0]), fabs((double)dt_f[t1]));
     const double bmax = 0.5 * (red[5] - red[4]);
     const double amax = 0.5 * ((red[3] - red[2]) - (red[5] - red[4]));
     const double e = c2d * bmax * fmax(dmax, amax + 0.5 * bmax);
     if (!(e <= kMaxExp2)) set_err(a.status, kDevRange);
-  }
-  for (int l = tid; l < Gp->tiles_pp; l += blockDim.x) {
-    const int mt = l / Gp->n_bg;
-    a.win_tile[(size_t)p * a.win_stride + l] = swin[2 * mt] | (swin[2 * mt + 1] << 16);
   }
 }
 
@@ -1384,6 +1408,36 @@ build_grid(y3b_engine* e, int gi)
   count_launch();
   Y3B_CUDA(cudaGetLastError());
   Y3B_CUDA(cudaStreamSynchronize(s));  // pz/pc are freed on return
+  {
+    // Support of each bin's kernel in lam_t: outside it K_i(t, q) is below
+    // 1e-12 of its maximum over t (for every q), so the contraction skips
+    // those stages for the bin's tiles.
+    std::vector<double> hk((size_t)nki);
+    Y3B_CUDA(cudaMemcpy(hk.data(), b->Ki.get(), hk.size() * sizeof(double),
+                        cudaMemcpyDeviceToHost));
+    for (int i = 0; i < kMaxLamBins; ++i) {
+      g.kt_lo[i] = 0;
+      g.kt_hi[i] = g.n_t - 1;
+    }
+    for (int i = 0; i < g.nI; ++i) {
+      int lo = g.n_t, hi = -1;
+      for (int q = 0; q < g.n_z; ++q) {
+        const double* k = hk.data() + ((size_t)i * g.n_z + q) * g.n_t;
+        double mx = 0.0;
+        for (int t = 0; t < g.n_t; ++t) mx = std::max(mx, k[t]);
+        if (!(mx > 0.0)) continue;
+        for (int t = 0; t < g.n_t; ++t)
+          if (k[t] > 1e-12 * mx) {
+            lo = std::min(lo, t);
+            hi = std::max(hi, t);
+          }
+      }
+      if (hi >= lo) {
+        g.kt_lo[i] = lo;
+        g.kt_hi[i] = hi;
+      }
+    }
+  }
   g.uk_zindep = 1;
   {
     const int np = (int)e->plob_z.size();

@@ -37,6 +37,9 @@ struct GridDev {
   int ncp_c;       // TMEM columns per CTA: nIc * n_z padded to 16
   int tiles_pp;    // contraction tiles per point: (n_m_pad / kGemmRows) * n_bg
   int cost_rank;   // 0 = the grid with the most expensive tiles (scheduled first)
+  // lam_t nodes where richness bin i's kernel K_i(t, q) exceeds 1e-12 of its
+  // maximum over t, for some z_t node q: [kt_lo[i], kt_hi[i]]
+  int kt_lo[kMaxLamBins], kt_hi[kMaxLamBins];
   double lnm_lo, lnm_hi, zt_lo, zt_hi, ll_lo, ll_hi, sz0;
   double sz_bin[8];   // sigma_z(z, j) = sz0 (1 + z) + sz_bin[j]
   const double* xm;   // [n_m]  lnM nodes
