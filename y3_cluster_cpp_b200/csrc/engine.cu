@@ -838,7 +838,9 @@ yf_kernel(PrepArgs a)
     const float* ra_s = rows + 3 * kGemmRows;
     const float* rvf_s = rows + 6 * kGemmRows;
     const int* rok_s = reinterpret_cast<const int*>(rows + 7 * kGemmRows);
-    const int qs = (n_z + nw - 1) / nw, qa = warp * qs, qb_end = min(n_z, qa + qs);
+    // Runs of whole pairs of z rows (n_z is a multiple of 16): Y is stored
+    // [lnM tile][z / 2][128 rows][2], one float2 per lane and row.
+    const int qs = ((n_z / 2 + nw - 1) / nw) * 2, qa = warp * qs, qb_end = min(n_z, qa + qs);
     float rn[4], rk[4], R0[4], R1[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -850,7 +852,11 @@ yf_kernel(PrepArgs a)
     const bool scaled = tinfo[2] != 0;
     float* __restrict__ yblk = s32 + Gp->f_Yt + (size_t)mt0 * n_z * kGemmRows;
     int ycur = -2;
-    for (int q = qa; q < qb_end; ++q) {
+    for (int q0 = qa; q0 < qb_end; q0 += 2) {
+    float yv[4][2];
+#pragma unroll
+    for (int dq = 0; dq < 2; ++dq) {
+      const int q = q0 + dq;
       const int yq = qy[q];
       if (yq != ycur) {  // warp-uniform
         const float* h1 = h32 + (size_t)(yq + 1) * n_hm;
@@ -922,7 +928,12 @@ yf_kernel(PrepArgs a)
         }
       }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) yblk[(size_t)q * kGemmRows + lane + 32 * j] = y[j];
+      for (int j = 0; j < 4; ++j) yv[j][dq] = y[j];
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      *reinterpret_cast<float2*>(yblk + ((size_t)(q0 >> 1) * kGemmRows + lane + 32 * j) * 2) =
+        make_float2(yv[j][0], yv[j][1]);
     }
   }
   // F'(t, k) for the contraction (the row scale above), split into bf16

@@ -761,6 +761,7 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
       y_pending = 0;
       tc_fence_after();
       const int rl = lq * 32 + lane;  // row inside the tile
+      const float2* Ys2 = reinterpret_cast<const float2*>(Ys);
       const int row = T.mtile * kGemmRows + rl;
       const bool valid = row < n_m;
       const uint32_t tbase = tmem + lane_base + (uint32_t)(buf * kAccCols);
@@ -777,19 +778,25 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
           float2 pN[NJ], pG[NJ];
 #pragma unroll
           for (int jj = 0; jj < NJ; ++jj) pN[jj] = pG[jj] = make_float2(0.f, 0.f);
+          // Y is [z / 2][row][2]: one 8-byte load per lane gives the row's
+          // pair of z nodes; the weights come four z nodes per load.
 #pragma unroll
-          for (int u = 0; u < 16; u += 2) {
+          for (int u = 0; u < 16; u += 4) {
             const int q = qc + u;
-            const float2 e = __fmul2_rn(make_float2(v[u], v[u + 1]),
-                                        make_float2(Ys[q * kGemmRows + rl],
-                                                    Ys[(q + 1) * kGemmRows + rl]));
+            const float2 y01 = Ys2[(q >> 1) * kGemmRows + rl];
+            const float2 y23 = Ys2[((q >> 1) + 1) * kGemmRows + rl];
+            const float2 e0 = __fmul2_rn(make_float2(v[u], v[u + 1]), y01);
+            const float2 e1 = __fmul2_rn(make_float2(v[u + 2], v[u + 3]), y23);
 #pragma unroll
             for (int jj = 0; jj < NJ; ++jj) {
-              pN[jj] = __ffma2_rn(*reinterpret_cast<const float2*>(CN_s + jj * n_z + q), e,
-                                  pN[jj]);
-              if (SHEAR)
-                pG[jj] = __ffma2_rn(*reinterpret_cast<const float2*>(CG_s + jj * n_z + q), e,
-                                    pG[jj]);
+              const float4 c = *reinterpret_cast<const float4*>(CN_s + jj * n_z + q);
+              pN[jj] = __ffma2_rn(make_float2(c.x, c.y), e0, pN[jj]);
+              pN[jj] = __ffma2_rn(make_float2(c.z, c.w), e1, pN[jj]);
+              if (SHEAR) {
+                const float4 g = *reinterpret_cast<const float4*>(CG_s + jj * n_z + q);
+                pG[jj] = __ffma2_rn(make_float2(g.x, g.y), e0, pG[jj]);
+                pG[jj] = __ffma2_rn(make_float2(g.z, g.w), e1, pG[jj]);
+              }
             }
           }
 #pragma unroll
