@@ -141,21 +141,27 @@ mbar_try_wait(uint32_t addr, uint32_t parity)
   return ok != 0;
 }
 
-// 32 lanes x 16 columns of FP32 from TMEM.
+// 32 lanes x 8 columns of FP32 from TMEM, issued without waiting: the
+// registers are valid only after tmem_ld_wait on the same array.
 __device__ __forceinline__ void
-tmem_ld16(uint32_t taddr, float* v)
+tmem_ld8_issue(uint32_t taddr, uint32_t* r)
 {
-  uint32_t r[16];
-  asm volatile(
-    "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-    "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-      "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-      "=r"(r[14]), "=r"(r[15])
-    : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                 "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+}
+
+// Waits for the thread's outstanding TMEM loads; the array's registers are
+// operands, so no use of them moves above the wait.
+__device__ __forceinline__ void
+tmem_ld_wait(uint32_t* r)
+{
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                 "+r"(r[6]), "+r"(r[7])
+               :
+               : "memory");
 }
 
 constexpr long long kWaitBudget = 2000000000LL;  // SM cycles (~1 s)
@@ -281,6 +287,38 @@ __host__ __device__ inline int
 vec_slot_floats(int nz_max, int ntp_max, int uk_max)
 {
   return 4 + kGemmRows + nz_max + ntp_max + uk_max;
+}
+
+// Eight columns of a row's accumulator: times Y(k, q) (Y stored
+// [z / 2][row][2], one 8-byte load per z pair), contracted with the z-bin
+// weights four z nodes per load into packed FP32x2 partial sums (even and
+// odd z nodes side by side).
+template <int NJ, bool SHEAR>
+__device__ __forceinline__ void
+epi_chunk8(const uint32_t* r, int qc, const float2* __restrict__ Ys2, int rl,
+           const float* __restrict__ CN_s, const float* __restrict__ CG_s, int n_z, float2* pN,
+           float2* pG)
+{
+#pragma unroll
+  for (int u = 0; u < 8; u += 4) {
+    const int q = qc + u;
+    const float2 y01 = Ys2[(q >> 1) * kGemmRows + rl];
+    const float2 y23 = Ys2[((q >> 1) + 1) * kGemmRows + rl];
+    const float2 e0 = __fmul2_rn(make_float2(__uint_as_float(r[u]), __uint_as_float(r[u + 1])), y01);
+    const float2 e1 =
+      __fmul2_rn(make_float2(__uint_as_float(r[u + 2]), __uint_as_float(r[u + 3])), y23);
+#pragma unroll
+    for (int jj = 0; jj < NJ; ++jj) {
+      const float4 c = *reinterpret_cast<const float4*>(CN_s + jj * n_z + q);
+      pN[jj] = __ffma2_rn(make_float2(c.x, c.y), e0, pN[jj]);
+      pN[jj] = __ffma2_rn(make_float2(c.z, c.w), e1, pN[jj]);
+      if (SHEAR) {
+        const float4 g = *reinterpret_cast<const float4*>(CG_s + jj * n_z + q);
+        pG[jj] = __ffma2_rn(make_float2(g.x, g.y), e0, pG[jj]);
+        pG[jj] = __ffma2_rn(make_float2(g.z, g.w), e1, pG[jj]);
+      }
+    }
+  }
 }
 
 struct Tile {
@@ -770,40 +808,29 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
         double accN[NJ], accG[NJ];
 #pragma unroll
         for (int jj = 0; jj < NJ; ++jj) accN[jj] = accG[jj] = 0.0;
+        // Two register sets: the TMEM load of the next 8 columns is in
+        // flight while the current ones are contracted.  Every 16 columns
+        // the FP32 partial sums are added in FP64 (n_z is a multiple of 16).
+        const uint32_t tb = tbase + (uint32_t)(il * n_z);
+        uint32_t ra[8], rb[8];
+        tmem_ld8_issue(tb, ra);
+        tmem_ld_wait(ra);
         for (int qc = 0; qc < n_z; qc += 16) {
-          float v[16];
-          tmem_ld16(tbase + (uint32_t)(il * n_z + qc), v);
-          // Even and odd z nodes summed side by side (packed FP32x2), then
-          // added in FP64.
           float2 pN[NJ], pG[NJ];
 #pragma unroll
           for (int jj = 0; jj < NJ; ++jj) pN[jj] = pG[jj] = make_float2(0.f, 0.f);
-          // Y is [z / 2][row][2]: one 8-byte load per lane gives the row's
-          // pair of z nodes; the weights come four z nodes per load.
-#pragma unroll
-          for (int u = 0; u < 16; u += 4) {
-            const int q = qc + u;
-            const float2 y01 = Ys2[(q >> 1) * kGemmRows + rl];
-            const float2 y23 = Ys2[((q >> 1) + 1) * kGemmRows + rl];
-            const float2 e0 = __fmul2_rn(make_float2(v[u], v[u + 1]), y01);
-            const float2 e1 = __fmul2_rn(make_float2(v[u + 2], v[u + 3]), y23);
-#pragma unroll
-            for (int jj = 0; jj < NJ; ++jj) {
-              const float4 c = *reinterpret_cast<const float4*>(CN_s + jj * n_z + q);
-              pN[jj] = __ffma2_rn(make_float2(c.x, c.y), e0, pN[jj]);
-              pN[jj] = __ffma2_rn(make_float2(c.z, c.w), e1, pN[jj]);
-              if (SHEAR) {
-                const float4 g = *reinterpret_cast<const float4*>(CG_s + jj * n_z + q);
-                pG[jj] = __ffma2_rn(make_float2(g.x, g.y), e0, pG[jj]);
-                pG[jj] = __ffma2_rn(make_float2(g.z, g.w), e1, pG[jj]);
-              }
-            }
-          }
+          tmem_ld8_issue(tb + (uint32_t)(qc + 8), rb);
+          epi_chunk8<NJ, SHEAR>(ra, qc, Ys2, rl, CN_s, CG_s, n_z, pN, pG);
+          tmem_ld_wait(rb);
+          const bool more = qc + 16 < n_z;  // warp-uniform
+          if (more) tmem_ld8_issue(tb + (uint32_t)(qc + 16), ra);
+          epi_chunk8<NJ, SHEAR>(rb, qc + 8, Ys2, rl, CN_s, CG_s, n_z, pN, pG);
 #pragma unroll
           for (int jj = 0; jj < NJ; ++jj) {
             accN[jj] += (double)pN[jj].x + (double)pN[jj].y;
             if (SHEAR) accG[jj] += (double)pG[jj].x + (double)pG[jj].y;
           }
+          if (more) tmem_ld_wait(ra);
         }
         if (valid) {
 #pragma unroll
