@@ -108,22 +108,21 @@ fast_exp2(float x)
 }
 
 // Split 8 FP32 values (4 pairs) into bf16 hi + bf16 lo and store one 16-byte
-// core-matrix row of each.  hi rounds to nearest (ties away) on the bit
-// pattern, lo = v - hi is exact in FP32 and keeps its top 16 bits, so
-// |v - hi - lo| <= 2^-16 |v|; the products hi*hi + hi*lo + lo*hi then carry a
-// relative error of a few 2^-17.  Integer and packed-FP32 instructions only:
-// the conversion unit stays free for the exponentials.
+// core-matrix row of each.  hi rounds to nearest (cvt.rn.bf16x2.f32, one
+// instruction per pair); lo = v - hi is exact in FP32 and keeps its top 16
+// bits, so |v - hi - lo| <= 2^-16 |v|; the products hi*hi + hi*lo + lo*hi
+// then carry a relative error of a few 2^-17.
 __device__ __forceinline__ void
 store_split8(uint8_t* hi, uint8_t* lo, const float2* v)
 {
   uint32_t h[4], l[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    const uint32_t hx = (__float_as_uint(v[k].x) + 0x8000u) & 0xFFFF0000u;
-    const uint32_t hy = (__float_as_uint(v[k].y) + 0x8000u) & 0xFFFF0000u;
-    const float2 r =
-      __ffma2_rn(make_float2(__uint_as_float(hx), __uint_as_float(hy)), make_float2(-1.f, -1.f), v[k]);
-    h[k] = __byte_perm(hx, hy, 0x7632);
+    uint32_t hh;  // .y in the upper half, .x in the lower (memory order x, y)
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(hh) : "f"(v[k].y), "f"(v[k].x));
+    const float2 hf = make_float2(__uint_as_float(hh << 16), __uint_as_float(hh & 0xFFFF0000u));
+    const float2 r = __ffma2_rn(hf, make_float2(-1.f, -1.f), v[k]);
+    h[k] = hh;
     l[k] = __byte_perm(__float_as_uint(r.x), __float_as_uint(r.y), 0x7632);
   }
   *reinterpret_cast<uint4*>(hi) = make_uint4(h[0], h[1], h[2], h[3]);
