@@ -356,7 +356,7 @@ def test_engine_autotune_keeps_results_within_tolerance(gpu):
     eng.close()
 
 
-@pytest.mark.parametrize("n", [1100, 2100])  # four and eight chunks
+@pytest.mark.parametrize("n", [1100, 2100])  # four and seven chunks (FP64 tables)
 def test_engine_chunked_host_eval_matches_one_launch(gpu, n):
     """A large host-buffer evaluation is split into chunks whose copies
     overlap the previous chunk's kernels; counts and the mass weights equal

@@ -2191,9 +2191,17 @@ y3b_engine_eval(y3b_engine* e, int precision, int n, const y3b_point* pts,
   cudaStream_t s = e->stream, xs = e->xstream;
   // About 256 points a chunk: the copies are the long pole, and only the
   // last chunk's kernels run after them.
-  const int chunks = n >= 2048 ? y3b::kEvalChunks : (n >= 1024 ? 4 : (n >= 256 ? 2 : 1));
-  const int csz = (n + chunks - 1) / chunks;
+  // Chunks of about 12.5 MB of host tables (at least 256 points, at most
+  // eight): the copy of the next chunk then outlasts the evaluation of the
+  // current one, whose fixed cost grows relative to its work as chunks
+  // shrink.  On one B200 over PCIe, 2048 points with FP32-HMF tables
+  // (25.5 KB per point) ran at 1.28 / 1.49 / 1.58 / 1.66 M points/s in
+  // 8 / 2 / 3 / 4 chunks, with FP64 tables (45.5 KB) best in eight.
   const size_t st = e->lay.stride;
+  const double host_bytes = (double)n * (double)(st * sizeof(double) + sizeof(y3b_point));
+  int chunks = (int)std::min<double>(y3b::kEvalChunks, std::max(1.0, std::floor(host_bytes / 12.5e6)));
+  chunks = std::max(1, std::min(chunks, n / 256));
+  const int csz = (n + chunks - 1) / chunks;
   const int nB = e->nB_max, nR = e->shear.n_R;
   const bool want_shear = e->cfg.with_shear && shear;
   int used = 0;
