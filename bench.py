@@ -873,13 +873,13 @@ def run_ours(a):
 
 # DRAM bytes (read + write) per point of one contraction launch at 4x nodes,
 # from one ncu capture of the small case:
-#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none \
-#       -k regex:contract_kernel -s 2 -c 1 python bench.py --steps 3 --warmup 1 \
-#       --batch 256 --no-cpu-baseline --serve-requests 0 --no-extra-workloads
-# (76.06 MB read + 2.70 MB written over 256 points).  Traffic grows with the
+#   ncu --set full --clock-control none -k regex:contract_kernel -s 2 -c 1 \
+#       python bench.py --steps 3 --warmup 3 --batch 256 --no-cpu-baseline \
+#       --serve-requests 0 --no-extra-workloads
+# (73.32 MB read + 2.90 MB written over 256 points).  Traffic grows with the
 # points (each reads its own operand blocks), so a launch of B points moves
 # B times this.
-CONTRACT_TRAFFIC_BYTES_PER_POINT_4X = 307652.0
+CONTRACT_TRAFFIC_BYTES_PER_POINT_4X = 297720.0
 
 
 def ncu_traffic(density, points):
