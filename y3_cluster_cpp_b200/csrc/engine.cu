@@ -88,6 +88,18 @@ smem_addr(const void* p)
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
+// Bulk async copy global -> shared completing on mbarrier `bar` (16-byte
+// aligned addresses, a size that is a multiple of 16).
+__device__ __forceinline__ void
+bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+  asm volatile(
+    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+      smem_addr(dst)),
+    "l"(src), "r"(bytes), "r"(smem_addr(bar))
+    : "memory");
+}
+
 struct PrepArgs {
   const GridDev* grids;
   const PointDev* pts;
@@ -159,6 +171,24 @@ ln_mor_norm(double a, double b)
   return log(mor_norm(a, b));
 }
 
+// ln D in FP32, the same cases as ln_mor_norm; with both tails open (mu
+// inside the domain) D = 1 - Q(-a) - Q(b) and ln D = log1p(-Q(-a) - Q(b)),
+// accurate to FP32 rounding near saturation.
+__device__ __forceinline__ float
+ln_mor_norm_f(float a, float b)
+{
+  constexpr float kInvSqrt2f = 0.70710678f;
+  if (a > 0.f) {
+    const float ra = erfcxf(a * kInvSqrt2f), rb = erfcxf(b * kInvSqrt2f);
+    return logf(0.5f * ra) - 0.5f * a * a + log1pf(-(rb / ra) * expf(-0.5f * (b - a) * (b + a)));
+  }
+  if (b < 0.f) {
+    const float ra = erfcxf(-a * kInvSqrt2f), rb = erfcxf(-b * kInvSqrt2f);
+    return logf(0.5f * rb) - 0.5f * b * b + log1pf(-(ra / rb) * expf(-0.5f * (a - b) * (a + b)));
+  }
+  return log1pf(-0.5f * erfcf(-a * kInvSqrt2f) - 0.5f * erfcf(b * kInvSqrt2f));
+}
+
 // The mixed form reads log2 D(mu) from a per-point FP64 table: log2 D and
 // its derivative at kDTab equally spaced mu over the point's range of
 // alpha_k + beta_q, cubic Hermite interpolation (log D is smooth, so the
@@ -178,11 +208,14 @@ constexpr int kEvalChunks = 8;  // chunks of a large host-buffer evaluation
 //   mixed form: a_k, b_q, delta_t, c1, c2, C_j(q), C^g_j(q) for the
 //         contraction, the lam_t windows, and yf_kernel's inputs (row
 //         blocks, z rows, the log2 D table).
-// Shared memory: table block | per-k and per-q vectors | FP32 delta_t.
+// Shared memory: table block | the grid's lnM and z_t nodes, z_t weights,
+// Omega(z_t) and K_j(z_t) (staged with it) | per-k and per-q vectors |
+// FP32 delta_t.
 __host__ __device__ inline size_t
-prep_smem_bytes(const TableLayout& L, int n_m, int n_z, int n_t_pad)
+prep_smem_bytes(const TableLayout& L, int n_m, int n_z, int n_t_pad, int nJ)
 {
   size_t b = (L.off[2] + L.stride - L.off[3]) * 8;         // table block without dn/dlnM
+  b += ((size_t)((n_m + 1) & ~1) + (size_t)(3 + nJ) * n_z) * 8;  // grid nodes, weights, K_j
   b += (size_t)n_m * (8 + 8 + 8 + 4);                      // alpha, t, kf, xi
   b += (size_t)n_z * (8 + 8 + 4);                          // beta, u, yi
   b += 16 + (size_t)n_t_pad * 4;                           // FP32 delta_t (mixed form)
@@ -212,7 +245,13 @@ prep_kernel(PrepArgs a)
   // reads it there, yf_kernel stages the mixed form's FP32 copy).
   const size_t head = L.off[2], tail = L.stride - L.off[3];
   double* tab = psh;                                                  // [head + tail]
-  double* k_alpha = tab + head + tail;
+  const int nJ = Gp->nJ, n_m2 = (n_m + 1) & ~1;
+  double* g_xm = tab + head + tail;  // [n_m2]  the grid's arrays, staged with the tables
+  double* g_xz = g_xm + n_m2;        // [n_z]
+  double* g_wz = g_xz + n_z;         // [n_z]
+  double* g_omz = g_wz + n_z;        // [n_z]
+  double* g_Kj = g_omz + n_z;        // [nJ n_z]
+  double* k_alpha = g_Kj + (size_t)nJ * n_z;
   double* k_t = k_alpha + n_m;
   double* k_f = k_t + n_m;
   double* q_beta = k_f + n_m;
@@ -226,7 +265,8 @@ prep_kernel(PrepArgs a)
   __shared__ int swin[16];  // lam_t stage window per lnM tile (n_m <= 1024)
 
   const double* src = a.tables + (size_t)(a.slot ? a.slot[p] : p) * L.stride;
-  const uint32_t bytes = (uint32_t)((head + tail) * sizeof(double));
+  const uint32_t bytes =
+    (uint32_t)((head + tail + n_m2 + (size_t)(3 + nJ) * n_z) * sizeof(double));
   if (tid == 0) {
     timed_out = 0;
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar)) : "memory");
@@ -248,6 +288,11 @@ prep_kernel(PrepArgs a)
         "[%3];" ::"r"(smem_addr(tab + head)),
         "l"(src + L.off[3]), "r"((uint32_t)(tail * sizeof(double))), "r"(smem_addr(&bar))
         : "memory");
+    bulk_copy_g2s(g_xm, Gp->xm, (uint32_t)(n_m2 * 8), &bar);
+    bulk_copy_g2s(g_xz, Gp->xz, (uint32_t)(n_z * 8), &bar);
+    bulk_copy_g2s(g_wz, Gp->wz, (uint32_t)(n_z * 8), &bar);
+    bulk_copy_g2s(g_omz, Gp->omz, (uint32_t)(n_z * 8), &bar);
+    bulk_copy_g2s(g_Kj, Gp->Kj, (uint32_t)((size_t)nJ * n_z * 8), &bar);
   }
   {
     long long t0 = clock64();
@@ -301,8 +346,8 @@ prep_kernel(PrepArgs a)
   double* s64 = a.s64 + (size_t)p * Gp->s64_stride;
   float* s32 = a.s32 + (size_t)p * Gp->s32_stride;
   const double lnMpiv = log(pt.Mpiv);
-  const double* xm = Gp->xm;
-  const double* xz = Gp->xz;
+  const double* xm = g_xm;
+  const double* xz = g_xz;
   for (int k = tid; k < n_m; k += blockDim.x) {
     const double x = xm[k];
     const double alpha = pt.B * (x - lnMpiv);
@@ -315,8 +360,7 @@ prep_kernel(PrepArgs a)
     k_f[k] = pt.hmf_s * (x * kLog10e - kHmfPivot) + pt.hmf_q;
   }
   const size_t o_cz = Gp->o_cz, o_czs = Gp->o_czs, o_beta = Gp->o_beta;
-  const double* Kj = Gp->Kj;
-  const int nJ = Gp->nJ;
+  const double* Kj = g_Kj;
   for (int q = tid; q < n_z; q += blockDim.x) {
     const double z = xz[q];
     const double beta = pt.A + pt.C * log1p(z);
@@ -331,7 +375,7 @@ prep_kernel(PrepArgs a)
       set_err(a.status, kDevDomain);
       dv = 0.0;
     }
-    const double cz = Gp->wz[q] * dv * Gp->omz[q];
+    const double cz = g_wz[q] * dv * g_omz[q];
     const double czs = cz * (L.n_sci > 1 ? interp1d_clamp(sz, sv, L.n_sci, z) : 1.0);
     s64[o_cz + q] = cz;
     s64[o_czs + q] = czs;
@@ -460,14 +504,28 @@ prep_kernel(PrepArgs a)
       dt64[j] = 0.0;
       dt64[kDTab + j] = 0.0;
     }
+    // Nodes evaluated in FP32 (transcendentals an order of magnitude faster
+    // than FP64 here); where log2 D < -12 (the FP32 value's absolute error
+    // would pass 1e-6) the node is evaluated again in FP64 for both tables.
+    // The FP64 table is read only by cells with log2 D < -16, whose Hermite
+    // nodes lie in that range.
     for (int r = tid; r < n_lo + n_hi; r += blockDim.x) {
       const int j = r < n_lo ? r : kDTab - n_hi + (r - n_lo);
       const double mu = mu0 + j * hmu;
       const double aa = (ll_lo - mu) * inv_s, bb = (ll_hi - mu) * inv_s;
-      const double lnD = ln_mor_norm(aa, bb);
-      const double l2 = kLog2e * lnD;
-      const double dl2 =
-        hmu * inv_s * kLog2e * (exp(-0.5 * aa * aa - lnD) - exp(-0.5 * bb * bb - lnD)) / kSqrt2Pi;
+      const float lnDf = ln_mor_norm_f((float)aa, (float)bb);
+      double l2, dl2;
+      if (lnDf * (float)kLog2e >= -12.f) {
+        const float af = (float)aa, bf = (float)bb;
+        l2 = (double)(lnDf * (float)kLog2e);
+        dl2 = (double)((float)(hmu * inv_s * kLog2e / kSqrt2Pi) *
+                       (expf(-0.5f * af * af - lnDf) - expf(-0.5f * bf * bf - lnDf)));
+      } else {
+        const double lnD = ln_mor_norm(aa, bb);
+        l2 = kLog2e * lnD;
+        dl2 = hmu * inv_s * kLog2e * (exp(-0.5 * aa * aa - lnD) - exp(-0.5 * bb * bb - lnD)) /
+              kSqrt2Pi;
+      }
       dt64[j] = l2;
       dt64[kDTab + j] = dl2;
       dt32[j] = (float)l2;
@@ -672,18 +730,6 @@ prep_kernel(PrepArgs a)
     const double e = c2d * bmax * fmax(dmax, amax + 0.5 * bmax);
     if (!(e <= kMaxExp2)) set_err(a.status, kDevRange);
   }
-}
-
-// Bulk async copy global -> shared completing on mbarrier `bar` (16-byte
-// aligned addresses, a size that is a multiple of 16).
-__device__ __forceinline__ void
-bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
-{
-  asm volatile(
-    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-      smem_addr(dst)),
-    "l"(src), "r"(bytes), "r"(smem_addr(bar))
-    : "memory");
 }
 
 // Shared memory of yf_kernel: HMF grid in FP32 | row block | row scale |
@@ -1365,7 +1411,7 @@ build_grid(y3b_engine* e, int gi)
   g.ll_hi = std::log(in.lam_t_hi);
   g.sz0 = in.sz0;
   for (int j = 0; j < 8; ++j) g.sz_bin[j] = j < in.n_z_bins ? in.sz_bin[j] : 0.0;
-  Y3B_TRY(b->xm.alloc(g.n_m));
+  Y3B_TRY(b->xm.alloc(pad2(g.n_m)));  // even, for the prep kernel's bulk copy
   Y3B_TRY(b->wm.alloc(g.n_m));
   Y3B_TRY(b->xz.alloc(g.n_z));
   Y3B_TRY(b->wz.alloc(g.n_z));
@@ -1665,7 +1711,7 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
   }
   int ntp_max = 0;
   for (const auto& g : e->grids) ntp_max = std::max(ntp_max, g.n_t_pad);
-  e->prep_smem = prep_smem_bytes(L, e->w_stride, e->nz_max, ntp_max);
+  e->prep_smem = prep_smem_bytes(L, e->w_stride, e->nz_max, ntp_max, e->grids[0].nJ);
   e->yf_smem = yf_smem_bytes(L, (e->nz_max + 3) & ~3, ntp_max);
   e->direct_smem = ((size_t)e->nI_max * e->nt_max + e->nt_max) * 8;
   if (e->prep_smem > 200 * 1024 || e->yf_smem > 200 * 1024 || e->direct_smem > 200 * 1024) {
