@@ -194,6 +194,10 @@ ln_mor_norm_f(float a, float b)
 // alpha_k + beta_q, cubic Hermite interpolation (log D is smooth, so the
 // relative error of D stays ~1e-9 from the domain's interior to deep tails).
 constexpr int kDTab = 1024;
+// Threads of the prep kernel's CTA (one point): 128, eight CTAs per SM (the
+// kernel is latency-bound on short FP64 and shared-memory chains, so more
+// points in flight beat more threads per point).
+constexpr int kPrepThreads = 128;
 constexpr int kYfHdr = 8;        // floats of yf_kernel's FP32 header
 constexpr int kYfRowFields = 8;  // fields of yf_kernel's per-row block
 
@@ -226,7 +230,7 @@ prep_smem_bytes(const TableLayout& L, int n_m, int n_z, int n_t_pad, int nJ)
 // prep kernel admits; FP32 and BF16 hold 2^-126 .. 2^127.
 constexpr double kMaxExp2 = 100.0;
 
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(kPrepThreads, 8)
 prep_kernel(PrepArgs a)
 {
   extern __shared__ __align__(16) double psh[];
@@ -1962,7 +1966,7 @@ enqueue(y3b_engine* e, int prec, int n, const PointDev* d_pts, const double* d_t
   }
   {
     StageTimer t(e, s, 0);
-    prep_kernel<<<n, 256, e->prep_smem, s>>>(pa);
+    prep_kernel<<<n, kPrepThreads, e->prep_smem, s>>>(pa);
     count_launch();
     cudaError_t perr = cudaGetLastError();
     if (mixed && perr == cudaSuccess) {
