@@ -503,8 +503,6 @@ prep_kernel(PrepArgs a)
       (int)fmin(fmax(floor((ll_hi - 5.6 * sig - 0.01 - mu0) * inv_hmu) - 2.0, 0.0), (double)kDTab);
     const int n_lo = min(j_sat0 + 1, kDTab), n_hi = kDTab - max(j_sat1, n_lo);
     for (int j = n_lo + tid; j < kDTab - n_hi; j += blockDim.x) {
-      dt32[j] = 0.f;
-      dt32[kDTab + j] = 0.f;
       dt64[j] = 0.0;
       dt64[kDTab + j] = 0.0;
     }
@@ -532,8 +530,17 @@ prep_kernel(PrepArgs a)
       }
       dt64[j] = l2;
       dt64[kDTab + j] = dl2;
-      dt32[j] = (float)l2;
-      dt32[kDTab + j] = (float)dl2;
+    }
+    __syncthreads();
+    // yf_kernel's FP32 table: per interval [j, j + 1] the cubic Hermite in
+    // t = (mu - mu_j) / h as coefficients c0 + c1 t + c2 t^2 + c3 t^3 (one
+    // 16-byte load and three FMAs per cell), formed in FP64.
+    for (int j = tid; j < kDTab; j += blockDim.x) {
+      const int j1 = min(j + 1, kDTab - 1);
+      const double T0 = dt64[j], T1 = dt64[j1], D0 = dt64[kDTab + j], D1 = dt64[kDTab + j1];
+      *reinterpret_cast<float4*>(dt32 + 4 * j) =
+        make_float4((float)T0, (float)D0, (float)(3.0 * (T1 - T0) - 2.0 * D0 - D1),
+                    (float)(2.0 * (T0 - T1) + D0 + D1));
     }
   }
   if (tid == 0) {
@@ -749,7 +756,7 @@ __host__ __device__ inline size_t
 yf_smem_bytes(const TableLayout& L, int nzp_max, int n_t_pad_max)
 {
   return yf_h32_bytes(L) + (size_t)kYfRowFields * kGemmRows * 4 + kGemmRows * 8 + 16 +
-         kYfHdr * 4 + 8 * 8 + 3 * (size_t)nzp_max * 4 + 2 * (size_t)kDTab * 4 +
+         kYfHdr * 4 + 8 * 8 + 3 * (size_t)nzp_max * 4 + 4 * (size_t)kDTab * 4 +
          (size_t)n_t_pad_max * 4;
 }
 
@@ -790,8 +797,8 @@ yf_kernel(PrepArgs a)
   const float* qu = reinterpret_cast<const float*>(qy + nzp);
   const float* qb = qu + nzp;
   o += 3 * (size_t)nzp * 4;
-  const float* dt32 = reinterpret_cast<const float*>(ysh + o);  // [2][kDTab]
-  o += 2 * (size_t)kDTab * 4;
+  const float* dt32 = reinterpret_cast<const float*>(ysh + o);  // [kDTab][4] cubic coefficients
+  o += 4 * (size_t)kDTab * 4;
   const float* dt_f = reinterpret_cast<const float*>(ysh + o);  // [n_t_pad]
   __shared__ __align__(8) uint64_t bar;
   __shared__ int timed_out;
@@ -799,7 +806,7 @@ yf_kernel(PrepArgs a)
   const size_t n_dn = (size_t)n_hz * n_hm;
   const uint32_t h_bytes = L.hmf_f32 ? (uint32_t)yf_h32_bytes(L) : 0u;
   const uint32_t bytes = h_bytes + kYfRowFields * kGemmRows * 4 + kGemmRows * 8 + 16 + kYfHdr * 4 +
-                         64 + 12u * nzp + 8u * kDTab + 4u * n_t_pad;
+                         64 + 12u * nzp + 16u * kDTab + 4u * n_t_pad;
   if (tid == 0) {
     timed_out = 0;
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar)) : "memory");
@@ -818,7 +825,7 @@ yf_kernel(PrepArgs a)
     bulk_copy_g2s((void*)fh, s32 + Gp->f_hdr, kYfHdr * 4, &bar);
     bulk_copy_g2s((void*)th, s64 + Gp->o_thdr, 64, &bar);
     bulk_copy_g2s((void*)qy, s32 + Gp->f_q, 12u * nzp, &bar);
-    bulk_copy_g2s((void*)dt32, s32 + Gp->f_dt32, 8u * kDTab, &bar);
+    bulk_copy_g2s((void*)dt32, s32 + Gp->f_dt32, 16u * kDTab, &bar);
     bulk_copy_g2s((void*)dt_f, s32 + Gp->f_delta, 4u * n_t_pad, &bar);
   }
   if (!L.hmf_f32) {  // FP64 grid: convert while the copies are in flight
@@ -946,10 +953,9 @@ yf_kernel(PrepArgs a)
           if (!rok_s[r] || (rk[j] > sat_lo && rk[j] < sat_hi)) continue;
           const float uu = (rk[j] + bb - mu0c) * inv_hmu_f;
           const int jj = min(max((int)floorf(uu), 0), kDTab - 2);
-          const float t = uu - (float)jj, t2 = t * t, t3 = t2 * t;
-          const float l2d = (2.f * t3 - 3.f * t2 + 1.f) * dt32[jj] +
-                            (t3 - 2.f * t2 + t) * dt32[kDTab + jj] +
-                            (3.f * t2 - 2.f * t3) * dt32[jj + 1] + (t3 - t2) * dt32[kDTab + jj + 1];
+          const float t = uu - (float)jj;
+          const float4 cf = *reinterpret_cast<const float4*>(dt32 + 4 * jj);
+          const float l2d = fmaf(fmaf(fmaf(cf.w, t, cf.z), t, cf.y), t, cf.x);
           if (l2d >= -16.f && rvf_s[r] == 0.f) {
             y[j] = nv[j] * fast_exp2(e[j] - l2d);
             continue;
@@ -1571,7 +1577,7 @@ build_grid(y3b_engine* e, int gi)
   g.f_q = f;
   f += 3 * (size_t)g.nzp;
   g.f_dt32 = f;
-  f += 2 * (size_t)kDTab;
+  f += 4 * (size_t)kDTab;
   g.f_rows = f;
   f += (size_t)kYfRowFields * g.n_m_pad;
   g.f_Yt = f;
