@@ -297,6 +297,14 @@ prep_kernel(PrepArgs a)
     bulk_copy_g2s(g_wz, Gp->wz, (uint32_t)(n_z * 8), &bar);
     bulk_copy_g2s(g_omz, Gp->omz, (uint32_t)(n_z * 8), &bar);
     bulk_copy_g2s(g_Kj, Gp->Kj, (uint32_t)((size_t)nJ * n_z * 8), &bar);
+    // The mixed form's HMF grid is read next by yf_kernel (both of the
+    // point's lnM tiles): start bringing it into L2 now.
+    if (a.mixed) {
+      const size_t n_dn = (size_t)n_hz * n_hm;
+      const uint32_t hb = (uint32_t)(L.hmf_f32 ? ((n_dn + 1) / 2 + 1) / 2 * 16 : (n_dn * 8 + 15) & ~size_t(15));
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src + L.off[2]), "r"(hb)
+                   : "memory");
+    }
   }
   {
     long long t0 = clock64();
