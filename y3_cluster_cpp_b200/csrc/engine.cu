@@ -1153,7 +1153,9 @@ shear_phi_kernel(const GridDev* grids, const PointDev* pts, int n_points, int w_
 // the mass, so DeltaSigma_mis(x, x_mis) is a smooth function of u = ln x
 // alone: tabulated once per engine in FP64 at kMisNx nodes per (i, R) pair
 // (the same direct quadrature as the FP64 form), read with 4-point Lagrange
-// interpolation in u (relative error ~1e-8 at this spacing).
+// interpolation in u (relative error ~1e-8 at this spacing).  One more row
+// after the (i, R) pairs holds the centred DeltaSigma_NFW(x) on the same
+// nodes, so the mixed form reads both profiles with the same weights.
 constexpr int kMisNx = 2048;
 
 __global__ void __launch_bounds__(128)
@@ -1161,8 +1163,12 @@ mis_table_kernel(ShearDev sh, MisQuad quad, int n_pairs, double u0, double du, d
 {
   const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (w >= (long long)n_pairs * kMisNx) return;
+  if (w >= (long long)(n_pairs + 1) * kMisNx) return;
   const int pair = (int)(w / kMisNx), j = (int)(w % kMisNx);
+  if (pair == n_pairs) {  // the centred profile (warp-uniform branch)
+    if (lane == 0) tab[w] = NfwUnit<double>::dsigma(exp(u0 + j * du));
+    return;
+  }
   const int i = pair / sh.n_R, iR = pair % sh.n_R;
   const double ratio = sh.tau_mis * pow(sh.lob[i] / 100.0, 0.2) / sh.R[iR];
   const double x = exp(u0 + j * du);
@@ -1171,10 +1177,11 @@ mis_table_kernel(ShearDev sh, MisQuad quad, int n_pairs, double u0, double du, d
 }
 
 // Phi_i(R, k) of the mixed form from the table, one thread per (point, k):
-// c(M), r_s and the normalisation once, the centred profile once per R, the
-// table read once per (i, R).  A point whose x = R / r_s falls outside the
-// table reports a domain error (the table covers Omega_m from 0.01 to 1 over
-// the engine's masses and radii).
+// c(M), r_s and the normalisation once; per R the table position
+// u = ln R - ln r_s and its 4-point Lagrange weights, then the centred
+// profile and the miscentred one of each bin i from their rows.  A point
+// whose x = R / r_s falls outside the table reports a domain error (the
+// table covers Omega_m from 0.01 to 1 over the engine's masses and radii).
 __global__ void __launch_bounds__(128)
 shear_tab_kernel(const GridDev* grids, const PointDev* pts, int n_points, int w_stride,
                  ShearDev sh, const double* tab, double u0, double inv_du, double* Phi,
@@ -1190,13 +1197,13 @@ shear_tab_kernel(const GridDev* grids, const PointDev* pts, int n_points, int w_
   const double lnM = G.xm[k];
   const double c = sh.c0 * pow(exp(lnM) / sh.c_pivot, sh.c_slope);
   const double rho = kRhoCrit * pt.om;
-  const double inv_rs = 1.0 / nfw_rs(lnM, c, rho);
+  const double rs = nfw_rs(lnM, c, rho);
   const double norm = nfw_norm(lnM, c, rho);
+  const double ln_rs = log(rs);
+  const double* cen_row = tab + (size_t)nI_max * sh.n_R * kMisNx;
   bool bad = false;
   for (int iR = 0; iR < sh.n_R; ++iR) {
-    const double x = sh.R[iR] * inv_rs;
-    const double cen = (1.0 - sh.f_mis) * NfwUnit<double>::dsigma(x);
-    const double tt = (log(x) - u0) * inv_du;
+    const double tt = (sh.lnR[iR] - ln_rs - u0) * inv_du;
     int j = (int)floor(tt);
     if (!(tt >= 1.0 && tt <= kMisNx - 2.0)) {
       bad = true;
@@ -1205,9 +1212,12 @@ shear_tab_kernel(const GridDev* grids, const PointDev* pts, int n_points, int w_
     const double f = tt - j;
     const double l0 = -f * (f - 1.0) * (f - 2.0) / 6.0, l1 = (f + 1.0) * (f - 1.0) * (f - 2.0) * 0.5;
     const double l2 = -(f + 1.0) * f * (f - 2.0) * 0.5, l3 = (f + 1.0) * f * (f - 1.0) / 6.0;
+    const double* yc = cen_row + j;
+    const double cen =
+      (1.0 - sh.f_mis) * (l0 * __ldg(yc - 1) + l1 * __ldg(yc) + l2 * __ldg(yc + 1) + l3 * __ldg(yc + 2));
     for (int i = 0; i < G.nI; ++i) {
       const double* y = tab + ((size_t)i * sh.n_R + iR) * kMisNx + j;
-      const double mis = l0 * y[-1] + l1 * y[0] + l2 * y[1] + l3 * y[2];
+      const double mis = l0 * __ldg(y - 1) + l1 * __ldg(y) + l2 * __ldg(y + 1) + l3 * __ldg(y + 2);
       Phi[(((size_t)p * nI_max + i) * sh.n_R + iR) * w_stride + k] =
         norm * (cen + sh.f_mis * mis);
     }
@@ -1282,7 +1292,7 @@ struct y3b_engine {
   y3b::TableLayout lay;
   y3b::ShearDev shear;
   y3b::MisQuadCache quad;
-  y3b::DevBuf<double> mis_tab;          // [nI_max * n_R][kMisNx], mixed form
+  y3b::DevBuf<double> mis_tab;          // [nI_max * n_R + 1][kMisNx], mixed form
   double mis_u0 = 0.0, mis_du = 1.0;
   cudaStream_t stream = nullptr;
   y3b::DevBuf<y3b::PointDev> pts;
@@ -1790,7 +1800,10 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
   std::memset(&sh, 0, sizeof(sh));
   if (cfg->with_shear) {
     sh.n_R = cfg->shear.n_R;
-    for (int r = 0; r < sh.n_R; ++r) sh.R[r] = cfg->shear.R[r];
+    for (int r = 0; r < sh.n_R; ++r) {
+      sh.R[r] = cfg->shear.R[r];
+      sh.lnR[r] = std::log(sh.R[r]);
+    }
     sh.f_mis = cfg->shear.f_mis;
     sh.tau_mis = cfg->shear.tau_mis;
     for (int i = 0; i < kMaxLamBins; ++i) sh.lob[i] = cfg->shear.lob_centers[i];
@@ -1817,8 +1830,8 @@ y3b_engine_create(const y3b_grid* grids, int n_grids, const y3b_engine_config* c
     e->mis_u0 = std::log(x_lo / 1.5);
     e->mis_du = (std::log(x_hi * 1.5) - e->mis_u0) / (kMisNx - 1);
     const int n_pairs = e->nI_max * sh.n_R;
-    if ((rc = e->mis_tab.alloc((size_t)n_pairs * kMisNx))) return fail(rc);
-    const long long threads = (long long)n_pairs * kMisNx * 32;
+    if ((rc = e->mis_tab.alloc((size_t)(n_pairs + 1) * kMisNx))) return fail(rc);
+    const long long threads = (long long)(n_pairs + 1) * kMisNx * 32;
     mis_table_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, e->stream>>>(
       sh, e->quad.view(), n_pairs, e->mis_u0, e->mis_du, e->mis_tab.get());
     count_launch();

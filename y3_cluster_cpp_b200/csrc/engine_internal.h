@@ -83,6 +83,7 @@ struct TableLayout {
 struct ShearDev {
   int n_R;
   double R[kMaxR];
+  double lnR[kMaxR];  // ln R, for the mixed form's table reads
   double f_mis, tau_mis;
   double lob[kMaxLamBins];
   double c0, c_slope, c_pivot;
