@@ -902,7 +902,6 @@ yf_kernel(PrepArgs a)
     const float* rn_s = rows + 2 * kGemmRows;
     const float* ra_s = rows + 3 * kGemmRows;
     const float* rvf_s = rows + 6 * kGemmRows;
-    const int* rok_s = reinterpret_cast<const int*>(rows + 7 * kGemmRows);
     // Runs of whole pairs of z rows (n_z is a multiple of 16): Y is stored
     // [lnM tile][z / 2][128 rows][2], one float2 per lane and row.
     const int qs = ((n_z / 2 + nw - 1) / nw) * 2, qa = warp * qs, qb_end = min(n_z, qa + qs);
@@ -955,39 +954,51 @@ yf_kernel(PrepArgs a)
         y[j] = nv[j] * fast_exp2(e[j]);
       }
       if (!(tmin > sat_lo && tmax < sat_hi)) {  // some cell of this z row is unsaturated
+        // The lane's four cells side by side and without branches (their
+        // chains interleave): the FP32 Hermite of log2 D for each, kept
+        // where the cell is unsaturated.  Deep-tail cells and rows that
+        // carry a scale follow in the rare FP64 pass below.
+        unsigned deep = 0u;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           const int r = lane + 32 * j;
-          if (!rok_s[r] || (rk[j] > sat_lo && rk[j] < sat_hi)) continue;
+          const bool sl = mt0 * kGemmRows + r < n_m && !(rk[j] > sat_lo && rk[j] < sat_hi);
           const float uu = (rk[j] + bb - mu0c) * inv_hmu_f;
           const int jj = min(max((int)floorf(uu), 0), kDTab - 2);
           const float t = uu - (float)jj;
           const float4 cf = *reinterpret_cast<const float4*>(dt32 + 4 * jj);
           const float l2d = fmaf(fmaf(fmaf(cf.w, t, cf.z), t, cf.y), t, cf.x);
-          if (l2d >= -16.f && rvf_s[r] == 0.f) {
-            y[j] = nv[j] * fast_exp2(e[j] - l2d);
-            continue;
-          }
-          const int k = mt0 * kGemmRows + r;
-          const double alpha = __ldg(s64 + Gp->o_alpha + k), beta = __ldg(s64 + Gp->o_beta + q);
-          const double mu = alpha + beta;
-          const double ud = (mu - th[2]) * th[3];
-          const int jd = min(max((int)floor(ud), 0), kDTab - 2);
-          const double td = ud - jd, td2 = td * td, td3 = td2 * td;
-          const double* d64 = s64 + Gp->o_dt64;
-          const double l2 = (2.0 * td3 - 3.0 * td2 + 1.0) * __ldg(d64 + jd) +
-                            (td3 - 2.0 * td2 + td) * __ldg(d64 + kDTab + jd) +
-                            (3.0 * td2 - 2.0 * td3) * __ldg(d64 + jd + 1) +
-                            (td3 - td2) * __ldg(d64 + kDTab + jd + 1);
-          const double ad = alpha - th[0], bd = beta - th[1];
-          const double ex = -(ad * bd + 0.5 * bd * bd) * th[4] - row_vv[r] - l2;
-          const double ei = rint(ex);
-          const float yf = mul_pow2(nv[j] * fast_exp2((float)(ex - ei)), ei);
-          if (!(fabsf(yf) <= 3.402823466e38f)) {  // not representable: report, never a NaN
-            set_err(a.status, kDevRange);
-            y[j] = 0.f;
-          } else {
-            y[j] = yf;
+          const float ys = nv[j] * fast_exp2(e[j] - l2d);
+          const bool shallow = l2d >= -16.f && (!scaled || rvf_s[r] == 0.f);
+          y[j] = sl && shallow ? ys : y[j];
+          deep |= (sl && !shallow) ? 1u << j : 0u;
+        }
+        if (deep) {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            if (!(deep & (1u << j))) continue;
+            const int r = lane + 32 * j;
+            const int k = mt0 * kGemmRows + r;
+            const double alpha = __ldg(s64 + Gp->o_alpha + k), beta = __ldg(s64 + Gp->o_beta + q);
+            const double mu = alpha + beta;
+            const double ud = (mu - th[2]) * th[3];
+            const int jd = min(max((int)floor(ud), 0), kDTab - 2);
+            const double td = ud - jd, td2 = td * td, td3 = td2 * td;
+            const double* d64 = s64 + Gp->o_dt64;
+            const double l2 = (2.0 * td3 - 3.0 * td2 + 1.0) * __ldg(d64 + jd) +
+                              (td3 - 2.0 * td2 + td) * __ldg(d64 + kDTab + jd) +
+                              (3.0 * td2 - 2.0 * td3) * __ldg(d64 + jd + 1) +
+                              (td3 - td2) * __ldg(d64 + kDTab + jd + 1);
+            const double ad = alpha - th[0], bd = beta - th[1];
+            const double ex = -(ad * bd + 0.5 * bd * bd) * th[4] - row_vv[r] - l2;
+            const double ei = rint(ex);
+            const float yf = mul_pow2(nv[j] * fast_exp2((float)(ex - ei)), ei);
+            if (!(fabsf(yf) <= 3.402823466e38f)) {  // not representable: report, never a NaN
+              set_err(a.status, kDevRange);
+              y[j] = 0.f;
+            } else {
+              y[j] = yf;
+            }
           }
         }
       }
