@@ -1262,16 +1262,38 @@ finalize_kernel(const GridDev* grids, const PointDev* pts, const double* W, cons
     }
   }
   if (shear && Phi) {
-    for (int u = warp; u < G.nB * n_R; u += nw) {
-      const int b = u / n_R, iR = u % n_R, i = b % G.nI;
-      const double* Wb = Wg + ((size_t)p * G.nB + b) * w_stride;
-      const double* ph = Phi + (((size_t)p * nI_max + i) * n_R + iR) * w_stride;
-      double acc = 0.0;
-      for (int k = lane; k < G.n_m; k += 32) acc += G.wm[k] * Wb[k] * ph[k];
-      acc = warp_sum(acc);
+    // Four outputs per warp pass, their loads and shuffle trees side by side
+    // (each output's own order is unchanged: lane partials over k, then the
+    // xor tree).
+    const int n_out = G.nB * n_R;
+    for (int u0 = warp; u0 < n_out; u0 += 4 * nw) {
+      double acc[4];
+      const double* Wb[4];
+      const double* ph[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int u = min(u0 + c * nw, n_out - 1);
+        const int b = u / n_R, iR = u % n_R, i = b % G.nI;
+        Wb[c] = Wg + ((size_t)p * G.nB + b) * w_stride;
+        ph[c] = Phi + (((size_t)p * nI_max + i) * n_R + iR) * w_stride;
+        acc[c] = 0.0;
+      }
+      for (int k = lane; k < G.n_m; k += 32) {
+        const double wk = G.wm[k];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[c] += wk * Wb[c][k] * ph[c][k];
+      }
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[c] = warp_sum(acc[c]);
       if (lane == 0) {
-        shear[((size_t)p * nB_max + b) * n_R + iR] = acc;
-        s_sh[u] = acc;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const int u = u0 + c * nw;
+          if (u >= n_out) break;
+          const int b = u / n_R, iR = u % n_R;
+          shear[((size_t)p * nB_max + b) * n_R + iR] = acc[c];
+          s_sh[u] = acc[c];
+        }
       }
     }
   }
