@@ -808,16 +808,21 @@ yf_kernel(PrepArgs a)
   const float* dt32 = reinterpret_cast<const float*>(ysh + o);  // [kDTab][4] cubic coefficients
   o += 4 * (size_t)kDTab * 4;
   const float* dt_f = reinterpret_cast<const float*>(ysh + o);  // [n_t_pad]
-  __shared__ __align__(8) uint64_t bar;
+  // Two groups of copies: what the F blocks need (row block, headers,
+  // z rows, delta_t) on `bar`, the HMF grid and the log2 D table on `bar2`,
+  // which land while the F blocks are written.
+  __shared__ __align__(8) uint64_t bar, bar2;
   __shared__ int timed_out;
   int bad = 0;
   const size_t n_dn = (size_t)n_hz * n_hm;
   const uint32_t h_bytes = L.hmf_f32 ? (uint32_t)yf_h32_bytes(L) : 0u;
-  const uint32_t bytes = h_bytes + kYfRowFields * kGemmRows * 4 + kGemmRows * 8 + 16 + kYfHdr * 4 +
-                         64 + 12u * nzp + 16u * kDTab + 4u * n_t_pad;
+  const uint32_t bytes = kYfRowFields * kGemmRows * 4 + kGemmRows * 8 + 16 + kYfHdr * 4 + 64 +
+                         12u * nzp + 4u * n_t_pad;
+  const uint32_t bytes2 = h_bytes + 16u * kDTab;
   if (tid == 0) {
     timed_out = 0;
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar2)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
@@ -825,7 +830,10 @@ yf_kernel(PrepArgs a)
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar)),
                  "r"(bytes)
                  : "memory");
-    if (h_bytes) bulk_copy_g2s(h32, src + L.off[2], h_bytes, &bar);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar2)),
+                 "r"(bytes2)
+                 : "memory");
+    if (h_bytes) bulk_copy_g2s(h32, src + L.off[2], h_bytes, &bar2);
     bulk_copy_g2s(rows, s32 + Gp->f_rows + (size_t)mt0 * kYfRowFields * kGemmRows,
                   kYfRowFields * kGemmRows * 4, &bar);
     bulk_copy_g2s(row_vv, s64 + Gp->o_vv + (size_t)mt0 * kGemmRows, kGemmRows * 8, &bar);
@@ -833,8 +841,65 @@ yf_kernel(PrepArgs a)
     bulk_copy_g2s((void*)fh, s32 + Gp->f_hdr, kYfHdr * 4, &bar);
     bulk_copy_g2s((void*)th, s64 + Gp->o_thdr, 64, &bar);
     bulk_copy_g2s((void*)qy, s32 + Gp->f_q, 12u * nzp, &bar);
-    bulk_copy_g2s((void*)dt32, s32 + Gp->f_dt32, 16u * kDTab, &bar);
+    bulk_copy_g2s((void*)dt32, s32 + Gp->f_dt32, 16u * kDTab, &bar2);
     bulk_copy_g2s((void*)dt_f, s32 + Gp->f_delta, 4u * n_t_pad, &bar);
+  }
+  // Bounded waits (every thread polls the phase); a CTA that gives up on the
+  // first group still waits, bounded, for the second before it leaves.
+  auto wait_bar = [&](uint64_t* b) {
+    long long t0 = clock64();
+    uint32_t ok = 0;
+    while (!ok) {
+      asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(b))
+        : "memory");
+      if (!ok && clock64() - t0 > 2000000000LL) {
+        timed_out = 1;
+        break;
+      }
+    }
+  };
+  wait_bar(&bar);
+  __syncthreads();
+  if (timed_out) {  // uniform exit; the copies only target this CTA's shared memory
+    wait_bar(&bar2);
+    if (tid == 0) set_err(a.status, kDevTimeout);
+    return;
+  }
+  const float sc1 = fh[3];
+  // F'(t, k) for the contraction (the row scale above), split into bf16
+  // hi + lo and written in its shared-memory stage layout: block
+  // (lnM tile, stage) of kFStageBytes, hi planes then lo planes, each plane
+  // 8 lam_t nodes x 128 rows of 16 bytes.  Rows past n_m are zero.  The
+  // exponent is >= 0 on every real node; the padded nodes past n_t (whose G
+  // is zero) take its magnitude, so F' <= 1 stays finite there too.  Only
+  // the stages inside the tile's window are ever read.
+  const int win = tinfo[3], w_lo = win & 0xFFFF, w_hi = win >> 16;
+  const float* row_am = rows + 4 * kGemmRows;
+  const float* row_vs2 = rows + 5 * kGemmRows;
+  const float2 sc2 = make_float2(sc1, sc1);
+  uint8_t* fb = a.fbuf + (size_t)p * a.f_stride;
+  const int nk = n_t_pad / 16;
+  for (int it = w_lo * 2 * kGemmRows + tid; it < w_hi * 2 * kGemmRows; it += blockDim.x) {
+    const int r = it % kGemmRows, t8 = it / kGemmRows;
+    const float am = row_am[r], vs = row_vs2[r];
+    const float2 nam2 = make_float2(-am, -am), vs2 = make_float2(vs, vs);
+    const float4 d0 = *reinterpret_cast<const float4*>(dt_f + t8 * 8);
+    const float4 d1 = *reinterpret_cast<const float4*>(dt_f + t8 * 8 + 4);
+    const float2 dd[4] = {make_float2(d0.x, d0.y), make_float2(d0.z, d0.w),
+                          make_float2(d1.x, d1.y), make_float2(d1.z, d1.w)};
+    float2 v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const float2 x = __ffma2_rn(dd[u], sc2, nam2);
+      const float2 e = __fmul2_rn(x, __fadd2_rn(x, vs2));
+      v[u] = make_float2(fast_exp2(-fabsf(e.x)), fast_exp2(-fabsf(e.y)));
+    }
+    uint8_t* st = fb + ((size_t)mt0 * nk + (t8 >> 1)) * kFStageBytes + (t8 & 1) * 2048 + r * 16;
+    store_split8(st, st + kFStageBytes / 2, v);
   }
   if (!L.hmf_f32) {  // FP64 grid: convert while the copies are in flight
     const double* __restrict__ dng = src + L.off[2];
@@ -854,24 +919,9 @@ yf_kernel(PrepArgs a)
       }
     }
   }
-  {
-    long long t0 = clock64();
-    uint32_t ok = 0;
-    while (!ok) {
-      asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok)
-        : "r"(smem_addr(&bar))
-        : "memory");
-      if (!ok && clock64() - t0 > 2000000000LL) {
-        timed_out = 1;
-        break;
-      }
-    }
-  }
+  wait_bar(&bar2);
   __syncthreads();
-  if (timed_out) {  // uniform exit; the copies only target this CTA's shared memory
+  if (timed_out) {
     if (tid == 0) set_err(a.status, kDevTimeout);
     return;
   }
@@ -882,7 +932,7 @@ yf_kernel(PrepArgs a)
     return;
   }
   const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
-  const float c2 = fh[0], mu_sat_lo = fh[1], mu_sat_hi = fh[2], sc1 = fh[3];
+  const float c2 = fh[0], mu_sat_lo = fh[1], mu_sat_hi = fh[2];
   const float mu0c = fh[4], inv_hmu_f = fh[5];
   // Y(k, q) = n(M_k, z_q) kf_k H(k, q) 2^-(v_k^2 c1) / (sqrt(2 pi) s D_kq).
   // Warp w takes a contiguous run of z rows and lane the tile rows
@@ -1010,38 +1060,6 @@ yf_kernel(PrepArgs a)
       *reinterpret_cast<float2*>(yblk + ((size_t)(q0 >> 1) * kGemmRows + lane + 32 * j) * 2) =
         make_float2(yv[j][0], yv[j][1]);
     }
-  }
-  // F'(t, k) for the contraction (the row scale above), split into bf16
-  // hi + lo and written in its shared-memory stage layout: block
-  // (lnM tile, stage) of kFStageBytes, hi planes then lo planes, each plane
-  // 8 lam_t nodes x 128 rows of 16 bytes.  Rows past n_m are zero.  The
-  // exponent is >= 0 on every real node; the padded nodes past n_t (whose G
-  // is zero) take its magnitude, so F' <= 1 stays finite there too.  Only
-  // the stages inside the tile's window are ever read.
-  (void)n_m;
-  const int win = tinfo[3], w_lo = win & 0xFFFF, w_hi = win >> 16;
-  const float* row_am = rows + 4 * kGemmRows;
-  const float* row_vs2 = rows + 5 * kGemmRows;
-  const float2 sc2 = make_float2(sc1, sc1);
-  uint8_t* fb = a.fbuf + (size_t)p * a.f_stride;
-  const int nk = n_t_pad / 16;
-  for (int it = w_lo * 2 * kGemmRows + tid; it < w_hi * 2 * kGemmRows; it += blockDim.x) {
-    const int r = it % kGemmRows, t8 = it / kGemmRows;
-    const float am = row_am[r], vs = row_vs2[r];
-    const float2 nam2 = make_float2(-am, -am), vs2 = make_float2(vs, vs);
-    const float4 d0 = *reinterpret_cast<const float4*>(dt_f + t8 * 8);
-    const float4 d1 = *reinterpret_cast<const float4*>(dt_f + t8 * 8 + 4);
-    const float2 dd[4] = {make_float2(d0.x, d0.y), make_float2(d0.z, d0.w),
-                          make_float2(d1.x, d1.y), make_float2(d1.z, d1.w)};
-    float2 v[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const float2 x = __ffma2_rn(dd[u], sc2, nam2);
-      const float2 e = __fmul2_rn(x, __fadd2_rn(x, vs2));
-      v[u] = make_float2(fast_exp2(-fabsf(e.x)), fast_exp2(-fabsf(e.y)));
-    }
-    uint8_t* st = fb + ((size_t)mt0 * nk + (t8 >> 1)) * kFStageBytes + (t8 & 1) * 2048 + r * 16;
-    store_split8(st, st + kFStageBytes / 2, v);
   }
 }
 
