@@ -218,8 +218,9 @@ constexpr int kEvalChunks = 8;  // chunks of a large host-buffer evaluation
 __host__ __device__ inline size_t
 prep_smem_bytes(const TableLayout& L, int n_m, int n_z, int n_t_pad, int nJ)
 {
-  size_t b = (L.off[2] + L.stride - L.off[3]) * 8;         // table block without dn/dlnM
-  b += ((size_t)((n_m + 1) & ~1) + (size_t)(3 + nJ) * n_z) * 8;  // grid nodes, weights, K_j
+  // table block without dn/dlnM, grid nodes, weights, K_j; later the log2 D table
+  const size_t b0 = (L.off[2] + L.stride - L.off[3]) + ((n_m + 1) & ~1) + (size_t)(3 + nJ) * n_z;
+  size_t b = (b0 > 2 * (size_t)kDTab ? b0 : 2 * (size_t)kDTab) * 8;
   b += (size_t)n_m * (8 + 8 + 8 + 4);                      // alpha, t, kf, xi
   b += (size_t)n_z * (8 + 8 + 4);                          // beta, u, yi
   b += 16 + (size_t)n_t_pad * 4;                           // FP32 delta_t (mixed form)
@@ -255,7 +256,10 @@ prep_kernel(PrepArgs a)
   double* g_wz = g_xz + n_z;         // [n_z]
   double* g_omz = g_wz + n_z;        // [n_z]
   double* g_Kj = g_omz + n_z;        // [nJ n_z]
-  double* k_alpha = g_Kj + (size_t)nJ * n_z;
+  // Once the per-lnM and per-z factors are formed, the log2 D table is built
+  // over the region of the staged tables and grid arrays.
+  double* dtS = psh;  // [2 kDTab]
+  double* k_alpha = psh + max((size_t)(g_Kj + (size_t)nJ * n_z - psh), (size_t)2 * kDTab);
   double* k_t = k_alpha + n_m;
   double* k_f = k_t + n_m;
   double* q_beta = k_f + n_m;
@@ -511,8 +515,8 @@ prep_kernel(PrepArgs a)
       (int)fmin(fmax(floor((ll_hi - 5.6 * sig - 0.01 - mu0) * inv_hmu) - 2.0, 0.0), (double)kDTab);
     const int n_lo = min(j_sat0 + 1, kDTab), n_hi = kDTab - max(j_sat1, n_lo);
     for (int j = n_lo + tid; j < kDTab - n_hi; j += blockDim.x) {
-      dt64[j] = 0.0;
-      dt64[kDTab + j] = 0.0;
+      dtS[j] = 0.0;
+      dtS[kDTab + j] = 0.0;
     }
     // Nodes evaluated in FP32 (transcendentals an order of magnitude faster
     // than FP64 here); where log2 D < -12 (the FP32 value's absolute error
@@ -536,16 +540,19 @@ prep_kernel(PrepArgs a)
         dl2 = hmu * inv_s * kLog2e * (exp(-0.5 * aa * aa - lnD) - exp(-0.5 * bb * bb - lnD)) /
               kSqrt2Pi;
       }
-      dt64[j] = l2;
-      dt64[kDTab + j] = dl2;
+      dtS[j] = l2;
+      dtS[kDTab + j] = dl2;
     }
     __syncthreads();
-    // yf_kernel's FP32 table: per interval [j, j + 1] the cubic Hermite in
-    // t = (mu - mu_j) / h as coefficients c0 + c1 t + c2 t^2 + c3 t^3 (one
-    // 16-byte load and three FMAs per cell), formed in FP64.
+    // The FP64 table, and yf_kernel's FP32 one: per interval [j, j + 1] the
+    // cubic Hermite in t = (mu - mu_j) / h as coefficients
+    // c0 + c1 t + c2 t^2 + c3 t^3 (one 16-byte load and three FMAs per
+    // cell), formed in FP64.
     for (int j = tid; j < kDTab; j += blockDim.x) {
       const int j1 = min(j + 1, kDTab - 1);
-      const double T0 = dt64[j], T1 = dt64[j1], D0 = dt64[kDTab + j], D1 = dt64[kDTab + j1];
+      const double T0 = dtS[j], T1 = dtS[j1], D0 = dtS[kDTab + j], D1 = dtS[kDTab + j1];
+      dt64[j] = T0;
+      dt64[kDTab + j] = D0;
       *reinterpret_cast<float4*>(dt32 + 4 * j) =
         make_float4((float)T0, (float)D0, (float)(3.0 * (T1 - T0) - 2.0 * D0 - D1),
                     (float)(2.0 * (T0 - T1) + D0 + D1));
