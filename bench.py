@@ -490,6 +490,69 @@ def prj_latency(n_calls=30):
             "reference_published_ms": 82.0}
 
 
+def bsel_run(n_calls=30, n_batch=256):
+    """The selection-bias operators P1, I1, J (y3b_bsel_eval; 12 (z_obs bin,
+    richness bin) points, default nodes: 60 lam_t x 24 lnM x up to 80 z x 10
+    theta, 80 reference z nodes): per-sample latency through the host-buffer
+    call, batched throughput over seeded walkers, and the reference's own
+    P_operator (compiled from its sources, where present) timed on one host
+    core on the same samples, next to the reference's published 66-74 ms."""
+    import numpy as np
+
+    from oracle import ref as R
+    from y3_cluster_cpp_b200 import engine, synthetic
+    grid = dict(zo_low=np.repeat([0.2, 0.35, 0.5], 4), zo_high=np.repeat([0.35, 0.5, 0.65], 4),
+                lambda_bin=np.tile(np.arange(4), 3))
+    lo, hi = np.log(1e13), np.log(10 ** 15.5)
+    hod = dict(log10_Mmin=11.7, log10_M1=12.9, alpha=0.85, epsilon=0.2, sigma_lambda=0.2)
+    pts = synthetic.walkers(n_batch, seed=3, densities=(1,), with_sci=False)
+    prj0 = synthetic.prj_tables(pts[0], n_r=120)
+    samples = [(engine.cosmo(p.om, p.h0), p.tables, synthetic.prj_tables(p, n_r=120),
+                dict(hod, alpha=0.8 + 0.1 * (i % 4) / 3)) for i, p in enumerate(pts)]
+    h1 = engine.BselMarg(grid, lo, hi, max_samples=1)
+    for _ in range(3):
+        h1.eval(samples[:1])
+    ts = []
+    for _ in range(n_calls):
+        t0 = time.perf_counter()
+        h1.eval(samples[:1])
+        ts.append(time.perf_counter() - t0)
+    h1.close()
+    hb = engine.BselMarg(grid, lo, hi, max_samples=n_batch)
+    hb.eval(samples)
+    tb = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        out = hb.eval(samples)
+        tb.append(time.perf_counter() - t0)
+    hb.close()
+    res = {"observable": "P_operator (b_sel_marg): P1, I1, J on 12 (z_obs bin, richness bin) "
+                         "points, 60 lam_t x 24 lnM x <=80 z x 10 theta",
+           "ms_per_sample": 1e3 * statistics.median(ts), "calls": n_calls,
+           "batched": {"samples": n_batch, "samples_per_s": n_batch / statistics.median(tb),
+                       "ms_per_call": 1e3 * statistics.median(tb)},
+           "reference_published_ms": [66.0, 74.0]}
+    del prj0
+    if R.available():
+        n_ref = 4
+        t0 = time.perf_counter()
+        refs = []
+        for p, smp in zip(pts[:n_ref], samples[:n_ref]):
+            cz = dict(omega_m=p.om, omega_nu=0.0, omega_lambda=1.0 - p.om, omega_k=0.0,
+                      h0=p.h0, hmf_s=0.0, hmf_q=1.0)
+            refs.append(R.bsel_marg(dict(lnm_low=lo, lnm_high=hi), cz, p.tables, smp[2], smp[3],
+                                    grid))
+        dt = (time.perf_counter() - t0) / n_ref
+        refs = np.stack(refs)
+        scale = np.max(np.abs(refs), axis=(0, 1))
+        res["reference_cpu"] = {"ms_per_sample": 1e3 * dt, "cores": 1, "kind": "reference",
+                                "sample": f"{n_ref} walkers, the reference's P_operator "
+                                          "compiled from its sources, 1 thread"}
+        res["max_abs_diff_vs_reference_over_scale"] = float(
+            np.max(np.abs(out[:n_ref] - refs) / scale))
+    return res
+
+
 def serving_run(a, rank, dev):
     """Serving workload: a Poisson request stream (mean gap 2 ms) of requests
     of 1..1024 points (log-uniform), points from the batched-config prior at
@@ -799,6 +862,7 @@ def run_ours(a):
         serving = serving_run(a, rank, dev)
     modlat = module_latency() if a.extra_workloads else None
     prjlat = prj_latency() if a.extra_workloads else None
+    bsel = bsel_run() if a.extra_workloads else None
     extra = None
     if a.extra_workloads:
         from y3_cluster_cpp_b200 import synthetic as _syn
@@ -862,6 +926,8 @@ def run_ours(a):
             line["module_execute"] = modlat
         if prjlat is not None:
             line["projection_shear"] = prjlat
+        if bsel is not None:
+            line["selection_bias"] = bsel
         if extra is not None:
             line["other_workloads"] = extra
         if cpu is not None:

@@ -22,6 +22,10 @@
  *   y3b_prj_*               src/models/sigma_prj_frozen_t.hh:34-512
  *                           (ShearPrjFrozenPhysics, module
  *                           src/modules/sigma_prj_cpu/ShearPrjFrozenPhysics.cc)
+ *   y3b_bsel_*              src/models/p_operator_t.hh:76-718
+ *                           (P_operator: the selection-bias operators P1,
+ *                           I1, J; module src/modules/b_sel_marg_cpu/
+ *                           BSelMargIntegrand.cc)
  *   y3b_engine_*            the fused fast_mass form of the same integrals
  *                           (NumCountsFastMass / Shear1hFastMass, documented
  *                           as identical to the two modules above), with the
@@ -258,6 +262,52 @@ int y3b_prj_set_mis_table(y3b_prj* h, int n_lx, const double* logx, int n_lxm,
  * lies outside distances/z. */
 int y3b_prj_eval(y3b_prj* h, const y3b_prj_sample* s, double* out);
 void y3b_prj_destroy(y3b_prj* h);
+
+/* ---------------------------------------------------------------------- */
+/* Selection-bias operators P1, I1, J on the (zo_low, zo_high, lambda_bin) */
+/* wall grid (P_operator, module label b_sel_marg,                          */
+/* src/models/p_operator_t.hh:76-718; outputs b_sel_marg_P1 / _I1 / _J).   */
+
+/* Module options (p_operator_t.hh:95-110): node counts (defaults n_lt 60,
+ * n_zring 20, n_zouter 30, n_lnm 24, n_theta 10, n_zt_ref 80), the reference
+ * z grid [zt_ref_low, zt_ref_high] (0.05, 0.90) and the mass range (required).
+ * max_samples bounds one device batch (the MOR table takes
+ * 4 n_zt_ref n_lnm n_lt doubles per sample); eval splits larger calls. */
+typedef struct {
+  int n_lt, n_zring, n_zouter, n_lnm, n_theta, n_zt_ref;
+  double zt_ref_low, zt_ref_high, lnm_low, lnm_high;
+  int n_gp;                              /* grid points (wall of numbers): */
+  const double *zo_low, *zo_high;        /*   z_obs bin edges              */
+  const int* lambda_bin;                 /*   richness bin 0..3            */
+  int max_samples;
+} y3b_bsel_config;
+
+/* One sample: cosmology and HMF / distances/{z, d_a} tables (the sci arrays
+ * are not read), distances/d_c [Mpc] on distances/z, haloModel/{lnM, z,
+ * bias [n_hz][n_hl]}, xi_nl/{r, z, xi_nl [n_xz][n_xr]} (r log-spaced and z
+ * evenly spaced, as the reference's lookup assumes) and the cluster_mor HOD
+ * parameters {log10_Mmin, log10_M1, alpha, epsilon, sigma_lambda, z_pivot}
+ * (z_pivot 0.45 when the section has none). */
+typedef struct {
+  y3b_cosmo cosmo;
+  y3b_tables t;
+  const double* dist_dc;
+  int n_hl, n_hz; const double *halo_lnM, *halo_z, *bias;
+  int n_xr, n_xz; const double *xi_r, *xi_z, *xi_nl;
+  double hod[6];
+} y3b_bsel_sample;
+
+typedef struct y3b_bsel y3b_bsel;
+/* setup(): GL nodes of lnM and of each richness bin's lambda_true range, the
+ * reference z grid, and each grid point's photo-z support (which depends on
+ * z_obs only). */
+int y3b_bsel_create(const y3b_bsel_config* cfg, y3b_bsel** out);
+/* set_sample() + evaluate() of every grid point for n_samples samples (all
+ * with the shapes of samples[0]) -> out[n_samples][n_gp][3] = (P1, I1, J).
+ * Host buffers; FP64 throughout.  Y3B_ERR_DOMAIN if the reference z grid
+ * leaves distances/z (the reference's Interp1D throws there). */
+int y3b_bsel_eval(y3b_bsel* h, int n_samples, const y3b_bsel_sample* samples, double* out);
+void y3b_bsel_destroy(y3b_bsel* h);
 
 /* ---------------------------------------------------------------------- */
 /* <Sigma_crit^-1>(z_l) (average_sigma_crit_inv.py:40-58), host buffers.   */

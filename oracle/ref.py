@@ -240,3 +240,64 @@ def shear_prj_frozen(cfg, cosmo, tables, prj, grid, data_root):
                                 C.byref(ps), _p(out), err, 512)
     _check(rc, err)
     return out
+
+
+class BselCfg(C.Structure):
+    _fields_ = [("n_lt", I), ("n_zring", I), ("n_zouter", I), ("n_lnm", I), ("n_theta", I),
+                ("n_zt_ref", I), ("zt_ref_low", D), ("zt_ref_high", D), ("lnm_low", D),
+                ("lnm_high", D), ("n_gp", I), ("zo_low", PD), ("zo_high", PD),
+                ("lambda_bin", PD)]
+
+
+class Hod(C.Structure):
+    _fields_ = [("log10_Mmin", D), ("log10_M1", D), ("alpha", D), ("epsilon", D),
+                ("sigma_lambda", D), ("z_pivot", D), ("has_z_pivot", I)]
+
+
+def bsel_marg(cfg, cosmo, tables, prj, hod, grid):
+    """P_operator (p_operator_t.hh), module label b_sel_marg: cfg dict
+    (lnm_low, lnm_high and optional n_lt, n_zring, n_zouter, n_lnm, n_theta,
+    n_zt_ref, zt_ref_low, zt_ref_high); hod dict (log10_Mmin, log10_M1, alpha,
+    epsilon, sigma_lambda, optional z_pivot); grid dict of the wall-grid
+    arrays zo_low, zo_high, lambda_bin; prj the tables of synthetic.prj_tables
+    (distances/d_c, haloModel bias, xi_nl).  Returns [n_gp, 3] = (P1, I1, J)."""
+    L = lib()
+    if not hasattr(L, "_bsel_declared"):
+        L.y3r_bsel_marg.argtypes = [C.POINTER(BselCfg), C.POINTER(Sample), C.POINTER(PrjSample),
+                                    C.POINTER(Hod), PD, C.c_char_p, I]
+        L._bsel_declared = True
+    keep = []
+
+    def arr(a):
+        a = _f64(a)
+        keep.append(a)
+        return a
+
+    c = BselCfg()
+    for k in ("n_lt", "n_zring", "n_zouter", "n_lnm", "n_theta", "n_zt_ref"):
+        setattr(c, k, int(cfg.get(k, 0)))
+    c.zt_ref_low = float(cfg.get("zt_ref_low", -1.0))
+    c.zt_ref_high = float(cfg.get("zt_ref_high", -1.0))
+    c.lnm_low, c.lnm_high = float(cfg["lnm_low"]), float(cfg["lnm_high"])
+    gp = {k: arr(grid[k]) for k in ("zo_low", "zo_high", "lambda_bin")}
+    c.n_gp = len(gp["zo_low"])
+    for k, v in gp.items():
+        setattr(c, k, _p(v))
+    inp = _Inputs(cosmo, tables, (np.array([0.0, 1.0]), np.array([0.0, 1.0]),
+                                  np.zeros((1, 2, 2))))
+    ps = PrjSample()
+    dc = arr(prj["dist_dc"])
+    ps.nd, ps.dist_dc = len(dc), _p(dc)
+    hl, hz, bi = arr(prj["halo_lnM"]), arr(prj["halo_z"]), arr(prj["bias"])
+    ps.n_hl, ps.n_hz, ps.halo_lnM, ps.halo_z, ps.bias = len(hl), len(hz), _p(hl), _p(hz), _p(bi)
+    xr, xz, xn = arr(prj["xi_r"]), arr(prj["xi_z"]), arr(prj["xi_nl"])
+    ps.n_xr, ps.n_xz, ps.xi_r, ps.xi_z, ps.xi_nl = len(xr), len(xz), _p(xr), _p(xz), _p(xn)
+    h = Hod(float(hod["log10_Mmin"]), float(hod["log10_M1"]), float(hod["alpha"]),
+            float(hod["epsilon"]), float(hod["sigma_lambda"]), float(hod.get("z_pivot", 0.0)),
+            int("z_pivot" in hod))
+    out = np.empty((c.n_gp, 3))
+    err = C.create_string_buffer(512)
+    rc = L.y3r_bsel_marg(C.byref(c), C.byref(inp.sample), C.byref(ps), C.byref(h), _p(out),
+                         err, 512)
+    _check(rc, err)
+    return out

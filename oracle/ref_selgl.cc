@@ -9,11 +9,13 @@
 // sel_function_t.hh:22-80; lensing_weights.hh:54-59,182-198) and calls
 // set_sample / evaluate the way the CosmoSIS scalar-evaluator module does
 // (CosmoSISScalarEvaluatorModule.hh:101-136): every grid point in order, bin
-// slow, R fast.
+// slow, R fast.  y3r_bsel_marg drives P_operator (src/models/p_operator_t.hh)
+// the same way over its (zo_low, zo_high, lambda_bin) wall grid.
 #include "ref_selgl.h"
 
 #include "models/n_operator_sel_gl_t.hh"
 #include "models/sigma_prj_frozen_t.hh"
+#include "models/p_operator_t.hh"
 
 #include <cstdio>
 #include <cstdlib>
@@ -259,6 +261,57 @@ y3r_shear_prj_frozen(const y3r_prj_cfg* c, const char* data_root, const y3r_samp
                                                          c->zo_high[i], c->radii[i]};
       auto const v = m.evaluate(pt);
       for (int k = 0; k != 9; ++k) out[(size_t)i * 9 + k] = v[k];
+    }
+    return 0;
+  }
+  catch (std::exception const& e) {
+    return fail(err, errlen, e.what());
+  }
+}
+
+int
+y3r_bsel_marg(const y3r_bsel_cfg* c, const y3r_sample* s, const y3r_prj_sample* ps,
+              const y3r_hod* hod, double* out, char* err, int errlen)
+{
+  try {
+    char const* label = y3_cluster::P_operator::module_label();
+    cosmosis::DataBlock cfg, b;
+    if (c->n_lt > 0) cfg.put_val(label, "n_lt", c->n_lt);
+    if (c->n_zring > 0) cfg.put_val(label, "n_zring", c->n_zring);
+    if (c->n_zouter > 0) cfg.put_val(label, "n_zouter", c->n_zouter);
+    if (c->n_lnm > 0) cfg.put_val(label, "n_lnm", c->n_lnm);
+    if (c->n_theta > 0) cfg.put_val(label, "n_theta", c->n_theta);
+    if (c->n_zt_ref > 0) cfg.put_val(label, "n_zt_ref", c->n_zt_ref);
+    if (c->zt_ref_low >= 0) cfg.put_val(label, "zt_ref_low", c->zt_ref_low);
+    if (c->zt_ref_high >= 0) cfg.put_val(label, "zt_ref_high", c->zt_ref_high);
+    cfg.put_val(label, "lnm_low", c->lnm_low);
+    cfg.put_val(label, "lnm_high", c->lnm_high);
+    put_sample(b, s);
+    b.put_val("distances", "d_c", vec(ps->dist_dc, ps->nd));
+    b.put_val("haloModel", "lnM", vec(ps->halo_lnM, ps->n_hl));
+    b.put_val("haloModel", "z", vec(ps->halo_z, ps->n_hz));
+    b.put_val("haloModel", "bias",
+              cosmosis::ndarray<double>(vec(ps->bias, ps->n_hl * ps->n_hz),
+                                        {static_cast<std::size_t>(ps->n_hz),
+                                         static_cast<std::size_t>(ps->n_hl)}));
+    b.put_val("xi_nl", "r", vec(ps->xi_r, ps->n_xr));
+    b.put_val("xi_nl", "z", vec(ps->xi_z, ps->n_xz));
+    b.put_val("xi_nl", "xi_nl",
+              cosmosis::ndarray<double>(vec(ps->xi_nl, ps->n_xr * ps->n_xz),
+                                        {static_cast<std::size_t>(ps->n_xz),
+                                         static_cast<std::size_t>(ps->n_xr)}));
+    b.put_val("cluster_mor", "log10_Mmin", hod->log10_Mmin);
+    b.put_val("cluster_mor", "log10_M1", hod->log10_M1);
+    b.put_val("cluster_mor", "alpha", hod->alpha);
+    b.put_val("cluster_mor", "epsilon", hod->epsilon);
+    b.put_val("cluster_mor", "sigma_lambda", hod->sigma_lambda);
+    if (hod->has_z_pivot) b.put_val("cluster_mor", "z_pivot", hod->z_pivot);
+    y3_cluster::P_operator m(cfg);
+    m.set_sample(b);
+    for (int i = 0; i != c->n_gp; ++i) {
+      y3_cluster::P_operator::grid_point_t pt{c->zo_low[i], c->zo_high[i], c->lambda_bin[i]};
+      auto const v = m.evaluate(pt);
+      for (int k = 0; k != 3; ++k) out[(size_t)i * 3 + k] = v[k];
     }
     return 0;
   }

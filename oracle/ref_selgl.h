@@ -98,6 +98,29 @@ int y3r_shear_prj_frozen(const y3r_prj_cfg* cfg, const char* data_root,
                          const y3r_sample* s, const y3r_prj_sample* ps, double* out,
                          char* err, int errlen);
 
+/* Options of the selection-bias operators (P_operator, module label
+ * b_sel_marg, src/models/p_operator_t.hh:76-110). */
+typedef struct {
+  int n_lt, n_zring, n_zouter, n_lnm, n_theta, n_zt_ref;  /* <= 0: unset (60, 20, 30, 24, 10, 80) */
+  double zt_ref_low, zt_ref_high;                         /* < 0: unset (0.05, 0.90) */
+  double lnm_low, lnm_high;
+  int n_gp;                                               /* wall grid: zo_low, zo_high, lambda_bin */
+  const double *zo_low, *zo_high, *lambda_bin;
+} y3r_bsel_cfg;
+
+/* cluster_mor HOD parameters (MOR_HOD_t(DataBlock&), mor_hod_t.hh:72-83);
+ * has_z_pivot = 0 leaves z_pivot unset (0.45). */
+typedef struct {
+  double log10_Mmin, log10_M1, alpha, epsilon, sigma_lambda, z_pivot;
+  int has_z_pivot;
+} y3r_hod;
+
+/* P_operator: set_sample, then evaluate every grid point -> out[n_gp][3]
+ * (P1, I1, J).  Reads distances/d_c, haloModel/{lnM, z, bias} and
+ * xi_nl/{r, z, xi_nl} from ps (its b_sel_marginalised arrays are unused). */
+int y3r_bsel_marg(const y3r_bsel_cfg* cfg, const y3r_sample* s, const y3r_prj_sample* ps,
+                  const y3r_hod* hod, double* out, char* err, int errlen);
+
 #ifdef __cplusplus
 }
 #endif

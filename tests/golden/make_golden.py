@@ -38,6 +38,11 @@ What it writes (tests/golden/*.npz / *.json):
   12 slices x 10 radii on the fiducial synthetic tables (counts' tables plus
   comoving distance, halo bias, xi_NL and the selection-bias asymptotes of
   synthetic.prj_tables), with a stand-in single-kernel miscentring table.
+* bsel_ref.npz -- P1, I1, J from the reference's compiled P_operator
+  (src/models/p_operator_t.hh, module b_sel_marg) on the same fiducial
+  tables with seeded HOD parameters: default node counts on 12 (z_obs bin,
+  richness bin) points, and reduced, odd node counts on 16 points for two
+  samples (the second with its own z_pivot, sigma_lambda and M1).
 * selgl_ref.npz -- numcountssel/vals, SelGLCore weights and
   shear1hmissel/vals (exact and idea2) from the reference's own C++
   (src/models/n_operator_sel_gl_t.hh:75-361), compiled from its sources by
@@ -439,6 +444,43 @@ def prj_reference(ref):
     return out
 
 
+BSEL_HOD = dict(log10_Mmin=11.7, log10_M1=12.9, alpha=0.85, epsilon=0.2, sigma_lambda=0.2)
+
+
+def bsel_reference(ref):
+    """Runs the reference's compiled P_operator (src/models/p_operator_t.hh,
+    module b_sel_marg) on the fiducial synthetic tables and HOD parameters:
+    default node counts on 12 (z_obs bin, richness bin) points, and reduced,
+    odd node counts (theta split 3 + 4) on 16 points that add a low-z_obs bin
+    and a second sample with its own z_pivot and sigma_lambda."""
+    from oracle import ref as R
+    from y3_cluster_cpp_b200 import synthetic
+
+    p = synthetic.fiducial()
+    prj = synthetic.prj_tables(p, n_r=120)
+    cosmo = dict(omega_m=p.om, omega_nu=0.0, omega_lambda=1.0 - p.om, omega_k=0.0, h0=p.h0,
+                 hmf_s=0.0, hmf_q=1.0)
+    grid = dict(zo_low=np.repeat([0.2, 0.35, 0.5], 4), zo_high=np.repeat([0.35, 0.5, 0.65], 4),
+                lambda_bin=np.tile(np.arange(4), 3).astype(float))
+    grid2 = dict(zo_low=np.repeat([0.1, 0.2, 0.35, 0.5], 4),
+                 zo_high=np.repeat([0.2, 0.35, 0.5, 0.65], 4),
+                 lambda_bin=np.tile(np.arange(4), 4).astype(float))
+    cfg = dict(lnm_low=np.log(1e13), lnm_high=np.log(10 ** 15.5))
+    cfg2 = dict(cfg, n_lt=24, n_zring=9, n_zouter=15, n_lnm=16, n_theta=7, n_zt_ref=40)
+    hod2 = dict(BSEL_HOD, z_pivot=0.3, sigma_lambda=0.3, log10_M1=13.1)
+    return dict(omega_m=p.om, h0=p.h0, **{"t_" + k: np.asarray(v) for k, v in p.tables.items()},
+                **{"prj_" + k: np.asarray(v) for k, v in prj.items()},
+                **{"gp_" + k: v for k, v in grid.items()},
+                **{"gp2_" + k: v for k, v in grid2.items()},
+                **{"cfg_" + k: v for k, v in cfg.items()},
+                **{"cfg2_" + k: v for k, v in cfg2.items()},
+                **{"hod_" + k: v for k, v in BSEL_HOD.items()},
+                **{"hod2_" + k: v for k, v in hod2.items()},
+                vals=R.bsel_marg(cfg, cosmo, p.tables, prj, BSEL_HOD, grid),
+                vals2=np.stack([R.bsel_marg(cfg2, cosmo, p.tables, prj, h, grid2)
+                                for h in (BSEL_HOD, hod2)]))
+
+
 class _OptionsIndex(dict):
     """options[section, key] and options.get_bool(section, key, default)."""
 
@@ -449,9 +491,19 @@ class _OptionsIndex(dict):
         return bool(self.get(key, default))
 
 
-def main(ref=None):
+def main(ref=None, *only):
+    """Writes every fixture, or with names after the checkout path (e.g.
+    `bsel_ref`) only those."""
     if ref is None:
-        raise SystemExit("usage: make_golden.py <reference-checkout>")
+        raise SystemExit("usage: make_golden.py <reference-checkout> [fixture ...]")
+    if only:
+        for name in only:
+            fn = {"bsel_ref": bsel_reference, "prj_ref": prj_reference,
+                  "selgl_ref": selgl_reference, "likelihood_ref": likelihood_reference,
+                  "sigma_crit_inv": sigma_crit_inv_reference}[name]
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), **fn(ref))
+        print("wrote", ", ".join(only), "to", HERE)
+        return
     _install_cosmosis_stub()
     with tempfile.TemporaryDirectory():
         lnm, z, S = run_sel_function(ref, lognormal=False)
@@ -472,6 +524,7 @@ def main(ref=None):
     np.savez_compressed(os.path.join(HERE, "selgl_ref.npz"), **selgl_reference(ref))
     np.savez_compressed(os.path.join(HERE, "likelihood_ref.npz"), **likelihood_reference(ref))
     np.savez_compressed(os.path.join(HERE, "prj_ref.npz"), **prj_reference(ref))
+    np.savez_compressed(os.path.join(HERE, "bsel_ref.npz"), **bsel_reference(ref))
     print("wrote golden fixtures to", HERE)
 
 

@@ -120,3 +120,21 @@ def test_prj_module_rejects_incomplete_options_on_cpu():
     o2 = DataBlock()
     o2[lab, "radii"] = np.array([0.5])
     assert not Module("ShearPrjFrozenPhysics").setup(o2)   # no box, no grid
+
+
+def test_bsel_module_rejects_incomplete_options_on_cpu():
+    """BSelMargIntegrand.so setup checks its options before any device work:
+    a missing mass range or mismatched grid arrays give NULL, never a throw."""
+    import numpy as np
+    from y3_cluster_cpp_b200.cosmosis import DataBlock, Module
+    lab = "b_sel_marg"
+    o = DataBlock()
+    o[lab, "zo_low"] = np.full(3, 0.2)
+    o[lab, "zo_high"] = np.full(2, 0.35)             # one short
+    o[lab, "lambda_bin"] = np.arange(3, dtype=np.int32)
+    o[lab, "lnm_low"], o[lab, "lnm_high"] = 29.9, 35.7
+    assert not Module("BSelMargIntegrand").setup(o)
+    o2 = DataBlock()
+    o2[lab, "zo_low"], o2[lab, "zo_high"] = np.full(3, 0.2), np.full(3, 0.35)
+    o2[lab, "lambda_bin"] = np.arange(3, dtype=np.int32)
+    assert not Module("BSelMargIntegrand").setup(o2)  # no mass range

@@ -164,3 +164,25 @@ def test_loglike_matches_reference_likelihood(form, space):
         v = O.loglike(g["thr_nc"][t], g["thr_s1h"][t], g["thr_prj"][t], log_space,
                       dn, icn, ds, ics)
         assert v == pytest.approx(ref[t], rel=1e-12, abs=1e-9)
+
+
+def test_bsel_golden_reproduced_by_compiled_reference():
+    """The selection-bias fixture (P_operator of p_operator_t.hh) comes back
+    bit for bit from the compiled reference library, where it is present."""
+    if not R.available():
+        pytest.skip("compiled reference library not present")
+    b = np.load(os.path.join(GOLD, "bsel_ref.npz"))
+
+    def sub(pre):
+        return {k[len(pre):]: (float(b[k]) if b[k].ndim == 0 else b[k]) for k in b.files
+                if k.startswith(pre)}
+
+    om, h0 = float(b["omega_m"]), float(b["h0"])
+    cosmo = dict(omega_m=om, omega_nu=0.0, omega_lambda=1.0 - om, omega_k=0.0, h0=h0,
+                 hmf_s=0.0, hmf_q=1.0)
+    t, prj = sub("t_"), sub("prj_")
+    out = R.bsel_marg(sub("cfg_"), cosmo, t, prj, sub("hod_"), sub("gp_"))
+    np.testing.assert_array_equal(out, b["vals"])
+    cfg2 = {k: (int(v) if k.startswith("n_") else v) for k, v in sub("cfg2_").items()}
+    out2 = R.bsel_marg(cfg2, cosmo, t, prj, sub("hod2_"), sub("gp2_"))
+    np.testing.assert_array_equal(out2, b["vals2"][1])

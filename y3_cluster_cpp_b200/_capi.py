@@ -130,6 +130,20 @@ class PrjSample(C.Structure):
                 ("b_small", PD), ("b_large", PD)]
 
 
+class BselConfig(C.Structure):
+    _fields_ = [("n_lt", I), ("n_zring", I), ("n_zouter", I), ("n_lnm", I), ("n_theta", I),
+                ("n_zt_ref", I), ("zt_ref_low", D), ("zt_ref_high", D), ("lnm_low", D),
+                ("lnm_high", D), ("n_gp", I), ("zo_low", PD), ("zo_high", PD),
+                ("lambda_bin", PI), ("max_samples", I)]
+
+
+class BselSample(C.Structure):
+    _fields_ = [("cosmo", Cosmo), ("t", Tables), ("dist_dc", PD),
+                ("n_hl", I), ("n_hz", I), ("halo_lnM", PD), ("halo_z", PD), ("bias", PD),
+                ("n_xr", I), ("n_xz", I), ("xi_r", PD), ("xi_z", PD), ("xi_nl", PD),
+                ("hod", D * 6)]
+
+
 class ServerStats(C.Structure):
     _fields_ = [("requests_done", C.c_longlong), ("points_done", C.c_longlong),
                 ("launches", C.c_longlong), ("max_launch_points", I), ("pool_points", I),
@@ -221,6 +235,10 @@ def _declare(L):
     L.y3b_prj_eval.argtypes = [VP, C.POINTER(PrjSample), PD]
     L.y3b_prj_destroy.argtypes = [VP]
     L.y3b_prj_destroy.restype = None
+    L.y3b_bsel_create.argtypes = [C.POINTER(BselConfig), C.POINTER(VP)]
+    L.y3b_bsel_eval.argtypes = [VP, I, C.POINTER(BselSample), PD]
+    L.y3b_bsel_destroy.argtypes = [VP]
+    L.y3b_bsel_destroy.restype = None
     L.y3b_engine_profile.argtypes = [VP, I]
     L.y3b_engine_profile_read.argtypes = [VP, PD, PI]
 
@@ -261,4 +279,5 @@ EXPORTED = [
     "y3b_planner_free_points", "y3b_engine_set_likelihood", "y3b_engine_loglike",
     "y3b_engine_eval_loglike", "y3b_gaussian_loglike", "y3b_prj_create",
     "y3b_prj_set_mis_table", "y3b_prj_eval", "y3b_prj_destroy",
+    "y3b_bsel_create", "y3b_bsel_eval", "y3b_bsel_destroy",
 ]

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <new>
@@ -85,6 +86,37 @@ class DevBuf {
   T* p_ = nullptr;
   size_t n_ = 0, cap_ = 0;
 };
+
+// Gauss-Legendre nodes and weights on [a, b] in FP64: Newton on P_n from the
+// Tricomi start cos(pi (i + 3/4) / (n + 1/2)) to |dz| <= 1e-14, nodes in
+// ascending order (p_operator_cuhre_t.hh:66-95, the grids of P_operator and
+// ShearPrjFrozenPhysics).
+inline void
+gl_nodes_host(double a, double b, int n, std::vector<double>& x, std::vector<double>& w)
+{
+  x.assign(n, 0.0);
+  w.assign(n, 0.0);
+  const double pi = 3.14159265358979323846;
+  const double mid = 0.5 * (a + b), hl = 0.5 * (b - a);
+  for (int i = 0; i < (n + 1) / 2; ++i) {
+    double z = std::cos(pi * (i + 0.75) / (n + 0.5)), z1, pp;
+    int guard = 0;
+    do {
+      double p1 = 1.0, p2 = 0.0;
+      for (int j = 0; j < n; ++j) {
+        double p3 = p2;
+        p2 = p1;
+        p1 = ((2.0 * j + 1.0) * z * p2 - j * p3) / (j + 1.0);
+      }
+      pp = n * (z * p1 - p2) / (z * z - 1.0);
+      z1 = z;
+      z = z1 - p1 / pp;
+    } while (std::fabs(z - z1) > 1e-14 && ++guard < 100);
+    x[i] = mid - hl * z;
+    x[n - 1 - i] = mid + hl * z;
+    w[i] = w[n - 1 - i] = 2.0 * hl / ((1.0 - z * z) * pp * pp);
+  }
+}
 
 // Device status word for kernel-side checks (domain errors, timeouts).
 int read_device_status(int* d_status, cudaStream_t s);

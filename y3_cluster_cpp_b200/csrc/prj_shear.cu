@@ -90,31 +90,11 @@ h_bilin_clamp(const double* xs, int nx, const double* ys, int ny, const double* 
          t * u * r1[1];
 }
 
-// Gauss-Legendre nodes on [a, b]: Newton on P_n from the Tricomi start, the
-// same recurrence as the device gl_nodes (p_operator_cuhre_t.hh:66-95).
+// Gauss-Legendre nodes on [a, b] (p_operator_cuhre_t.hh:66-95).
 void
 h_gl(double a, double b, int n, std::vector<double>& x, std::vector<double>& w)
 {
-  x.assign(n, 0.0);
-  w.assign(n, 0.0);
-  const double mid = 0.5 * (a + b), hl = 0.5 * (b - a);
-  for (int i = 0; i < (n + 1) / 2; ++i) {
-    double z = std::cos(kPiP * (i + 0.75) / (n + 0.5)), z1, pp;
-    do {
-      double p1 = 1.0, p2 = 0.0;
-      for (int j = 0; j < n; ++j) {
-        double p3 = p2;
-        p2 = p1;
-        p1 = ((2.0 * j + 1.0) * z * p2 - j * p3) / (j + 1.0);
-      }
-      pp = n * (z * p1 - p2) / (z * z - 1.0);
-      z1 = z;
-      z = z1 - p1 / pp;
-    } while (std::fabs(z - z1) > 1e-14);
-    x[i] = mid - hl * z;
-    x[n - 1 - i] = mid + hl * z;
-    w[i] = w[n - 1 - i] = 2.0 * hl / ((1.0 - z * z) * pp * pp);
-  }
+  gl_nodes_host(a, b, n, x, w);
 }
 
 double

@@ -241,6 +241,67 @@ class PrjShear:
         return out
 
 
+class BselMarg:
+    """Selection-bias operators P1, I1, J of P_operator (module b_sel_marg):
+    the wall grid (zo_low, zo_high, lambda_bin) and node counts are fixed at
+    construction; eval() takes a list of samples, each (cosmo, tables, prj,
+    hod) with tables as synthetic.make_tables, prj as synthetic.prj_tables
+    (distances/d_c, haloModel bias, xi_nl) and hod the cluster_mor
+    parameters (log10_Mmin, log10_M1, alpha, epsilon, sigma_lambda, optional
+    z_pivot), and returns [n_samples, n_gp, 3]."""
+
+    HOD_KEYS = ("log10_Mmin", "log10_M1", "alpha", "epsilon", "sigma_lambda")
+
+    def __init__(self, grid, lnm_low, lnm_high, n_lt=60, n_zring=20, n_zouter=30, n_lnm=24,
+                 n_theta=10, n_zt_ref=80, zt_ref_low=0.05, zt_ref_high=0.90, max_samples=64):
+        self._keep = [f64(grid["zo_low"]), f64(grid["zo_high"]),
+                      np.ascontiguousarray(np.asarray(grid["lambda_bin"], dtype=np.int32))]
+        c = A.BselConfig()
+        c.n_lt, c.n_zring, c.n_zouter, c.n_lnm = n_lt, n_zring, n_zouter, n_lnm
+        c.n_theta, c.n_zt_ref = n_theta, n_zt_ref
+        c.zt_ref_low, c.zt_ref_high, c.lnm_low, c.lnm_high = (zt_ref_low, zt_ref_high, lnm_low,
+                                                              lnm_high)
+        c.n_gp = len(self._keep[0])
+        c.zo_low, c.zo_high, c.lambda_bin = (ptr(a) for a in self._keep)
+        c.max_samples = max_samples
+        h = C.c_void_p()
+        check(lib().y3b_bsel_create(C.byref(c), C.byref(h)))
+        self._h = h
+        self.n_gp = c.n_gp
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().y3b_bsel_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def eval(self, samples):
+        n = len(samples)
+        arr = (A.BselSample * max(n, 1))()
+        keep = []
+        for k, (cz, tables, prj, hod) in enumerate(samples):
+            t = [f64(tables[x]) for x in ("hmf_m_h", "hmf_z", "dndlnmh", "dist_z", "dist_da")]
+            p = {x: f64(prj[x]) for x in ("dist_dc", "halo_lnM", "halo_z", "bias", "xi_r",
+                                          "xi_z", "xi_nl")}
+            keep += t + list(p.values())
+            s = arr[k]
+            s.cosmo = cz
+            s.t = A.Tables(len(t[0]), ptr(t[0]), len(t[1]), ptr(t[1]), ptr(t[2]), len(t[3]),
+                           ptr(t[3]), ptr(t[4]), 0, None, None)
+            s.dist_dc = ptr(p["dist_dc"])
+            s.n_hl, s.n_hz = len(p["halo_lnM"]), len(p["halo_z"])
+            s.halo_lnM, s.halo_z, s.bias = ptr(p["halo_lnM"]), ptr(p["halo_z"]), ptr(p["bias"])
+            s.n_xr, s.n_xz = len(p["xi_r"]), len(p["xi_z"])
+            s.xi_r, s.xi_z, s.xi_nl = ptr(p["xi_r"]), ptr(p["xi_z"]), ptr(p["xi_nl"])
+            for i, key in enumerate(self.HOD_KEYS):
+                s.hod[i] = float(hod[key])
+            s.hod[5] = float(hod.get("z_pivot", 0.45))
+        out = np.empty((n, self.n_gp, 3))
+        check(lib().y3b_bsel_eval(self._h, n, arr, ptr(out)))
+        return out
+
+
 def sigma_crit_inv(zl, zs, pz, delta_z, h0, dist_z, dist_da):
     zl, zs, pz, dz, da = map(f64, (zl, zs, pz, dist_z, dist_da))
     out = np.empty(len(zl))
