@@ -307,6 +307,9 @@ int y3b_bsel_create(const y3b_bsel_config* cfg, y3b_bsel** out);
  * Host buffers; FP64 throughout.  Y3B_ERR_DOMAIN if the reference z grid
  * leaves distances/z (the reference's Interp1D throws there). */
 int y3b_bsel_eval(y3b_bsel* h, int n_samples, const y3b_bsel_sample* samples, double* out);
+/* Device time of the last y3b_bsel_eval's kernels (CUDA events around each
+ * chunk's two kernels, summed; the copies and host packing excluded). */
+int y3b_bsel_kernel_ms(const y3b_bsel* h, double* ms);
 void y3b_bsel_destroy(y3b_bsel* h);
 
 /* ---------------------------------------------------------------------- */

@@ -237,6 +237,7 @@ def _declare(L):
     L.y3b_prj_destroy.restype = None
     L.y3b_bsel_create.argtypes = [C.POINTER(BselConfig), C.POINTER(VP)]
     L.y3b_bsel_eval.argtypes = [VP, I, C.POINTER(BselSample), PD]
+    L.y3b_bsel_kernel_ms.argtypes = [VP, PD]
     L.y3b_bsel_destroy.argtypes = [VP]
     L.y3b_bsel_destroy.restype = None
     L.y3b_engine_profile.argtypes = [VP, I]
@@ -279,5 +280,5 @@ EXPORTED = [
     "y3b_planner_free_points", "y3b_engine_set_likelihood", "y3b_engine_loglike",
     "y3b_engine_eval_loglike", "y3b_gaussian_loglike", "y3b_prj_create",
     "y3b_prj_set_mis_table", "y3b_prj_eval", "y3b_prj_destroy",
-    "y3b_bsel_create", "y3b_bsel_eval", "y3b_bsel_destroy",
+    "y3b_bsel_create", "y3b_bsel_eval", "y3b_bsel_kernel_ms", "y3b_bsel_destroy",
 ]

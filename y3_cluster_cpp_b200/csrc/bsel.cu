@@ -487,8 +487,12 @@ struct y3b_bsel {
   double* h_out = nullptr;  // pinned: results
   size_t h_out_cap = 0;
   cudaStream_t stream = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};  // around each chunk's kernels
+  double last_kernel_ms = 0.0;
   ~y3b_bsel()
   {
+    for (cudaEvent_t e : ev)
+      if (e) cudaEventDestroy(e);
     if (h_stage) cudaFreeHost(h_stage);
     if (h_out) cudaFreeHost(h_out);
     if (stream) cudaStreamDestroy(stream);
@@ -670,6 +674,8 @@ y3b_bsel_create(const y3b_bsel_config* cfg, y3b_bsel** out)
                        "cudaStreamCreate");
   std::vector<int> ints(h->gp_bin);
   ints.push_back(0);
+  for (int i = 0; i < 2 && !rc; ++i)
+    rc = cuda_status(cudaEventCreate(&h->ev[i]), "cudaEventCreate");
   if (!rc) rc = h->d_const.upload(cst.data(), cst.size(), h->stream);
   if (!rc) rc = h->d_int.upload(ints.data(), ints.size(), h->stream);
   if (!rc) rc = cuda_status(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
@@ -678,6 +684,18 @@ y3b_bsel_create(const y3b_bsel_config* cfg, y3b_bsel** out)
     return rc;
   }
   *out = h;
+  return Y3B_OK;
+}
+
+extern "C" int
+y3b_bsel_kernel_ms(const y3b_bsel* h, double* ms)
+{
+  y3b::clear_error();
+  if (!h || !ms) {
+    y3b::set_error("y3b_bsel_kernel_ms: invalid arguments");
+    return Y3B_ERR_INVALID;
+  }
+  *ms = h->last_kernel_ms;
   return Y3B_OK;
 }
 
@@ -766,6 +784,7 @@ y3b_bsel_eval(y3b_bsel* h, int n_samples, const y3b_bsel_sample* S, double* out)
   Y3B_TRY(h->d_out.alloc(outn));
   cudaStream_t st = h->stream;
   Y3B_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), st));
+  h->last_kernel_ms = 0.0;
   for (int k0 = 0; k0 < n_samples; k0 += chunk) {
     const int nk = std::min(chunk, n_samples - k0);
     // The previous chunk's copies out of the staging buffers are done.
@@ -793,6 +812,7 @@ y3b_bsel_eval(y3b_bsel* h, int n_samples, const y3b_bsel_sample* S, double* out)
     }
     Y3B_CUDA(cudaMemcpyAsync(h->d_blocks.get(), h->h_stage, sizeof(double) * nk * D.blk,
                              cudaMemcpyHostToDevice, st));
+    Y3B_CUDA(cudaEventRecord(h->ev[0], st));
     bsel_sample_kernel<<<dim3(D.n_zr, nk), kSampleThreads, 3 * sizeof(double) * c.n_lnm, st>>>(
       D, h->d_blocks.get(), h->d_work.get(), d_status);
     count_launch();
@@ -801,9 +821,13 @@ y3b_bsel_eval(y3b_bsel* h, int n_samples, const y3b_bsel_sample* S, double* out)
                                                                  h->d_work.get(), h->d_out.get());
     count_launch();
     Y3B_CUDA(cudaGetLastError());
+    Y3B_CUDA(cudaEventRecord(h->ev[1], st));
     Y3B_CUDA(cudaMemcpyAsync(h->h_out, h->d_out.get(), sizeof(double) * nk * ngp * 3,
                              cudaMemcpyDeviceToHost, st));
     Y3B_CUDA(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    Y3B_CUDA(cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]));
+    h->last_kernel_ms += ms;
     std::memcpy(out + (size_t)k0 * ngp * 3, h->h_out, sizeof(double) * nk * ngp * 3);
   }
   return read_device_status(d_status, st);

@@ -301,6 +301,12 @@ class BselMarg:
         check(lib().y3b_bsel_eval(self._h, n, arr, ptr(out)))
         return out
 
+    def kernel_ms(self):
+        """Device time of the last eval's kernels (copies and packing excluded)."""
+        ms = C.c_double()
+        check(lib().y3b_bsel_kernel_ms(self._h, C.byref(ms)))
+        return ms.value
+
 
 def sigma_crit_inv(zl, zs, pz, delta_z, h0, dist_z, dist_da):
     zl, zs, pz, dz, da = map(f64, (zl, zs, pz, dist_z, dist_da))
