@@ -21,11 +21,13 @@
 // One launch covers the points of every grid: a planner kernel orders the
 // points by the cost of their grid's tiles and a persistent CTA per SM walks
 // the (point, 128-row lnM tile, richness-bin group) tiles in that order:
-// warps 1-8 generate F and warps 9-16 generate the other operand into an
-// 8-stage shared-memory ring, warp 0 issues the MMAs into one of two TMEM
-// accumulators, warps 17-24 drain the other; full/empty mbarriers (empty
-// signalled by tcgen05.commit) order the ring and the accumulators, and every
-// wait is bounded.
+// warps 1-16 generate the operand u_t K_i G(t, q) into a shared-memory ring
+// of up to 8 stages (filled two stages at a time), warp 26 streams the
+// matching F(t, k) blocks (written by the prep kernels) by bulk copies, one
+// per pair of stages, warp 0 issues the MMAs of a pair of stages into one of
+// two TMEM accumulators, warps 17-24 drain the other; full/empty mbarriers
+// (empty signalled by tcgen05.commit) order the rings and the accumulators,
+// and every wait is bounded.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -172,11 +174,11 @@ constexpr int kProdWarps = kAWarps;
 constexpr int kEpiWarp0 = 17;      // warps 17..24 drain TMEM (warp w reads lanes 32 (w % 4)..)
 constexpr int kEpiWarps = 8;
 constexpr int kLoadWarp = 25;      // stages the next tile's factor vectors in shared memory
-constexpr int kFLoadWarp = 26;     // copies every stage's F(t, k) block (prep kernel output)
+constexpr int kFLoadWarp = 26;     // copies the F(t, k) blocks of each pair of stages (prep kernel output)
 constexpr int kThreads = 32 * 27;  // 864
 constexpr int kStageK = 16;        // lam_t nodes per pipeline stage (one MMA k-step)
 constexpr int kMaxStages = 8;      // depth of the A ring (tuned), at most 8
-constexpr int kMaxFStages = 16;    // depth of the F ring: what shared memory leaves, at most 16
+constexpr int kMaxFStages = 16;    // F ring in stages (even: slots of two): what shared memory leaves
 constexpr int kAccCols = 256;      // TMEM columns per accumulator buffer (2 buffers)
 constexpr uint32_t kFPlane = kGemmRows * kStageK * 2;        // one bf16 plane of F: 4 KB
 constexpr uint32_t kAPlane = kAccCols * kStageK * 2;         // one bf16 plane of A: 8 KB
@@ -462,6 +464,7 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int n_tiles = __ldg(tile_start + n_points);
   const int nst = n_stages, nfs = n_fstages;
+  const int nfp = nfs / 2;  // F ring slots: one pair of stages (16 KB) each
   uint8_t* fring = smem + nst * kStageBytes;                          // [nfs][8 KB]
   float* Ys = reinterpret_cast<float*>(fring + nfs * kFStageBytes);  // [n_z][128]
   float* CN_s = Ys + (size_t)nz_max * kGemmRows;
@@ -495,7 +498,7 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
       mbar_init(smem_u32(&full[i]), kProdWarps);
       mbar_init(smem_u32(&empty[i]), 1);
     }
-    for (int i = 0; i < nfs; ++i) {
+    for (int i = 0; i < nfp; ++i) {
       mbar_init(smem_u32(&fbar[i]), 1);
       mbar_init(smem_u32(&fempty[i]), 1);
     }
@@ -532,25 +535,37 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
         const uint32_t idesc = umma_idesc_bf16(kGemmRows, ncp);
         const uint32_t lboA = (uint32_t)ncp * 16u;
         bool broke = false;
-        for (int kc = T.kc_lo; kc < T.kc_hi; ++kc, rp.next(nst), rf.next(nfs)) {
-          const int s = rp.s, f = rf.s;
-          if (!mbar_poll_or_abort(smem_u32(&full[s]), rp.ph, abort_s) ||
+        // Stages in pairs (a window's count is even), as the producers fill
+        // them: one wait on the pair's second full barrier (each producer
+        // warp arrives on the first before the second) and one on its F
+        // block pair, six MMAs, and one commit per ring slot.
+        for (int kc = T.kc_lo; kc < T.kc_hi; kc += 2, rf.next(nfp)) {
+          const int s0 = rp.s;
+          rp.next(nst);
+          const int s1 = rp.s;
+          const uint32_t ph1 = rp.ph;
+          rp.next(nst);
+          const int f = rf.s;
+          if (!mbar_poll_or_abort(smem_u32(&full[s1]), ph1, abort_s) ||
               !mbar_poll_or_abort(smem_u32(&fbar[f]), rf.ph, abort_s)) {
             broke = true;
             break;
           }
           tc_fence_after();
-          const uint32_t fh = smem_u32(fring + f * kFStageBytes), fl = fh + kFPlane;
-          const uint32_t ah = smem_u32(smem + s * kStageBytes), al = ah + kAPlane;
-          const uint64_t dfh = umma_desc(fh, kLboF, 128), dfl = umma_desc(fl, kLboF, 128);
-          const uint64_t dah = umma_desc(ah, lboA, 128), dal = umma_desc(al, lboA, 128);
-          umma_bf16(dacc, dfh, dah, idesc, kc != T.kc_lo);
-          umma_bf16(dacc, dfh, dal, idesc, 1u);
-          umma_bf16(dacc, dfl, dah, idesc, 1u);
-          umma_commit(smem_u32(&empty[s]));
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const uint32_t fh = smem_u32(fring + (2 * f + h) * kFStageBytes), fl = fh + kFPlane;
+            const uint32_t ah = smem_u32(smem + (h ? s1 : s0) * kStageBytes), al = ah + kAPlane;
+            const uint64_t dfh = umma_desc(fh, kLboF, 128), dfl = umma_desc(fl, kLboF, 128);
+            const uint64_t dah = umma_desc(ah, lboA, 128), dal = umma_desc(al, lboA, 128);
+            umma_bf16(dacc, dfh, dah, idesc, (kc + h) != T.kc_lo);
+            umma_bf16(dacc, dfh, dal, idesc, 1u);
+            umma_bf16(dacc, dfl, dah, idesc, 1u);
+            umma_commit(smem_u32(&empty[h ? s1 : s0]));
+          }
           umma_commit(smem_u32(&fempty[f]));
-          last_stage = s;
-          last_parity = (int)rp.ph;
+          last_stage = s1;
+          last_parity = (int)ph1;
         }
         if (broke) break;
         umma_commit(smem_u32(&acc_full[buf]));  // tile j's accumulator is complete
@@ -705,11 +720,11 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
     }
     __syncwarp();
   } else if (warp == kFLoadWarp) {
-    // ---------------- F(t, k) blocks, one bulk copy per stage ----------------
+    // ---------------- F(t, k) blocks, one bulk copy per pair of stages ----------------
     if (lane == 0) {
       RingPos rp;
       int chunk = 0;
-      uint32_t issued = 0, last_ph = 0;  // per stage: copy issued, parity of its last use
+      uint32_t issued = 0, last_ph = 0;  // per slot: copy issued, parity of its last use
       for (int t = blockIdx.x; t < n_tiles && !*abort_s; t += gridDim.x) {
         const Tile T = decode_tile(t, tile_list, win_tile, win_stride, pts, grids);
         const int nk = T.G->n_t_pad / kStageK;
@@ -721,32 +736,33 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
           const int nkn = Tn.G->n_t_pad / kStageK;
           const uint8_t* nsrc =
             fbuf + (size_t)Tn.p * f_stride + (size_t)Tn.mtile * nkn * kFStageBytes;
-          for (int kc = Tn.kc_lo; kc < Tn.kc_hi; ++kc)
+          for (int kc = Tn.kc_lo; kc < Tn.kc_hi; kc += 2)
             asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(
                            nsrc + (size_t)kc * kFStageBytes),
-                         "r"((uint32_t)kFStageBytes)
+                         "r"((uint32_t)(2 * kFStageBytes))
                          : "memory");
         }
         bool broke = false;
-        for (int kc = T.kc_lo; kc < T.kc_hi; ++kc, ++chunk, rp.next(nfs)) {
+        for (int kc = T.kc_lo; kc < T.kc_hi; kc += 2, ++chunk, rp.next(nfp)) {
           const int s = rp.s;
-          if (chunk >= nfs && !mbar_poll_or_abort(smem_u32(&fempty[s]), rp.ph ^ 1u, abort_s)) {
+          if (chunk >= nfp && !mbar_poll_or_abort(smem_u32(&fempty[s]), rp.ph ^ 1u, abort_s)) {
             broke = true;
             break;
           }
           const uint32_t fb = smem_u32(&fbar[s]);
           asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb),
-                       "r"((uint32_t)kFStageBytes)
+                       "r"((uint32_t)(2 * kFStageBytes))
                        : "memory");
-          bulk_g2s(fring + s * kFStageBytes, src + (size_t)kc * kFStageBytes, kFStageBytes, fb);
+          bulk_g2s(fring + 2 * s * kFStageBytes, src + (size_t)kc * kFStageBytes,
+                   2 * kFStageBytes, fb);
           issued |= 1u << s;
           last_ph = (last_ph & ~(1u << s)) | (rp.ph << s);
         }
         if (broke) break;
       }
       // No copy may still be in flight when the CTA's shared memory is
-      // released: wait for the last one issued into every stage (bounded).
-      for (int s = 0; s < nfs; ++s) {
+      // released: wait for the last one issued into every slot (bounded).
+      for (int s = 0; s < nfp; ++s) {
         if (!((issued >> s) & 1u)) continue;
         long long t0 = clock64();
         while (!mbar_try_wait(smem_u32(&fbar[s]), (last_ph >> s) & 1u) &&
@@ -873,13 +889,13 @@ contract_smem_base(int stages, const ContractShape& c)
   return b + 8 * (2 * kMaxStages + 2 * kMaxFStages + 9) + 16;
 }
 
-// F ring depth that fits next to `stages` A stages (<= 16).
+// F ring depth in stages that fits next to `stages` A stages (even, <= 16).
 int
 contract_fstages(int stages, const ContractShape& c)
 {
   const size_t base = contract_smem_base(stages, c), cap = 227 * 1024;
   if (base >= cap) return 0;
-  return (int)std::min<size_t>(kMaxFStages, (cap - base) / kFStageBytes);
+  return (int)std::min<size_t>(kMaxFStages, (cap - base) / kFStageBytes) & ~1;
 }
 
 static size_t
