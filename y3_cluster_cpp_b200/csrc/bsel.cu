@@ -26,7 +26,7 @@
 //
 // Device layout: one packed FP64 block per sample (scalars and tables);
 // one kernel per (reference z node, sample) writes the per-sample tables and
-// the MOR table of the richness bins in use; one 256-thread CTA per
+// the MOR table of the richness bins in use; one 512-thread CTA per
 // (grid point, sample) builds its grids in shared memory and does the sums.
 // Every sum runs in the reference's order (mass, lambda_true, z, theta), and
 // this file is compiled without FMA contraction, so the results follow the
@@ -51,7 +51,7 @@ lob_centre(int b)
 {
   return b == 0 ? 25.0 : (b == 1 ? 37.5 : (b == 2 ? 52.5 : 130.0));
 }
-constexpr int kPointThreads = 256;
+constexpr int kPointThreads = 512;
 constexpr int kSampleThreads = 128;
 constexpr int kScal = 16;  // scalars at the head of a sample block
 
@@ -168,7 +168,7 @@ point_smem_doubles(const BselDims& D)
 {
   const long NZ = D.nz_max;
   return 9 * NZ + 4L * D.n_zouter + 5L * D.n_th + D.n_xr + 2L * D.n_lt * NZ +
-         3L * D.n_th * NZ + kScal + 8 + (NZ + 1) / 2;
+         3L * D.n_th * NZ + kScal + 16 + (NZ + 1) / 2;
 }
 
 // Lower bracket of z on the reference grid: i = min(trunc(u), n - 2) with
@@ -186,7 +186,7 @@ ref_bracket(const BselDims& D, double z, double* f)
 
 // One CTA per (grid point, sample): P_operator::evaluate
 // (p_operator_t.hh:222-477) with its grids in shared memory.
-__global__ void __launch_bounds__(kPointThreads)
+__global__ void __launch_bounds__(kPointThreads, 2)
 bsel_point_kernel(BselDims D, const double* __restrict__ blocks,
                   const double* __restrict__ work, double* __restrict__ out)
 {
@@ -221,7 +221,7 @@ bsel_point_kernel(BselDims D, const double* __restrict__ blocks,
   double* pI = pP + (size_t)NT * NZ;
   double* pJ = pI + (size_t)NT * NZ;
   double* sc = pJ + (size_t)NT * NZ;
-  int* izl = reinterpret_cast<int*>(sc + kScal + 8);
+  int* izl = reinterpret_cast<int*>(sc + kScal + 16);  // after 8 doubles of counts and 5 chi(z)
   // scalars: 0 zob, 1 chi_o, 2 theta_lob, 3 R_excl, 4 ln R_excl, 5 ln(chi_o - chi_fg),
   // 6 ln(chi_bg - chi_o), 7 ring lo, 8 ring hi, 9 th_lo, 10 th_hi, 11 th_mid,
   // 12 ln r_0, 13 1 / dln r, 14 k_sig, 15 th0_sig; ints after: n_fg, n_ring, n_bg, split, empty
@@ -229,16 +229,23 @@ bsel_point_kernel(BselDims D, const double* __restrict__ blocks,
   const int bin = D.gp_bin[g];
   const double ddz = 1.0e-3;
 
+  if (tid < 5) {  // the five chi(z) this point needs, one lookup per thread
+    const double zob = D.gp_zob[g];
+    const double zq[5] = {zob, D.gp_zfg[g], D.gp_zbg[g], zob + ddz, zob - ddz};
+    sc[kScal + 8 + tid] = chi_at(D, B, zq[tid]);
+  }
+  __syncthreads();
   if (tid == 0) {
     const double zob = D.gp_zob[g];
     const double Rlob = pow(lob_centre(bin) / 100.0, 0.2);  // p_op_detail::R_lambda
-    const double chi_o = chi_at(D, B, zob);
+    const double* cq = sc + kScal + 8;
+    const double chi_o = cq[0];
     const double theta_lob = Rlob * (1.0 + zob) / chi_o;
     const double R_excl = Rlob * (1.0 + zob);
     // build_z_grid_ (p_operator_t.hh:503-583)
     const double zfg = D.gp_zfg[g], zbg = D.gp_zbg[g];
-    const double chi_fg = chi_at(D, B, zfg), chi_bg = chi_at(D, B, zbg);
-    const double dchi_dz = (chi_at(D, B, zob + ddz) - chi_at(D, B, zob - ddz)) / (2.0 * ddz);
+    const double chi_fg = cq[1], chi_bg = cq[2];
+    const double dchi_dz = (cq[3] - cq[4]) / (2.0 * ddz);
     const double dz_excl = R_excl / dchi_dz;
     const double zr_lo = fmax(zob - dz_excl, zfg), zr_hi = fmin(zob + dz_excl, zbg);
     const double dfg = chi_o - chi_fg, dbg = chi_bg - chi_o;
