@@ -294,9 +294,14 @@ struct NfwUnit<double> {
     }
     return 2.0 * (g(x) + log(0.5 * x)) / (x * x);
   }
+  // sigma_bar(x) - sigma(x) with g(x) evaluated once where both need it
+  // (x >= 0.5 away from x = 1): the same values as the two calls.
   static __device__ __forceinline__ double dsigma(double x)
   {
-    return sigma_bar(x) - sigma(x);
+    const double w = 1.0 - x * x;
+    if (x < 0.5 || fabs(w) < 0.1) return sigma_bar(x) - sigma(x);
+    const double gx = g(x);
+    return 2.0 * (gx + log(0.5 * x)) / (x * x) - (gx - 1.0) / w;
   }
 };
 
@@ -343,7 +348,10 @@ struct NfwUnit<float> {
   }
   static __device__ __forceinline__ float dsigma(float x)
   {
-    return sigma_bar(x) - sigma(x);
+    const float w = 1.0f - x * x;
+    if (x < 0.5f || fabsf(w) < 0.05f) return sigma_bar(x) - sigma(x);
+    const float gx = g(x);
+    return 2.0f * (gx + logf(0.5f * x)) / (x * x) - (gx - 1.0f) / w;
   }
 };
 
@@ -353,7 +361,20 @@ struct NfwUnit<float> {
 // centre, (1/pi) int_0^pi dth DSigma(d) (2 a^2 / d^2 - 1) with
 // d^2 = x^2 + x_mis^2 - 2 x x_mis cos th, a = x - x_mis cos th.  Returns the
 // sum over the GL nodes t0, t0 + dt, ... of [0, pi] (without the 1/pi), so
-// a warp can split the nodes.
+// a warp can split the nodes.  The _cos form takes cos(theta) of the nodes.
+__device__ __forceinline__ double
+dsigma_single_partial_cos(const double* cth, const double* wth, int n, double x, double xm,
+                          int t0, int dt)
+{
+  double acc = 0.0;
+  for (int t = t0; t < n; t += dt) {
+    const double ct = cth[t];
+    const double d2 = x * x + xm * xm - 2.0 * x * xm * ct, a = x - xm * ct;
+    acc += wth[t] * NfwUnit<double>::dsigma(sqrt(d2)) * (2.0 * a * a / d2 - 1.0);
+  }
+  return acc;
+}
+
 __device__ __forceinline__ double
 dsigma_single_partial(const double* th, const double* wth, int n, double x, double xm, int t0,
                       int dt)

@@ -123,7 +123,7 @@ struct PrjTables {
   int n_lx, n_lxm;
   const double *lx, *lxm, *ltab; // single-kernel table (n_lx = 0: quadrature)
   int n_th;
-  const double *th, *wth;        // GL on [0, pi] for the quadrature
+  const double *th, *wth;        // cos(theta) and weights of the GL nodes on [0, pi]
   double omega_m;
 };
 
@@ -145,7 +145,7 @@ dsigma_single(const PrjTables& T, double R, double Rmis, double lnM)
   if (T.n_lx) {
     unit = exp(interp2d_clamp(T.lx, T.n_lx, T.lxm, T.n_lxm, T.ltab, log(x), log(xm)));
   } else {  // mean tangential shear on the circle x around the offset centre
-    unit = dsigma_single_partial(T.th, T.wth, T.n_th, x, xm, 0, 1) / kPiP;
+    unit = dsigma_single_partial_cos(T.th, T.wth, T.n_th, x, xm, 0, 1) / kPiP;
   }
   return nfw_norm(lnM, kConc, kRhoCrit) * T.omega_m * unit;
 }
@@ -204,22 +204,38 @@ prj_psi_kernel(PrjTables T, int n_theta_tot, const int* tslice, const double* th
   psi[i] = acc;
 }
 
-// One block per grid point: the (theta, M) sums of both channels.
+// The single-kernel profile DSigma_mis(R | theta D_A, M) of every (grid
+// point, theta node of its slice, mass node): one thread each, written to
+// V[g][(it - t0) n_lnm + iM] (max_pairs per grid point).
 __global__ void __launch_bounds__(256)
-prj_eval_kernel(PrjTables T, int n_lnm, const double* lnm_x, const int* gp_slice,
-                const double* gp_R, const int* t0, const double* theta, const double* geom,
+prj_profile_kernel(PrjTables T, int n_lnm, const double* lnm_x, const int* gp_slice,
+                   const double* gp_R, const int* t0, const double* theta, const double* DA,
+                   int max_pairs, double* V)
+{
+  const int g = blockIdx.y, sl = gp_slice[g];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n_pairs = (t0[sl + 1] - t0[sl]) * n_lnm;
+  if (k >= n_pairs) return;
+  const int it = t0[sl] + k / n_lnm, iM = k % n_lnm;
+  V[(size_t)g * max_pairs + k] = dsigma_single(T, gp_R[g], theta[it] * DA[sl], lnm_x[iM]);
+}
+
+// One block per grid point: the (theta, M) sums of both channels over the
+// profile values of prj_profile_kernel.
+__global__ void __launch_bounds__(256)
+prj_eval_kernel(int n_lnm, const int* gp_slice, const int* t0, const double* geom,
                 const double* bsel, const double* psi, const double* wrnd, const double* wcl,
-                const double* DA, const double* sci, double* out)
+                const double* sci, int max_pairs, const double* V, double* out)
 {
   __shared__ double red[256];
   const int g = blockIdx.x, sl = gp_slice[g];
-  const double R = gp_R[g], da = DA[sl];
+  const double* Vg = V + (size_t)g * max_pairs;
   double rnd = 0.0, cl = 0.0;
   for (int it = t0[sl] + threadIdx.x; it < t0[sl + 1]; it += blockDim.x) {
-    const double Rmis = theta[it] * da;
+    const double* v_it = Vg + (size_t)(it - t0[sl]) * n_lnm;
     double ar = 0.0, ac = 0.0;
     for (int iM = 0; iM < n_lnm; ++iM) {
-      const double v = dsigma_single(T, R, Rmis, lnm_x[iM]);
+      const double v = v_it[iM];
       ar += wrnd[(size_t)sl * n_lnm + iM] * v;
       ac += wcl[(size_t)sl * n_lnm + iM] * v;
     }
@@ -241,6 +257,15 @@ prj_eval_kernel(PrjTables T, int n_lnm, const double* lnm_x, const int* gp_slice
 }
 
 }  // namespace
+
+// Device buffers of one evaluation, kept by the handle and grown on demand.
+struct PrjBufs {
+  DevBuf<double> d_mh, d_hz, d_dn, d_bl, d_bz, d_bi, d_xr, d_xz, d_xi, d_lx, d_lxm, d_lt, d_th,
+    d_wth, d_lnx, d_lnw, d_theta, d_geom, d_bsel, d_zz, d_zc, d_chiz, d_thex, d_anchor, d_denom,
+    d_wcl, d_AB, d_WZ, d_wrnd, d_psi, d_chio, d_zob, d_da, d_sci, d_gpR, d_out, d_V;
+  DevBuf<int> d_t0, d_z0, d_ts, d_zs, d_gps;
+};
+
 }  // namespace y3b
 
 struct y3b_prj {
@@ -254,6 +279,7 @@ struct y3b_prj {
   std::vector<std::vector<double>> sl_Rs;    // distinct radii, first-appearance order
   std::vector<double> lnm_x, lnm_w;
   std::vector<double> tab_lx, tab_lxm, tab_v;
+  y3b::PrjBufs bufs;
   cudaStream_t stream = nullptr;
   ~y3b_prj()
   {
@@ -266,11 +292,12 @@ y3b_prj_create(const y3b_prj_config* cfg, y3b_prj** out)
 {
   using namespace y3b;
   clear_error();
-  if (!cfg || !out || cfg->n_gp < 1 || !cfg->lambda_bin || !cfg->zo_low || !cfg->zo_high ||
+  if (!cfg || !out || cfg->n_gp < 1 || cfg->n_gp > 65535 || !cfg->lambda_bin || !cfg->zo_low ||
+      !cfg->zo_high ||
       !cfg->radii || cfg->n_lnm < 1 || cfg->n_per_seg < 1 || cfg->n_zring < 1 ||
       cfg->n_zouter < 1 || !(cfg->zt_high > cfg->zt_low) || !(cfg->lnm_high > cfg->lnm_low)) {
-    set_error("y3b_prj_create: invalid configuration (grid points, node counts >= 1, ordered "
-              "bounds)");
+    set_error("y3b_prj_create: invalid configuration (1..65535 grid points, node counts >= 1, "
+              "ordered bounds)");
     return Y3B_ERR_INVALID;
   }
   *out = nullptr;
@@ -535,90 +562,96 @@ y3b_prj_eval(y3b_prj* h, const y3b_prj_sample* S, double* out)
   }
   // Device buffers.
   cudaStream_t s = h->stream;
-  DevBuf<double> d_mh, d_hz, d_dn, d_bl, d_bz, d_bi, d_xr, d_xz, d_xi, d_lx, d_lxm, d_lt, d_th,
-    d_wth, d_lnx, d_lnw, d_theta, d_geom, d_bsel, d_zz, d_zc, d_chiz, d_thex, d_anchor, d_denom,
-    d_wcl, d_AB, d_WZ, d_wrnd, d_psi, d_chio, d_zob, d_da, d_sci, d_gpR, d_out;
-  DevBuf<int> d_t0, d_z0, d_ts, d_zs, d_gps;
-  Y3B_TRY(d_mh.upload(mh.data(), mh.size(), s));
-  Y3B_TRY(d_hz.upload(t.hmf_z, t.n_hz, s));
-  Y3B_TRY(d_dn.upload(t.dndlnmh, (size_t)t.n_hz * t.n_hm, s));
-  Y3B_TRY(d_bl.upload(S->halo_lnM, S->n_hl, s));
-  Y3B_TRY(d_bz.upload(S->halo_z, S->n_hz, s));
-  Y3B_TRY(d_bi.upload(S->bias, (size_t)S->n_hl * S->n_hz, s));
-  Y3B_TRY(d_xr.upload(S->xi_r, S->n_xr, s));
-  Y3B_TRY(d_xz.upload(S->xi_z, S->n_xz, s));
-  Y3B_TRY(d_xi.upload(S->xi_nl, (size_t)S->n_xr * S->n_xz, s));
+  y3b::PrjBufs& B = h->bufs;  // kept by the handle: no device allocation after the first call
+  Y3B_TRY(B.d_mh.upload(mh.data(), mh.size(), s));
+  Y3B_TRY(B.d_hz.upload(t.hmf_z, t.n_hz, s));
+  Y3B_TRY(B.d_dn.upload(t.dndlnmh, (size_t)t.n_hz * t.n_hm, s));
+  Y3B_TRY(B.d_bl.upload(S->halo_lnM, S->n_hl, s));
+  Y3B_TRY(B.d_bz.upload(S->halo_z, S->n_hz, s));
+  Y3B_TRY(B.d_bi.upload(S->bias, (size_t)S->n_hl * S->n_hz, s));
+  Y3B_TRY(B.d_xr.upload(S->xi_r, S->n_xr, s));
+  Y3B_TRY(B.d_xz.upload(S->xi_z, S->n_xz, s));
+  Y3B_TRY(B.d_xi.upload(S->xi_nl, (size_t)S->n_xr * S->n_xz, s));
   const bool table = !h->tab_lx.empty();
   std::vector<double> thq, wthq;
   if (table) {
-    Y3B_TRY(d_lx.upload(h->tab_lx.data(), h->tab_lx.size(), s));
-    Y3B_TRY(d_lxm.upload(h->tab_lxm.data(), h->tab_lxm.size(), s));
-    Y3B_TRY(d_lt.upload(h->tab_v.data(), h->tab_v.size(), s));
+    Y3B_TRY(B.d_lx.upload(h->tab_lx.data(), h->tab_lx.size(), s));
+    Y3B_TRY(B.d_lxm.upload(h->tab_lxm.data(), h->tab_lxm.size(), s));
+    Y3B_TRY(B.d_lt.upload(h->tab_v.data(), h->tab_v.size(), s));
   } else {
     h_gl(0.0, kPiP, 256, thq, wthq);
-    Y3B_TRY(d_th.upload(thq.data(), thq.size(), s));
-    Y3B_TRY(d_wth.upload(wthq.data(), wthq.size(), s));
+    for (double& x : thq) x = std::cos(x);  // the quadrature reads cos(theta) of its nodes
+    Y3B_TRY(B.d_th.upload(thq.data(), thq.size(), s));
+    Y3B_TRY(B.d_wth.upload(wthq.data(), wthq.size(), s));
   }
-  Y3B_TRY(d_lnx.upload(h->lnm_x.data(), n_lnm, s));
-  Y3B_TRY(d_lnw.upload(h->lnm_w.data(), n_lnm, s));
-  Y3B_TRY(d_theta.upload(theta.data(), theta.size(), s));
-  Y3B_TRY(d_geom.upload(geom.data(), geom.size(), s));
-  Y3B_TRY(d_bsel.upload(bsel.data(), bsel.size(), s));
-  Y3B_TRY(d_ts.upload(tslice.data(), tslice.size(), s));
-  Y3B_TRY(d_t0.upload(t0.data(), t0.size(), s));
-  Y3B_TRY(d_z0.upload(z0.data(), z0.size(), s));
+  Y3B_TRY(B.d_lnx.upload(h->lnm_x.data(), n_lnm, s));
+  Y3B_TRY(B.d_lnw.upload(h->lnm_w.data(), n_lnm, s));
+  Y3B_TRY(B.d_theta.upload(theta.data(), theta.size(), s));
+  Y3B_TRY(B.d_geom.upload(geom.data(), geom.size(), s));
+  Y3B_TRY(B.d_bsel.upload(bsel.data(), bsel.size(), s));
+  Y3B_TRY(B.d_ts.upload(tslice.data(), tslice.size(), s));
+  Y3B_TRY(B.d_t0.upload(t0.data(), t0.size(), s));
+  Y3B_TRY(B.d_z0.upload(z0.data(), z0.size(), s));
   const int nz_tot = (int)zz.size(), nth_tot = (int)theta.size(), ngp = c.n_gp;
   if (nz_tot) {
-    Y3B_TRY(d_zz.upload(zz.data(), nz_tot, s));
-    Y3B_TRY(d_zc.upload(zc.data(), nz_tot, s));
-    Y3B_TRY(d_chiz.upload(chiz.data(), nz_tot, s));
-    Y3B_TRY(d_thex.upload(thex.data(), nz_tot, s));
-    Y3B_TRY(d_zs.upload(zslice.data(), nz_tot, s));
+    Y3B_TRY(B.d_zz.upload(zz.data(), nz_tot, s));
+    Y3B_TRY(B.d_zc.upload(zc.data(), nz_tot, s));
+    Y3B_TRY(B.d_chiz.upload(chiz.data(), nz_tot, s));
+    Y3B_TRY(B.d_thex.upload(thex.data(), nz_tot, s));
+    Y3B_TRY(B.d_zs.upload(zslice.data(), nz_tot, s));
   }
-  Y3B_TRY(d_anchor.upload(anchor.data(), anchor.size(), s));
-  Y3B_TRY(d_denom.upload(denom.data(), nsl, s));
-  Y3B_TRY(d_wcl.upload(wcl.data(), wcl.size(), s));
-  Y3B_TRY(d_chio.upload(sl_chi.data(), nsl, s));
-  Y3B_TRY(d_zob.upload(h->sl_zob.data(), nsl, s));
-  Y3B_TRY(d_da.upload(sl_da.data(), nsl, s));
-  Y3B_TRY(d_sci.upload(sl_sci.data(), nsl, s));
-  Y3B_TRY(d_gps.upload(h->gp_slice.data(), ngp, s));
-  Y3B_TRY(d_gpR.upload(h->gp_R.data(), ngp, s));
-  Y3B_TRY(d_AB.alloc(std::max(nz_tot, 1)));
-  Y3B_TRY(d_WZ.alloc((size_t)std::max(nz_tot, 1) * n_lnm));
-  Y3B_TRY(d_wrnd.alloc((size_t)nsl * n_lnm));
-  Y3B_TRY(d_psi.alloc(std::max(nth_tot, 1)));
-  Y3B_TRY(d_out.alloc((size_t)ngp * 9));
-  PrjTables T{t.n_hm, t.n_hz, d_mh.get(), d_hz.get(), d_dn.get(), S->cosmo.hmf_s,
-              S->cosmo.hmf_q, S->n_hl, S->n_hz, d_bl.get(), d_bz.get(), d_bi.get(), S->n_xr,
-              S->n_xz, d_xr.get(), d_xz.get(), d_xi.get(),
+  Y3B_TRY(B.d_anchor.upload(anchor.data(), anchor.size(), s));
+  Y3B_TRY(B.d_denom.upload(denom.data(), nsl, s));
+  Y3B_TRY(B.d_wcl.upload(wcl.data(), wcl.size(), s));
+  Y3B_TRY(B.d_chio.upload(sl_chi.data(), nsl, s));
+  Y3B_TRY(B.d_zob.upload(h->sl_zob.data(), nsl, s));
+  Y3B_TRY(B.d_da.upload(sl_da.data(), nsl, s));
+  Y3B_TRY(B.d_sci.upload(sl_sci.data(), nsl, s));
+  Y3B_TRY(B.d_gps.upload(h->gp_slice.data(), ngp, s));
+  Y3B_TRY(B.d_gpR.upload(h->gp_R.data(), ngp, s));
+  Y3B_TRY(B.d_AB.alloc(std::max(nz_tot, 1)));
+  Y3B_TRY(B.d_WZ.alloc((size_t)std::max(nz_tot, 1) * n_lnm));
+  Y3B_TRY(B.d_wrnd.alloc((size_t)nsl * n_lnm));
+  Y3B_TRY(B.d_psi.alloc(std::max(nth_tot, 1)));
+  Y3B_TRY(B.d_out.alloc((size_t)ngp * 9));
+  PrjTables T{t.n_hm, t.n_hz, B.d_mh.get(), B.d_hz.get(), B.d_dn.get(), S->cosmo.hmf_s,
+              S->cosmo.hmf_q, S->n_hl, S->n_hz, B.d_bl.get(), B.d_bz.get(), B.d_bi.get(), S->n_xr,
+              S->n_xz, B.d_xr.get(), B.d_xz.get(), B.d_xi.get(),
               table ? (int)h->tab_lx.size() : 0, table ? (int)h->tab_lxm.size() : 0,
-              d_lx.get(), d_lxm.get(), d_lt.get(), table ? 0 : (int)thq.size(), d_th.get(),
-              d_wth.get(), om};
+              B.d_lx.get(), B.d_lxm.get(), B.d_lt.get(), table ? 0 : (int)thq.size(), B.d_th.get(),
+              B.d_wth.get(), om};
   if (nz_tot) {
-    prj_z_kernel<<<nz_tot, 128, 0, s>>>(T, n_lnm, d_lnx.get(), d_lnw.get(), d_zs.get(),
-                                        d_zz.get(), d_zc.get(), d_anchor.get(), d_denom.get(),
-                                        d_AB.get(), d_WZ.get());
+    prj_z_kernel<<<nz_tot, 128, 0, s>>>(T, n_lnm, B.d_lnx.get(), B.d_lnw.get(), B.d_zs.get(),
+                                        B.d_zz.get(), B.d_zc.get(), B.d_anchor.get(), B.d_denom.get(),
+                                        B.d_AB.get(), B.d_WZ.get());
     count_launch();
     Y3B_CUDA(cudaGetLastError());
   }
-  prj_wrnd_kernel<<<(nsl * n_lnm + 127) / 128, 128, 0, s>>>(nsl, n_lnm, d_z0.get(), d_WZ.get(),
-                                                             d_wrnd.get());
+  prj_wrnd_kernel<<<(nsl * n_lnm + 127) / 128, 128, 0, s>>>(nsl, n_lnm, B.d_z0.get(), B.d_WZ.get(),
+                                                             B.d_wrnd.get());
   count_launch();
   Y3B_CUDA(cudaGetLastError());
-  prj_psi_kernel<<<(nth_tot + 127) / 128, 128, 0, s>>>(T, nth_tot, d_ts.get(), d_theta.get(),
-                                                       d_z0.get(), d_chiz.get(), d_thex.get(),
-                                                       d_AB.get(), d_chio.get(), d_zob.get(),
-                                                       d_psi.get());
+  prj_psi_kernel<<<(nth_tot + 127) / 128, 128, 0, s>>>(T, nth_tot, B.d_ts.get(), B.d_theta.get(),
+                                                       B.d_z0.get(), B.d_chiz.get(), B.d_thex.get(),
+                                                       B.d_AB.get(), B.d_chio.get(), B.d_zob.get(),
+                                                       B.d_psi.get());
   count_launch();
   Y3B_CUDA(cudaGetLastError());
-  prj_eval_kernel<<<ngp, 256, 0, s>>>(T, n_lnm, d_lnx.get(), d_gps.get(), d_gpR.get(),
-                                      d_t0.get(), d_theta.get(), d_geom.get(), d_bsel.get(),
-                                      d_psi.get(), d_wrnd.get(), d_wcl.get(), d_da.get(),
-                                      d_sci.get(), d_out.get());
+  int max_nt = 0;
+  for (int k = 0; k < nsl; ++k) max_nt = std::max(max_nt, t0[k + 1] - t0[k]);
+  const int max_pairs = std::max(max_nt * n_lnm, 1);
+  Y3B_TRY(B.d_V.alloc((size_t)ngp * max_pairs));
+  prj_profile_kernel<<<dim3((max_pairs + 255) / 256, ngp), 256, 0, s>>>(
+    T, n_lnm, B.d_lnx.get(), B.d_gps.get(), B.d_gpR.get(), B.d_t0.get(), B.d_theta.get(), B.d_da.get(),
+    max_pairs, B.d_V.get());
   count_launch();
   Y3B_CUDA(cudaGetLastError());
-  Y3B_CUDA(cudaMemcpyAsync(out, d_out.get(), (size_t)ngp * 9 * sizeof(double),
+  prj_eval_kernel<<<ngp, 256, 0, s>>>(n_lnm, B.d_gps.get(), B.d_t0.get(), B.d_geom.get(),
+                                      B.d_bsel.get(), B.d_psi.get(), B.d_wrnd.get(), B.d_wcl.get(),
+                                      B.d_sci.get(), max_pairs, B.d_V.get(), B.d_out.get());
+  count_launch();
+  Y3B_CUDA(cudaGetLastError());
+  Y3B_CUDA(cudaMemcpyAsync(out, B.d_out.get(), (size_t)ngp * 9 * sizeof(double),
                            cudaMemcpyDeviceToHost, s));
   Y3B_CUDA(cudaStreamSynchronize(s));
   return Y3B_OK;
