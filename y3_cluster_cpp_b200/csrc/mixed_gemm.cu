@@ -487,6 +487,9 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
   uint64_t* fempty = fbar + kMaxFStages;  // F ring: MMAs done with the block
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(fempty + kMaxFStages);
   volatile int* abort_s = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  // Per vector slot, the decoded tile the loader staged: point, lnM tile,
+  // richness-bin group, window [kc_lo, kc_hi), grid index.
+  int* tinfo_s = reinterpret_cast<int*>(tmem_slot + 4);
 
   // Zero the operand ring once: columns a tile does not write stay finite.
   for (uint32_t i = tid * 16u; i < nst * kStageBytes; i += kThreads * 16u)
@@ -590,13 +593,22 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
     int chunk = 0, jt = 0;
     RingPos rp;
     for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++jt) {
-      const Tile T = decode_tile(t, tile_list, win_tile, win_stride, pts, grids);
-      const GridDev* G = T.G;
-      const int n_z = G->n_z, ntp = G->n_t_pad;
-      const int i0 = T.bg * G->nIc, nIh = min(G->nIc, G->nI - i0);
       const int slot = jt & 1;
       const float* vs = vec_s + slot * vec_floats;
       if (!warp_wait(smem_u32(&vec_full[slot]), (jt >> 1) & 1, abort_s, lane)) continue;
+      __syncwarp();  // orders lane 0's acquire before every lane's reads
+      // The tile as the loader decoded it (no global-memory chain here).
+      const int* ti = tinfo_s + 8 * slot;
+      Tile T;
+      T.p = ti[0];
+      T.mtile = ti[1];
+      T.bg = ti[2];
+      T.kc_lo = ti[3];
+      T.kc_hi = ti[4];
+      T.G = grids + ti[5];
+      const GridDev* G = T.G;
+      const int n_z = G->n_z, ntp = G->n_t_pad;
+      const int i0 = T.bg * G->nIc, nIh = min(G->nIc, G->nI - i0);
       const float c2 = vs[1];
       const float* dsm = vs + 132 + nz_max;
       // This thread's item: z node q, half g of the stage's 16 lam_t nodes,
@@ -696,6 +708,13 @@ contract_kernel(const GridDev* __restrict__ grids, const PointDev* __restrict__ 
         float* vs = vec_s + slot * vec_floats;
         const uint32_t bytes = 4u * (4 + n_z + ntp + (uks ? nIh * ntp : 0));
         const uint32_t vb = smem_u32(&vec_full[slot]);
+        int* ti = tinfo_s + 8 * slot;  // published by the arrive below (release)
+        ti[0] = T.p;
+        ti[1] = T.mtile;
+        ti[2] = T.bg;
+        ti[3] = T.kc_lo;
+        ti[4] = T.kc_hi;
+        ti[5] = (int)(T.G - grids);
         fence_proxy_async_smem();  // the producers' reads of this slot come first
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(vb),
                      "r"(bytes)
@@ -886,7 +905,7 @@ contract_smem_base(int stages, const ContractShape& c)
              4u * ((size_t)c.nz_max * kGemmRows + 2u * c.nJ * c.nz_max +
                    2u * vec_slot_floats(c.nz_max, c.ntp_max, c.uk_max));
   b = (b + 15) & ~size_t(15);
-  return b + 8 * (2 * kMaxStages + 2 * kMaxFStages + 9) + 16;
+  return b + 8 * (2 * kMaxStages + 2 * kMaxFStages + 9) + 16 + 2 * 8 * 4;
 }
 
 // F ring depth in stages that fits next to `stages` A stages (even, <= 16).
