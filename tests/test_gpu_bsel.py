@@ -46,6 +46,7 @@ def test_bsel_default_nodes_match_compiled_reference(gpu):
     out = h.eval([_sample(g, hod)])
     assert out.shape == (1, 12, 3)
     _check(out[0], g["vals"])
+    assert h.kernel_ms() > 0.0
     # the same sample again on the same handle, and twice in one batch
     out2 = h.eval([_sample(g, hod)] * 2)
     np.testing.assert_array_equal(out2[0], out[0])
