@@ -947,10 +947,10 @@ def run_ours(a):
 #   ncu --set full --clock-control none -k regex:contract_kernel -s 2 -c 1 \
 #       python bench.py --steps 3 --warmup 3 --batch 256 --no-cpu-baseline \
 #       --serve-requests 0 --no-extra-workloads
-# (73.32 MB read + 2.90 MB written over 256 points).  Traffic grows with the
+# (73.32 MB read + 3.07 MB written over 256 points).  Traffic grows with the
 # points (each reads its own operand blocks), so a launch of B points moves
 # B times this.
-CONTRACT_TRAFFIC_BYTES_PER_POINT_4X = 297720.0
+CONTRACT_TRAFFIC_BYTES_PER_POINT_4X = 298426.0
 
 
 def ncu_traffic(density, points):
