@@ -41,8 +41,9 @@ What it writes (tests/golden/*.npz / *.json):
 * bsel_ref.npz -- P1, I1, J from the reference's compiled P_operator
   (src/models/p_operator_t.hh, module b_sel_marg) on the same fiducial
   tables with seeded HOD parameters: default node counts on 12 (z_obs bin,
-  richness bin) points, and reduced, odd node counts on 16 points for two
-  samples (the second with its own z_pivot, sigma_lambda and M1).
+  richness bin) points, reduced, odd node counts on 16 points for two
+  samples (the second with its own z_pivot, sigma_lambda and M1), and one
+  and two nodes per axis on four edge bins.
 * selgl_ref.npz -- numcountssel/vals, SelGLCore weights and
   shear1hmissel/vals (exact and idea2) from the reference's own C++
   (src/models/n_operator_sel_gl_t.hh:75-361), compiled from its sources by
@@ -468,6 +469,12 @@ def bsel_reference(ref):
     cfg = dict(lnm_low=np.log(1e13), lnm_high=np.log(10 ** 15.5))
     cfg2 = dict(cfg, n_lt=24, n_zring=9, n_zouter=15, n_lnm=16, n_theta=7, n_zt_ref=40)
     hod2 = dict(BSEL_HOD, z_pivot=0.3, sigma_lambda=0.3, log10_M1=13.1)
+    # Degenerate node counts (one node per axis; two) on edge bins: a narrow
+    # low-z_obs bin and one whose line of sight leaves the reference z grid.
+    grid3 = dict(zo_low=np.array([0.1, 0.5, 0.8, 0.2]), zo_high=np.array([0.12, 0.65, 0.86, 0.35]),
+                 lambda_bin=np.array([0.0, 3.0, 1.0, 2.0]))
+    cfg3 = dict(cfg, n_lt=1, n_zring=1, n_zouter=1, n_lnm=1, n_theta=1, n_zt_ref=2)
+    cfg4 = dict(cfg, n_lt=3, n_zring=2, n_zouter=2, n_lnm=2, n_theta=2, n_zt_ref=5)
     return dict(omega_m=p.om, h0=p.h0, **{"t_" + k: np.asarray(v) for k, v in p.tables.items()},
                 **{"prj_" + k: np.asarray(v) for k, v in prj.items()},
                 **{"gp_" + k: v for k, v in grid.items()},
@@ -476,6 +483,11 @@ def bsel_reference(ref):
                 **{"cfg2_" + k: v for k, v in cfg2.items()},
                 **{"hod_" + k: v for k, v in BSEL_HOD.items()},
                 **{"hod2_" + k: v for k, v in hod2.items()},
+                **{"gp3_" + k: v for k, v in grid3.items()},
+                **{"cfg3_" + k: v for k, v in cfg3.items()},
+                **{"cfg4_" + k: v for k, v in cfg4.items()},
+                vals3=R.bsel_marg(cfg3, cosmo, p.tables, prj, BSEL_HOD, grid3),
+                vals4=R.bsel_marg(cfg4, cosmo, p.tables, prj, BSEL_HOD, grid3),
                 vals=R.bsel_marg(cfg, cosmo, p.tables, prj, BSEL_HOD, grid),
                 vals2=np.stack([R.bsel_marg(cfg2, cosmo, p.tables, prj, h, grid2)
                                 for h in (BSEL_HOD, hod2)]))

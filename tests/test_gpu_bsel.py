@@ -64,6 +64,21 @@ def test_bsel_reduced_nodes_two_samples_match_compiled_reference(gpu):
     h.close()
 
 
+@pytest.mark.parametrize("case", ["3", "4"])
+def test_bsel_degenerate_nodes_and_edge_bins_match_compiled_reference(gpu, case):
+    """One and two nodes per axis (GL of one node; a theta grid that cannot
+    split; two reference z nodes) on a narrow low-z_obs bin and a bin whose
+    line of sight leaves the reference z grid (linear extrapolation there, as
+    the reference's bracket does)."""
+    g = _golden()
+    grid, cfg = _sub(g, "gp3_"), _sub(g, "cfg" + case + "_")
+    nodes = {k: int(v) for k, v in cfg.items() if k.startswith("n_")}
+    h = E.BselMarg(grid, cfg["lnm_low"], cfg["lnm_high"], **nodes)
+    out = h.eval([_sample(g, _sub(g, "hod_"))])
+    _check(out[0], g["vals" + case])
+    h.close()
+
+
 def test_bsel_chunked_batch_matches_single_calls(gpu):
     """A batch larger than the handle's device chunk equals per-sample calls."""
     g = _golden()
