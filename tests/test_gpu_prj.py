@@ -194,3 +194,22 @@ def test_prj_module_setup_execute_matches_golden(gpu, tmp_path, monkeypatch):
     out = np.stack([b[s, n] for s, n in cols], axis=1)
     _check(out, ref)
     assert m.cleanup() == 0
+
+
+def test_prj_line_of_sight_outside_distances_is_a_domain_error(gpu):
+    """A line-of-sight z node beyond distances/z (the reference's Interp1D on
+    d_a throws there) returns Y3B_ERR_DOMAIN before any launch, and the same
+    handle then evaluates a complete sample."""
+    g = _golden()
+    t, prj, grid, cfg = _inputs(g)
+    cos = E.cosmo(float(g["omega_m"]), float(g["h0"]))
+    keep = t["dist_z"] <= 0.45
+    t_cut = dict(t, dist_z=t["dist_z"][keep], dist_da=t["dist_da"][keep])
+    prj_cut = dict(prj, dist_dc=prj["dist_dc"][keep])
+    h = E.PrjShear(grid, **cfg)
+    h.set_mis_table(g["single_logx"], g["single_logxmis"], g["single_log_tab"])
+    with pytest.raises(E.A.Y3BError) as e:
+        h.eval(cos, t_cut, prj_cut)
+    assert e.value.status == E.A.ERR_DOMAIN
+    _check(h.eval(cos, t, prj), g["vals"])
+    h.close()
